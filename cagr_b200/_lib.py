@@ -1,0 +1,86 @@
+"""ctypes binding of libcagr_b200.so (the C ABI in include/cagr.h).
+
+The library is required: there is no CPU fallback.  Importing works on a
+machine without a GPU (the .so links the CUDA runtime statically and only
+touches the device when a function is called), so the CPU test suite can
+check that every declared symbol is exported.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+from .build import LIB_PATH, ROOT
+
+HEADER = os.path.join(ROOT, "include", "cagr.h")
+
+# status codes (include/cagr.h)
+CAGR_OK = 0
+# dtypes
+CAGR_F32, CAGR_F64 = 0, 1
+# operators
+OPS = {"A": 0, "AT": 1, "A3": 2, "A21": 3, "A22": 4, "A23": 5, "A2T1": 6, "A2T2": 7,
+       "A2T3": 8, "G": 9, "A2_FUSED": 10}
+ATTR_DIM = {"A": 3, "AT": 1, "A3": 3, "A21": 3, "A22": 3, "A23": 3, "A2T1": 1, "A2T2": 1,
+            "A2T3": 1, "G": 3, "A2_FUSED": 3}
+OUT_DIM = {"A": 1, "AT": 3, "A3": 1, "A21": 1, "A22": 1, "A23": 1, "A2T1": 3, "A2T2": 3,
+           "A2T3": 3, "G": 3, "A2_FUSED": 3}
+
+_p = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_i32 = ctypes.c_int
+_pp = ctypes.POINTER(ctypes.c_void_p)
+_pi64 = ctypes.POINTER(ctypes.c_int64)
+
+_SIGNATURES = {
+    "cagr_version": (_i32, []),
+    "cagr_status_string": (ctypes.c_char_p, [_i32]),
+    "cagr_last_error": (ctypes.c_char_p, []),
+    "cagr_tree_build": (_i32, [_p, _i64, _i32, _i32, _i32, _p, _pp]),
+    "cagr_tree_destroy": (_i32, [_p]),
+    "cagr_tree_info": (_i32, [_p, _pi64, _pi64, _pi64, _pi64, _pi64]),
+    "cagr_tree_export": (_i32, [_p] * 9),
+    "cagr_tree_morton_order": (_i32, [_p, _p, _p]),
+    "cagr_scatter": (_i32, [_p, _i32, _p, _i32, _p, _p]),
+    "cagr_scatter_export": (_i32, [_p, _i32, _p, _p, _p, _p]),
+    "cagr_multiply": (_i32, [_p, _i32, _p, _p, _i64, _p, ctypes.c_double, _i32, _p, _i64, _p]),
+    "cagr_forward": (_i32, [_p, _i32, _p, _p, ctypes.c_double, _i32, _p, _p]),
+}
+
+_lib = None
+
+
+class CagrError(RuntimeError):
+    """A cagr_* call returned a non-zero status."""
+
+
+def header_symbols() -> list[str]:
+    """Names of every function declared in include/cagr.h."""
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\**\s+\**(cagr_\w+)\s*\(", text, re.M)))
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m cagr_b200.build` "
+                "(the treecode has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != CAGR_OK:
+        L = lib()
+        msg = L.cagr_last_error().decode(errors="replace")
+        kind = L.cagr_status_string(rc).decode()
+        raise CagrError(f"{what}: {kind} ({rc}): {msg}")

@@ -1,0 +1,162 @@
+// extern "C" entry points declared in include/cagr.h.
+#include <string>
+
+#include "../../include/cagr.h"
+#include "internal.h"
+
+struct cagr_tree {
+    cagr::Tree* t;
+};
+
+namespace cagr {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+int set_error(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+}  // namespace cagr
+
+using cagr::set_error;
+
+namespace {
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int check_tree(const cagr_tree* h) {
+    if (!h || !h->t) return set_error(CAGR_ERR_INVALID, "tree handle is null");
+    return CAGR_OK;
+}
+
+int op_attr_dim(int op) {
+    switch (op) {
+        case CAGR_OP_AT:
+        case CAGR_OP_A2T1:
+        case CAGR_OP_A2T2:
+        case CAGR_OP_A2T3: return 1;
+        case CAGR_OP_A:
+        case CAGR_OP_A3:
+        case CAGR_OP_A21:
+        case CAGR_OP_A22:
+        case CAGR_OP_A23:
+        case CAGR_OP_G:
+        case CAGR_OP_A2_FUSED: return 3;
+        default: return 0;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int cagr_version(void) { return 100; }
+
+const char* cagr_status_string(int status) {
+    switch (status) {
+        case CAGR_OK: return "ok";
+        case CAGR_ERR_INVALID: return "invalid argument";
+        case CAGR_ERR_CUDA: return "CUDA error";
+        case CAGR_ERR_ALLOC: return "device allocation failed";
+        case CAGR_ERR_OVERFLOW: return "size exceeds index range";
+        case CAGR_ERR_STATE: return "invalid call order";
+        default: return "unknown status";
+    }
+}
+
+const char* cagr_last_error(void) { return cagr::g_last_error.c_str(); }
+
+int cagr_tree_build(const void* points_dev, int64_t n, int dtype, int max_depth, int leaf_size,
+                    void* stream, cagr_tree** out_tree) {
+    if (!out_tree) return set_error(CAGR_ERR_INVALID, "out_tree is null");
+    *out_tree = nullptr;
+    cagr::Tree* t = nullptr;
+    int rc = cagr::tree_build(points_dev, n, dtype, max_depth, leaf_size, as_stream(stream), &t);
+    if (rc != CAGR_OK) return rc;
+    *out_tree = new cagr_tree{t};
+    return CAGR_OK;
+}
+
+int cagr_tree_destroy(cagr_tree* tree) {
+    if (!tree) return CAGR_OK;
+    cagr::tree_free(tree->t);
+    delete tree;
+    return CAGR_OK;
+}
+
+int cagr_tree_info(const cagr_tree* tree, int64_t* num_points, int64_t* num_nodes,
+                   int64_t* num_leaves, int64_t* depth, int64_t* n2p_len) {
+    if (int rc = check_tree(tree)) return rc;
+    const cagr::Tree* t = tree->t;
+    if (num_points) *num_points = t->n;
+    if (num_nodes) *num_nodes = t->m;
+    if (num_leaves) *num_leaves = t->num_leaves;
+    if (depth) *depth = t->depth;
+    if (n2p_len) *n2p_len = t->n2p_len;
+    return CAGR_OK;
+}
+
+int cagr_tree_export(const cagr_tree* tree, int64_t* parent_dev, int64_t* children_dev,
+                     uint8_t* is_leaf_dev, void* half_w_dev, int64_t* npts_dev, int64_t* n2p_dev,
+                     int64_t* n2p_start_dev, void* stream) {
+    if (int rc = check_tree(tree)) return rc;
+    return cagr::tree_export(tree->t, parent_dev, children_dev, is_leaf_dev, half_w_dev, npts_dev,
+                             n2p_dev, n2p_start_dev, as_stream(stream));
+}
+
+int cagr_tree_morton_order(const cagr_tree* tree, int32_t* perm_dev, void* stream) {
+    if (int rc = check_tree(tree)) return rc;
+    if (!perm_dev) return set_error(CAGR_ERR_INVALID, "perm_dev is null");
+    cudaError_t e = cudaMemcpyAsync(perm_dev, tree->t->perm, sizeof(int32_t) * tree->t->n,
+                                    cudaMemcpyDeviceToDevice, as_stream(stream));
+    if (e != cudaSuccess) return set_error(CAGR_ERR_CUDA, cudaGetErrorString(e));
+    return CAGR_OK;
+}
+
+int cagr_scatter(cagr_tree* tree, int slot, const void* attrs_dev, int attr_dim,
+                 const void* weights_dev, void* stream) {
+    if (int rc = check_tree(tree)) return rc;
+    return cagr::moments(tree->t, slot, attrs_dev, attr_dim, weights_dev, as_stream(stream));
+}
+
+int cagr_scatter_export(const cagr_tree* tree, int slot, void* node_attrs_dev,
+                        void* reppoints_dev, void* node_weights_dev, void* stream) {
+    if (int rc = check_tree(tree)) return rc;
+    return cagr::moments_export(tree->t, slot, node_attrs_dev, reppoints_dev, node_weights_dev,
+                                as_stream(stream));
+}
+
+int cagr_multiply(const cagr_tree* tree, int op, const void* queries_dev,
+                  const int32_t* query_order_dev, int64_t nq, const void* widths_dev,
+                  double width, int continuous, void* out_dev, int64_t out_stride, void* stream) {
+    if (int rc = check_tree(tree)) return rc;
+    if (op_attr_dim(op) == 0) return set_error(CAGR_ERR_INVALID, "unknown operator");
+    if (out_stride < 0 || out_stride > (1 << 20))
+        return set_error(CAGR_ERR_INVALID, "out_stride out of range");
+    cagr::TraverseArgs a;
+    a.op = op;
+    a.continuous = continuous;
+    a.queries = queries_dev;
+    a.qorder = query_order_dev;
+    a.nq = nq;
+    a.widths = widths_dev;
+    a.width = width;
+    a.out = out_dev;
+    a.out_stride = (int)out_stride;
+    return cagr::traverse(tree->t, a, as_stream(stream));
+}
+
+int cagr_forward(cagr_tree* tree, int op, const void* values_dev, const void* widths_dev,
+                 double width, int continuous, void* out_dev, void* stream) {
+    if (int rc = check_tree(tree)) return rc;
+    const int dim = op_attr_dim(op);
+    if (dim == 0) return set_error(CAGR_ERR_INVALID, "unknown operator");
+    if (int rc = cagr::moments(tree->t, 0, values_dev, dim, nullptr, as_stream(stream))) return rc;
+    return cagr_multiply(tree, op, nullptr, nullptr, 0, widths_dev, width, continuous, out_dev, 0,
+                         stream);
+}
+
+}  // extern "C"

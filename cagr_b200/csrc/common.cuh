@@ -1,0 +1,109 @@
+// Shared definitions for the CAGR treecode library (sm_100a).
+//
+// Layout in HBM (one tree, N points, M nodes, nodes numbered in preorder
+// exactly as the reference serialiser numbers them):
+//   perm[N]        int32  Morton-sorted position -> original point index
+//   meta[M]        int4   {next (preorder skip pointer), pstart (first sorted
+//                          position covered), npts (points under the node),
+//                          depth | is_leaf << 8 | nchild << 16}
+//   parent[M]      int32  parent id (-1 for the root)
+//   leaf_ids[NL]   int32  leaf node ids in preorder
+//   rec[(M+N)*12]  T      source records: [0, M) node records (centroid,
+//                          exp(-c/2), attribute sums, weight), [M, M+N)
+//                          point records in Morton order (position,
+//                          exp(-y/2), attribute) -- rewritten by every
+//                          moment pass.
+//   counters[M]    uint32 arrival counters for the bottom-up moment pass
+//                          (self-resetting).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define CAGR_MAX_DEPTH 21
+#define CAGR_REC_STRIDE 12  // scalars per source record
+
+// Record slots (in units of T) inside one record of CAGR_REC_STRIDE scalars.
+#define REC_X 0
+#define REC_Y 1
+#define REC_Z 2
+#define REC_E1 3
+#define REC_E2 4
+#define REC_E3 5
+#define REC_A0 6
+#define REC_A1 7
+#define REC_A2 8
+#define REC_W 9
+
+namespace cagr {
+
+// Status codes returned by every extern "C" entry point (mirrored in include/cagr.h).
+enum Status : int {
+    kOk = 0,
+    kErrInvalid = 1,
+    kErrCuda = 2,
+    kErrAlloc = 3,
+    kErrOverflow = 4,
+    kErrState = 5,
+};
+
+__host__ __device__ inline int meta_depth(int w) { return w & 0xff; }
+__host__ __device__ inline bool meta_leaf(int w) { return (w >> 8) & 1; }
+__host__ __device__ inline int meta_nchild(int w) { return (w >> 16) & 0xff; }
+
+// Squared distance in the reference's operation order: d = x - c per axis,
+// then ((dx*dx + dy*dy) + dz*dz), each step rounded (no FMA contraction), so
+// acceptance and width decisions match the reference bit for bit.
+__device__ __forceinline__ float dist2_exact(float dx, float dy, float dz) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+__device__ __forceinline__ double dist2_exact(double dx, double dy, double dz) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float sqrt_rn(float a) { return __fsqrt_rn(a); }
+__device__ __forceinline__ double sqrt_rn(double a) { return __dsqrt_rn(a); }
+__device__ __forceinline__ float rsqrt_t(float a) { return rsqrtf(a); }
+__device__ __forceinline__ double rsqrt_t(double a) { return rsqrt(a); }
+__device__ __forceinline__ float exp_t(float a) { return expf(a); }
+__device__ __forceinline__ double exp_t(double a) { return exp(a); }
+
+// Smallest t >= 0 with sqrt_rn(t) >= w, so that for any r2 computed with
+// dist2_exact:  sqrt_rn(r2) >= w  <=>  r2 >= t.  The reference tests
+// `sqrt(r2) >= w` (wn_treecode_cuda_kernels.cu:90,127); this lets the inner
+// loop compare squares without losing bit-exactness of the decision.
+template <typename T>
+__device__ __forceinline__ T width_threshold(T w) {
+    if (w != w) return T(INFINITY);  // NaN width: `r >= w` is false for every pair
+    if (!(w > T(0))) return T(0);    // w <= 0: every pair passes `r >= w`
+    T t = mul_rn(w, w);
+    if (!(t < T(INFINITY))) return t;
+    // walk down while the predecessor still satisfies the test, then up
+    for (int it = 0; it < 8; it++) {
+        T prev = nextafter(t, T(0));
+        if (sqrt_rn(prev) >= w) t = prev;
+        else break;
+    }
+    for (int it = 0; it < 8; it++) {
+        if (sqrt_rn(t) >= w) break;
+        t = nextafter(t, T(INFINITY));
+    }
+    return t;
+}
+
+// (4 * half_w)^2 for a node at `depth` (half_w = 2^-depth): the reference
+// acceptance threshold `pow(4 * half_w, 2)` (wn_treecode_cuda_kernels.cu:595),
+// exact in both precisions.
+template <typename T>
+__device__ __forceinline__ T mac_radius2(int depth) {
+    return T(16.0) * ldexp(T(1.0), -2 * depth);
+}
+
+}  // namespace cagr

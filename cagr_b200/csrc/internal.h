@@ -1,0 +1,98 @@
+// Host-side structures shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "common.cuh"
+
+namespace cagr {
+
+// Records the message for cagr_last_error() and returns `code`.
+int set_error(int code, const std::string& msg);
+
+// CUDA call check inside functions returning a status code.
+#define CAGR_CUDA(call)                                                                  \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            return ::cagr::set_error(::cagr::kErrCuda, std::string(#call) + ": " +       \
+                                                           cudaGetErrorString(e_));      \
+        }                                                                                \
+    } while (0)
+
+// Device arrays owned by one tree.  All pointers are device pointers.
+struct Tree {
+    int dtype = 0;  // 0 = float32, 1 = float64
+    int max_depth = 15;
+    int leaf_size = 1;
+    int device = 0;
+    int64_t n = 0;           // points
+    int64_t m = 0;           // nodes
+    int64_t num_leaves = 0;
+    int64_t depth = 0;       // deepest node
+    int64_t n2p_len = 0;     // total length of the per-node point lists
+
+    int32_t* perm = nullptr;       // [N] sorted position -> original index
+    int32_t* invperm = nullptr;    // [N] original index -> sorted position
+    int4* meta = nullptr;          // [M]
+    int32_t* parent = nullptr;     // [M]
+    int32_t* children = nullptr;   // [M*8], -1 = none
+    int32_t* leaf_ids = nullptr;   // [num_leaves]
+    int64_t* n2p_start = nullptr;  // [M]
+    int32_t* n2p = nullptr;        // [n2p_len] original indices
+    void* spos = nullptr;          // [N*3] T, positions in sorted order
+    uint32_t* counters = nullptr;  // [M], zero between moment passes
+    void* rec[3] = {nullptr, nullptr, nullptr};  // [(M+N)*CAGR_REC_STRIDE] T per slot
+    int rec_dim[3] = {0, 0, 0};    // attribute dim the slot was filled with (0 = empty)
+};
+
+int tree_build(const void* points, int64_t n, int dtype, int max_depth, int leaf_size,
+               cudaStream_t stream, Tree** out);
+void tree_free(Tree* t);
+int tree_export(const Tree* t, int64_t* parent, int64_t* children, uint8_t* is_leaf,
+                void* half_w, int64_t* npts, int64_t* n2p, int64_t* n2p_start,
+                cudaStream_t stream);
+
+// Bottom-up node moments into record slot `slot`.  attrs: [N, dim] in the
+// tree dtype (original point order); weights: [N] or null (then |attr|).
+int moments(Tree* t, int slot, const void* attrs, int dim, const void* weights,
+            cudaStream_t stream);
+// Copy node moments of a slot out in the reference layout:
+// node_attrs [M, dim], reppoints [M, 3], weights [M].
+int moments_export(const Tree* t, int slot, void* node_attrs, void* reppoints, void* weights,
+                   cudaStream_t stream);
+
+// Operator codes (mirrored in include/cagr.h).
+enum Op : int {
+    kOpA = 0,
+    kOpAT = 1,
+    kOpA3 = 2,
+    kOpA21 = 3,
+    kOpA22 = 4,
+    kOpA23 = 5,
+    kOpA2T1 = 6,
+    kOpA2T2 = 7,
+    kOpA2T3 = 8,
+    kOpG = 9,
+    kOpA2Fused = 10,    // (A21, A22, A23) in one traversal -> [N', 3]
+    kOpA2TFused = 11,   // sum_k A2Tk(s_k), slots 0..2 -> [N', 3]
+};
+
+struct TraverseArgs {
+    int op = 0;
+    int continuous = 0;
+    const void* queries = nullptr;     // [nq, 3] T or null (= the tree's points)
+    const int32_t* qorder = nullptr;   // [nq] processing order or null
+    int64_t nq = 0;
+    const void* widths = nullptr;      // [nq] T or null (then `width`)
+    double width = 0.0;
+    void* out = nullptr;               // [nq, out_dim] T
+    int out_stride = 0;                // scalars between consecutive queries (0 = out_dim)
+};
+
+int traverse(const Tree* t, const TraverseArgs& a, cudaStream_t stream);
+
+}  // namespace cagr

@@ -1,0 +1,573 @@
+// Device octree build, bit-exact with the reference serialised layout.
+//
+// Reference semantics (mayueji/CAGR, CUDA-based/ext/wn_treecode/wn_treecode_cpu/
+// wn_treecode_cpu_treeutils.cpp:90-177 and :202-258): recursive split of
+// [-1,1]^3 around dyadic centres with octant code (x>=cx) + 2(y>=cy) + 4(z>=cz),
+// leaf when depth == max_depth or the node holds <= leaf_size points, nodes
+// numbered in preorder (octants in order), and every node's point list (ascending
+// original index) concatenated in preorder.
+//
+// B200 formulation (no recursion, O(N log N) parallel work):
+//  1. Per-axis integer keys floor(x * 2^(D-1)) + 2^(D-1) (exact: a power-of-two
+//     scale, a floor and an integer add; D = max_depth), bit-interleaved into a
+//     3D-bit Morton code whose j-th 3-bit digit is the reference octant code at
+//     depth j.  Bit b of the key is set exactly when x >= the depth-(D-1-b)
+//     centre the reference compares against.
+//  2. Stable radix sort of (code, index): equal codes keep ascending index.
+//  3. lcp[i] = number of equal leading digits of codes i-1 and i.  Position i
+//     opens cells at depths lcp[i]+1..D.  The cell at depth d starting at i is a
+//     node iff its parent cell holds > leaf_size points, and it is internal iff
+//     it holds > leaf_size points and d < D; the nodes starting at position i
+//     therefore form one chain of depths d0..dlast.
+//  4. Preorder id of node (d, i) = (nodes at positions < i) + (d - d0): sorting
+//     nodes by (first point, depth) is preorder.  Subtree ends and parents come
+//     from a sparse-table search over lcp.
+//  5. Per-node point lists: (node, index) pairs emitted in index order by a
+//     root-to-leaf walk, then a stable radix sort by node id.
+#include <cub/cub.cuh>
+
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace cagr {
+namespace {
+
+constexpr int kBlock = 256;
+
+inline unsigned grid_for(int64_t n, int block = kBlock) {
+    return (unsigned)((n + block - 1) / block);
+}
+
+// Stream-ordered temporary buffer.
+struct Tmp {
+    void* p = nullptr;
+    cudaStream_t s = nullptr;
+    ~Tmp() {
+        if (p) cudaFreeAsync(p, s);
+    }
+};
+
+int tmp_alloc(Tmp& t, size_t bytes, cudaStream_t s) {
+    t.s = s;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMallocAsync(&t.p, bytes, s);
+    if (e != cudaSuccess) {
+        t.p = nullptr;
+        return set_error(kErrAlloc, std::string("cudaMallocAsync(") + std::to_string(bytes) +
+                                        "): " + cudaGetErrorString(e));
+    }
+    return kOk;
+}
+
+int dev_alloc(void** p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return set_error(kErrAlloc, std::string("cudaMalloc(") + std::to_string(bytes) +
+                                        "): " + cudaGetErrorString(e));
+    }
+    return kOk;
+}
+
+// ---- step 1: Morton codes -------------------------------------------------
+
+template <typename T>
+__device__ __forceinline__ uint32_t axis_key(T v, int D) {
+    if (D == 0 || v != v) return 0u;  // NaN fails every `>=`: all-zero key
+    const T half = ldexp(T(1), D - 1);
+    const T s = floor(v * half);  // power-of-two scale: exact
+    if (s < -half) return 0u;
+    if (s >= half) return (1u << D) - 1u;
+    return (uint32_t)((int64_t)s + (int64_t)half);
+}
+
+__device__ __forceinline__ uint64_t spread3(uint32_t v) {
+    uint64_t x = v & 0x1fffffu;
+    x = (x | (x << 32)) & 0x1f00000000ffffull;
+    x = (x | (x << 16)) & 0x1f0000ff0000ffull;
+    x = (x | (x << 8)) & 0x100f00f00f00f00full;
+    x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
+    x = (x | (x << 2)) & 0x1249249249249249ull;
+    return x;
+}
+
+template <typename T>
+__global__ void k_morton(const T* __restrict__ pts, int64_t n, int D, uint64_t* __restrict__ keys,
+                         int32_t* __restrict__ idx) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t kx = axis_key(pts[3 * i + 0], D);
+    uint32_t ky = axis_key(pts[3 * i + 1], D);
+    uint32_t kz = axis_key(pts[3 * i + 2], D);
+    keys[i] = spread3(kx) | (spread3(ky) << 1) | (spread3(kz) << 2);
+    idx[i] = (int32_t)i;
+}
+
+__device__ __forceinline__ int digit_at(uint64_t code, int D, int d) {
+    // octant chosen by the split of a depth-d node (child at depth d+1)
+    return (int)((code >> (3 * (D - 1 - d))) & 7u);
+}
+
+// ---- step 3: lcp and node chains --------------------------------------------
+
+__global__ void k_lcp(const uint64_t* __restrict__ sk, int64_t n, int D, int8_t* __restrict__ lcp) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (i == 0) {
+        lcp[0] = -1;
+        return;
+    }
+    uint64_t x = sk[i - 1] ^ sk[i];
+    lcp[i] = (x == 0) ? (int8_t)D : (int8_t)((__clzll((long long)x) - (64 - 3 * D)) / 3);
+}
+
+__global__ void k_chain(const int8_t* __restrict__ lcp, int64_t n, int D, int s,
+                        int32_t* __restrict__ nn, int8_t* __restrict__ d0a,
+                        int8_t* __restrict__ dla, int32_t* __restrict__ isleafpos) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int d0 = (i == 0) ? 0 : lcp[i] + 1;
+    bool exists;
+    if (i == 0) {
+        exists = true;
+    } else if (d0 > D) {
+        exists = false;  // same code as the previous point: shares its leaf
+    } else {
+        // the parent cell (depth L = lcp[i]) must hold more than s points
+        const int L = lcp[i];
+        int64_t total = 1, a = i, b = i + 1;
+        while (total <= s && a > 0 && lcp[a] >= L) {
+            a--;
+            total++;
+        }
+        while (total <= s && b < n && lcp[b] >= L) {
+            b++;
+            total++;
+        }
+        exists = total > s;
+    }
+    int m = -1;  // min lcp over (i, i+s]: the deepest depth whose cell at i holds > s points
+    if (i + s < n) {
+        m = CAGR_MAX_DEPTH + 1;
+        for (int j = 1; j <= s; j++) m = min(m, (int)lcp[i + j]);
+    }
+    int dlast = (d0 < D && m >= d0) ? min(m + 1, D) : d0;
+    nn[i] = exists ? (dlast - d0 + 1) : 0;
+    d0a[i] = (int8_t)d0;
+    dla[i] = exists ? (int8_t)dlast : (int8_t)0;  // no node here: keep out of the depth max
+    isleafpos[i] = exists ? 1 : 0;
+}
+
+// sparse table level k from level k-1: st[k][j] = min(lcp[j .. j + 2^k - 1])
+__global__ void k_sparse_level(const int8_t* __restrict__ prev, int8_t* __restrict__ cur,
+                               int64_t n, int64_t half) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    int8_t a = prev[j];
+    cur[j] = (j + half < n) ? (int8_t)min((int)a, (int)prev[j + half]) : a;
+}
+
+// first j > i with lcp[j] < d, or n
+__device__ __forceinline__ int64_t fwd_search(const int8_t* __restrict__ st, int K, int64_t n,
+                                              int64_t i, int d) {
+    int64_t pos = i + 1;
+    for (int k = K - 1; k >= 0; k--) {
+        int64_t len = 1LL << k;
+        if (pos + len <= n && st[(int64_t)k * n + pos] >= d) pos += len;
+    }
+    return pos;
+}
+
+// largest j < i with lcp[j] < t (exists because lcp[0] = -1 and t >= 0)
+__device__ __forceinline__ int64_t bwd_search(const int8_t* __restrict__ st, int K, int64_t n,
+                                              int64_t i, int t) {
+    int64_t pos = i - 1;
+    for (int k = K - 1; k >= 0; k--) {
+        int64_t len = 1LL << k;
+        if (pos - len + 1 >= 0 && st[(int64_t)k * n + (pos - len + 1)] >= t) pos -= len;
+    }
+    return pos;
+}
+
+__global__ void k_emit(const uint64_t* __restrict__ sk, const int8_t* __restrict__ st, int K,
+                       int64_t n, int D, int64_t M, const int32_t* __restrict__ nn,
+                       const int32_t* __restrict__ base, const int8_t* __restrict__ d0a,
+                       const int8_t* __restrict__ dla, int4* __restrict__ meta,
+                       int32_t* __restrict__ parent, int32_t* __restrict__ children,
+                       int32_t* __restrict__ nchild, int64_t* __restrict__ npts64) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || nn[i] == 0) return;
+    const int d0 = d0a[i], dlast = dla[i];
+    const int64_t b = base[i];
+    for (int d = d0; d <= dlast; d++) {
+        const int64_t id = b + (d - d0);
+        const int64_t end = fwd_search(st, K, n, i, d);
+        const int64_t next = (end < n) ? (int64_t)base[end] : M;
+        int64_t par;
+        if (d == 0) {
+            par = -1;
+        } else if (d > d0) {
+            par = id - 1;
+        } else {
+            const int64_t p = bwd_search(st, K, n, i, d - 1);
+            par = (int64_t)base[p] + (d - 1 - d0a[p]);
+        }
+        const bool leaf = (d == dlast);
+        meta[id] = make_int4((int)next, (int)i, (int)(end - i), d | ((leaf ? 1 : 0) << 8));
+        parent[id] = (int32_t)par;
+        npts64[id] = end - i;
+        if (par >= 0) {
+            children[par * 8 + digit_at(sk[i], D, d - 1)] = (int32_t)id;
+            atomicAdd(&nchild[par], 1);
+        }
+    }
+}
+
+__global__ void k_pack(int4* __restrict__ meta, const int32_t* __restrict__ nchild, int64_t M) {
+    int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= M) return;
+    meta[id].w |= (nchild[id] & 0xff) << 16;
+}
+
+__global__ void k_leaf_ids(const int32_t* __restrict__ nn, const int32_t* __restrict__ base,
+                           const int8_t* __restrict__ d0a, const int8_t* __restrict__ dla,
+                           const int32_t* __restrict__ leafrank, int64_t n,
+                           int32_t* __restrict__ leaf_ids) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || nn[i] == 0) return;
+    leaf_ids[leafrank[i]] = base[i] + (dla[i] - d0a[i]);
+}
+
+__global__ void k_inv(const int32_t* __restrict__ perm, int64_t n, int32_t* __restrict__ inv) {
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    inv[perm[s]] = (int32_t)s;
+}
+
+template <typename T>
+__global__ void k_spos(const T* __restrict__ pts, const int32_t* __restrict__ perm, int64_t n,
+                       T* __restrict__ spos) {
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    int64_t p = perm[s];
+    spos[3 * s + 0] = pts[3 * p + 0];
+    spos[3 * s + 1] = pts[3 * p + 1];
+    spos[3 * s + 2] = pts[3 * p + 2];
+}
+
+// root-to-leaf walk for original point p: counts (WRITE=false) or emits pairs
+template <bool WRITE>
+__global__ void k_walk(const int32_t* __restrict__ invperm, const uint64_t* __restrict__ sk,
+                       const int4* __restrict__ meta, const int32_t* __restrict__ children, int D,
+                       int64_t n, int32_t* __restrict__ cnt, const int64_t* __restrict__ off,
+                       int32_t* __restrict__ pair_node, int32_t* __restrict__ pair_pt) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const uint64_t code = sk[invperm[p]];
+    int node = 0;
+    int64_t k = WRITE ? off[p] : 0;
+    int c = 0;
+    while (true) {
+        if (WRITE) {
+            pair_node[k + c] = node;
+            pair_pt[k + c] = (int32_t)p;
+        }
+        c++;
+        const int w = meta[node].w;
+        if (meta_leaf(w) || c > CAGR_MAX_DEPTH + 1) break;
+        node = children[node * 8 + digit_at(code, D, meta_depth(w))];
+        if (node < 0) break;  // unreachable for a consistent tree; never index with -1
+    }
+    if (!WRITE) cnt[p] = c;
+}
+
+__global__ void k_fill_i32(int32_t* a, int64_t n, int32_t v) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
+
+template <typename T>
+__global__ void k_export(const int4* __restrict__ meta, const int32_t* __restrict__ parent,
+                         const int32_t* __restrict__ children, const int64_t* __restrict__ n2ps,
+                         int64_t M, int64_t* __restrict__ o_parent, int64_t* __restrict__ o_children,
+                         uint8_t* __restrict__ o_leaf, T* __restrict__ o_half_w,
+                         int64_t* __restrict__ o_npts, int64_t* __restrict__ o_n2ps) {
+    int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= M) return;
+    const int4 mt = meta[id];
+    if (o_parent) o_parent[id] = parent[id];
+    if (o_children)
+        for (int k = 0; k < 8; k++) o_children[id * 8 + k] = children[id * 8 + k];
+    if (o_leaf) o_leaf[id] = meta_leaf(mt.w) ? 1 : 0;
+    if (o_half_w) o_half_w[id] = ldexp(T(1), -meta_depth(mt.w));
+    if (o_npts) o_npts[id] = mt.z;
+    if (o_n2ps) o_n2ps[id] = n2ps[id];
+}
+
+__global__ void k_widen(const int32_t* __restrict__ a, int64_t n, int64_t* __restrict__ b) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i];
+}
+
+// cub helpers -------------------------------------------------------------------
+
+template <typename F>
+int cub_call(F&& f, cudaStream_t s) {
+    size_t bytes = 0;
+    CAGR_CUDA(f(nullptr, bytes));
+    Tmp tmp;
+    if (int rc = tmp_alloc(tmp, bytes, s)) return rc;
+    CAGR_CUDA(f(tmp.p, bytes));
+    return kOk;
+}
+
+int bit_width(int64_t v) {
+    int b = 0;
+    while ((int64_t(1) << b) <= v && b < 62) b++;
+    return b;
+}
+
+template <typename T>
+int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) {
+    const unsigned gN = grid_for(n);
+    // 1-2: codes and stable sort
+    Tmp keys, keys2, idx, sorted_keys;
+    if (int rc = tmp_alloc(keys, sizeof(uint64_t) * n, st)) return rc;
+    if (int rc = tmp_alloc(sorted_keys, sizeof(uint64_t) * n, st)) return rc;
+    if (int rc = tmp_alloc(idx, sizeof(int32_t) * n, st)) return rc;
+    if (int rc = dev_alloc((void**)&t->perm, sizeof(int32_t) * n)) return rc;
+    k_morton<T><<<gN, kBlock, 0, st>>>(pts, n, D, (uint64_t*)keys.p, (int32_t*)idx.p);
+    CAGR_CUDA(cudaGetLastError());
+    const int end_bit = 3 * D;
+    if (end_bit > 0) {
+        if (int rc = cub_call(
+                [&](void* tp, size_t& b) {
+                    return cub::DeviceRadixSort::SortPairs(tp, b, (const uint64_t*)keys.p,
+                                                           (uint64_t*)sorted_keys.p,
+                                                           (const int32_t*)idx.p, t->perm, n, 0,
+                                                           end_bit, st);
+                },
+                st))
+            return rc;
+    } else {
+        CAGR_CUDA(cudaMemcpyAsync(sorted_keys.p, keys.p, sizeof(uint64_t) * n,
+                                  cudaMemcpyDeviceToDevice, st));
+        CAGR_CUDA(cudaMemcpyAsync(t->perm, idx.p, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice,
+                                  st));
+    }
+    const uint64_t* sk = (const uint64_t*)sorted_keys.p;
+
+    // 3: lcp, chains, sparse table
+    int K = 1;
+    while ((int64_t(1) << K) < n) K++;
+    Tmp stab, nn, d0a, dla, isleafpos, base, leafrank;
+    if (int rc = tmp_alloc(stab, (size_t)K * n, st)) return rc;
+    if (int rc = tmp_alloc(nn, sizeof(int32_t) * n, st)) return rc;
+    if (int rc = tmp_alloc(d0a, n, st)) return rc;
+    if (int rc = tmp_alloc(dla, n, st)) return rc;
+    if (int rc = tmp_alloc(isleafpos, sizeof(int32_t) * n, st)) return rc;
+    if (int rc = tmp_alloc(base, sizeof(int32_t) * (n + 1), st)) return rc;
+    if (int rc = tmp_alloc(leafrank, sizeof(int32_t) * (n + 1), st)) return rc;
+    int8_t* lcp = (int8_t*)stab.p;
+    k_lcp<<<gN, kBlock, 0, st>>>(sk, n, D, lcp);
+    k_chain<<<gN, kBlock, 0, st>>>(lcp, n, D, s, (int32_t*)nn.p, (int8_t*)d0a.p, (int8_t*)dla.p,
+                                   (int32_t*)isleafpos.p);
+    for (int k = 1; k < K; k++)
+        k_sparse_level<<<gN, kBlock, 0, st>>>(lcp + (int64_t)(k - 1) * n, lcp + (int64_t)k * n, n,
+                                              int64_t(1) << (k - 1));
+    CAGR_CUDA(cudaGetLastError());
+    if (int rc = cub_call(
+            [&](void* tp, size_t& b) {
+                return cub::DeviceScan::ExclusiveSum(tp, b, (const int32_t*)nn.p,
+                                                     (int32_t*)base.p, n + 0, st);
+            },
+            st))
+        return rc;
+    if (int rc = cub_call(
+            [&](void* tp, size_t& b) {
+                return cub::DeviceScan::ExclusiveSum(tp, b, (const int32_t*)isleafpos.p,
+                                                     (int32_t*)leafrank.p, n + 0, st);
+            },
+            st))
+        return rc;
+    int32_t last_base = 0, last_nn = 0, last_rank = 0, last_leaf = 0;
+    CAGR_CUDA(cudaMemcpyAsync(&last_base, (int32_t*)base.p + (n - 1), 4, cudaMemcpyDeviceToHost, st));
+    CAGR_CUDA(cudaMemcpyAsync(&last_nn, (int32_t*)nn.p + (n - 1), 4, cudaMemcpyDeviceToHost, st));
+    CAGR_CUDA(cudaMemcpyAsync(&last_rank, (int32_t*)leafrank.p + (n - 1), 4,
+                              cudaMemcpyDeviceToHost, st));
+    CAGR_CUDA(cudaMemcpyAsync(&last_leaf, (int32_t*)isleafpos.p + (n - 1), 4,
+                              cudaMemcpyDeviceToHost, st));
+    CAGR_CUDA(cudaStreamSynchronize(st));
+    const int64_t M = (int64_t)last_base + last_nn;
+    const int64_t NL = (int64_t)last_rank + last_leaf;
+    if (M <= 0 || M >= (int64_t(1) << 31) - 2)
+        return set_error(kErrOverflow, "node count out of range: " + std::to_string(M));
+    t->m = M;
+    t->num_leaves = NL;
+
+    // 4: nodes
+    if (int rc = dev_alloc((void**)&t->meta, sizeof(int4) * M)) return rc;
+    if (int rc = dev_alloc((void**)&t->parent, sizeof(int32_t) * M)) return rc;
+    if (int rc = dev_alloc((void**)&t->children, sizeof(int32_t) * M * 8)) return rc;
+    if (int rc = dev_alloc((void**)&t->leaf_ids, sizeof(int32_t) * NL)) return rc;
+    if (int rc = dev_alloc((void**)&t->n2p_start, sizeof(int64_t) * (M + 1))) return rc;
+    if (int rc = dev_alloc((void**)&t->counters, sizeof(uint32_t) * M)) return rc;
+    CAGR_CUDA(cudaMemsetAsync(t->counters, 0, sizeof(uint32_t) * M, st));
+    Tmp nchild, npts64;
+    if (int rc = tmp_alloc(nchild, sizeof(int32_t) * M, st)) return rc;
+    if (int rc = tmp_alloc(npts64, sizeof(int64_t) * (M + 1), st)) return rc;
+    CAGR_CUDA(cudaMemsetAsync(nchild.p, 0, sizeof(int32_t) * M, st));
+    k_fill_i32<<<grid_for(M * 8), kBlock, 0, st>>>(t->children, M * 8, -1);
+    k_emit<<<gN, kBlock, 0, st>>>(sk, lcp, K, n, D, M, (const int32_t*)nn.p,
+                                  (const int32_t*)base.p, (const int8_t*)d0a.p,
+                                  (const int8_t*)dla.p, t->meta, t->parent, t->children,
+                                  (int32_t*)nchild.p, (int64_t*)npts64.p);
+    k_pack<<<grid_for(M), kBlock, 0, st>>>(t->meta, (const int32_t*)nchild.p, M);
+    k_leaf_ids<<<gN, kBlock, 0, st>>>((const int32_t*)nn.p, (const int32_t*)base.p,
+                                      (const int8_t*)d0a.p, (const int8_t*)dla.p,
+                                      (const int32_t*)leafrank.p, n, t->leaf_ids);
+    CAGR_CUDA(cudaGetLastError());
+
+    // per-node point lists
+    CAGR_CUDA(cudaMemsetAsync((int64_t*)npts64.p + M, 0, sizeof(int64_t), st));
+    if (int rc = cub_call(
+            [&](void* tp, size_t& b) {
+                return cub::DeviceScan::ExclusiveSum(tp, b, (const int64_t*)npts64.p, t->n2p_start,
+                                                     M + 1, st);
+            },
+            st))
+        return rc;
+    int64_t L = 0;
+    CAGR_CUDA(cudaMemcpyAsync(&L, t->n2p_start + M, 8, cudaMemcpyDeviceToHost, st));
+    if (int rc = dev_alloc((void**)&t->invperm, sizeof(int32_t) * n)) return rc;
+    k_inv<<<gN, kBlock, 0, st>>>(t->perm, n, t->invperm);
+    Tmp cnt, off;
+    if (int rc = tmp_alloc(cnt, sizeof(int32_t) * n, st)) return rc;
+    if (int rc = tmp_alloc(off, sizeof(int64_t) * n, st)) return rc;
+    k_walk<false><<<gN, kBlock, 0, st>>>(t->invperm, sk, t->meta, t->children, D, n,
+                                         (int32_t*)cnt.p, nullptr, nullptr, nullptr);
+    if (int rc = cub_call(
+            [&](void* tp, size_t& b) {
+                return cub::DeviceScan::ExclusiveSum(tp, b, (const int32_t*)cnt.p,
+                                                     (int64_t*)off.p, n + 0, st);
+            },
+            st))
+        return rc;
+    CAGR_CUDA(cudaStreamSynchronize(st));
+    if (L <= 0 || L >= (int64_t(1) << 31) - 2)
+        return set_error(kErrOverflow, "point-list length out of range: " + std::to_string(L));
+    t->n2p_len = L;
+    Tmp pn, pp, pn2;
+    if (int rc = tmp_alloc(pn, sizeof(int32_t) * L, st)) return rc;
+    if (int rc = tmp_alloc(pp, sizeof(int32_t) * L, st)) return rc;
+    if (int rc = tmp_alloc(pn2, sizeof(int32_t) * L, st)) return rc;
+    if (int rc = dev_alloc((void**)&t->n2p, sizeof(int32_t) * L)) return rc;
+    k_walk<true><<<gN, kBlock, 0, st>>>(t->invperm, sk, t->meta, t->children, D, n, nullptr,
+                                        (const int64_t*)off.p, (int32_t*)pn.p, (int32_t*)pp.p);
+    CAGR_CUDA(cudaGetLastError());
+    const int node_bits = bit_width(M);
+    if (int rc = cub_call(
+            [&](void* tp, size_t& b) {
+                return cub::DeviceRadixSort::SortPairs(tp, b, (const uint32_t*)pn.p,
+                                                       (uint32_t*)pn2.p, (const int32_t*)pp.p,
+                                                       t->n2p, L, 0, node_bits, st);
+            },
+            st))
+        return rc;
+
+    // sorted positions
+    if (int rc = dev_alloc(&t->spos, sizeof(T) * 3 * n)) return rc;
+    k_spos<T><<<gN, kBlock, 0, st>>>(pts, t->perm, n, (T*)t->spos);
+    CAGR_CUDA(cudaGetLastError());
+
+    // tree depth = deepest node
+    int32_t maxd = 0;
+    {
+        Tmp dmax;
+        if (int rc = tmp_alloc(dmax, sizeof(int8_t), st)) return rc;
+        if (int rc = cub_call(
+                [&](void* tp, size_t& b) {
+                    return cub::DeviceReduce::Max(tp, b, (const int8_t*)dla.p, (int8_t*)dmax.p,
+                                                  n, st);
+                },
+                st))
+            return rc;
+        int8_t h = 0;
+        CAGR_CUDA(cudaMemcpyAsync(&h, dmax.p, 1, cudaMemcpyDeviceToHost, st));
+        CAGR_CUDA(cudaStreamSynchronize(st));
+        maxd = h;
+    }
+    t->depth = maxd;
+    return kOk;
+}
+
+}  // namespace
+
+void tree_free(Tree* t) {
+    if (!t) return;
+    cudaFree(t->perm);
+    cudaFree(t->invperm);
+    cudaFree(t->meta);
+    cudaFree(t->parent);
+    cudaFree(t->children);
+    cudaFree(t->leaf_ids);
+    cudaFree(t->n2p_start);
+    cudaFree(t->n2p);
+    cudaFree(t->spos);
+    cudaFree(t->counters);
+    for (int k = 0; k < 3; k++) cudaFree(t->rec[k]);
+    delete t;
+}
+
+int tree_build(const void* points, int64_t n, int dtype, int max_depth, int leaf_size,
+               cudaStream_t stream, Tree** out) {
+    *out = nullptr;
+    if (n <= 0) return set_error(kErrInvalid, "tree build needs at least one point");
+    if (n >= (int64_t(1) << 31) - 2) return set_error(kErrInvalid, "too many points");
+    if (max_depth < 0 || max_depth > CAGR_MAX_DEPTH)
+        return set_error(kErrInvalid, "max_depth must be in [0, 21]");
+    if (leaf_size < 1 || leaf_size > 4096)
+        return set_error(kErrInvalid, "leaf_size must be in [1, 4096]");
+    if (dtype != 0 && dtype != 1) return set_error(kErrInvalid, "dtype must be 0 (f32) or 1 (f64)");
+    if (!points) return set_error(kErrInvalid, "points is null");
+    Tree* t = new Tree();
+    t->dtype = dtype;
+    t->n = n;
+    t->max_depth = max_depth;
+    t->leaf_size = leaf_size;
+    cudaGetDevice(&t->device);
+    int rc = dtype == 0 ? build_impl<float>((const float*)points, n, max_depth, leaf_size, stream, t)
+                        : build_impl<double>((const double*)points, n, max_depth, leaf_size,
+                                             stream, t);
+    if (rc != kOk) {
+        cudaStreamSynchronize(stream);
+        tree_free(t);
+        return rc;
+    }
+    *out = t;
+    return kOk;
+}
+
+int tree_export(const Tree* t, int64_t* parent, int64_t* children, uint8_t* is_leaf,
+                void* half_w, int64_t* npts, int64_t* n2p, int64_t* n2p_start,
+                cudaStream_t stream) {
+    const int64_t M = t->m;
+    if (t->dtype == 0)
+        k_export<float><<<grid_for(M), kBlock, 0, stream>>>(t->meta, t->parent, t->children,
+                                                            t->n2p_start, M, parent, children,
+                                                            is_leaf, (float*)half_w, npts,
+                                                            n2p_start);
+    else
+        k_export<double><<<grid_for(M), kBlock, 0, stream>>>(t->meta, t->parent, t->children,
+                                                             t->n2p_start, M, parent, children,
+                                                             is_leaf, (double*)half_w, npts,
+                                                             n2p_start);
+    if (n2p) k_widen<<<grid_for(t->n2p_len), kBlock, 0, stream>>>(t->n2p, t->n2p_len, n2p);
+    CAGR_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+}  // namespace cagr

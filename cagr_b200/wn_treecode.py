@@ -1,0 +1,269 @@
+"""Drop-in for the reference's ``wn_treecode`` Python operator object.
+
+Mirrors ``WindingNumberTreecode`` of mayueji/CAGR
+(CUDA-based/ext/wn_treecode/wn_treecode_func.py:3-392): same constructor,
+same ``forward_*`` names, argument shapes, output shapes and assertion
+behaviour.  Every call goes through the C ABI of ``libcagr_b200.so``
+(include/cagr.h) on the tensors' own CUDA stream; torch is used only to own
+device memory.  Differences, all additive:
+
+* the octree is built on the GPU (the reference builds it on the CPU and
+  copies it over, wn_treecode_func.py:23-27) -- the seven reference-layout
+  tree tensors are still available as attributes, bit-identical;
+* ``forward_A2`` evaluates A21, A22 and A23 in one traversal ([N, 3]);
+* ``forward_A3`` (the GaussRecon field operator) and ``multiply`` evaluate at
+  arbitrary query points;
+* ``leaf_size`` is a constructor argument (the reference hard-codes 1).
+
+There is no CPU path: a CPU tensor raises, and so does a missing library.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import ATTR_DIM, OPS, OUT_DIM, check
+
+
+def _stream(device: torch.device) -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def _ptr(t: torch.Tensor | None) -> ctypes.c_void_p | None:
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+class WindingNumberTreecode:
+    """Treecode operators over a fixed point set (wn_treecode_func.py:3-43)."""
+
+    def __init__(self, points: torch.Tensor, max_tree_depth: int = 15, leaf_size: int = 1):
+        """points: [N, 3] CUDA tensor (float32 or float64)."""
+        assert len(points.shape) == 2
+        assert points.shape[1] == 3
+        if not points.is_cuda:
+            raise RuntimeError("WindingNumberTreecode (B200) needs a CUDA tensor; "
+                               "there is no CPU implementation")
+        if points.dtype not in (torch.float32, torch.float64):
+            raise RuntimeError(f"points must be float32 or float64, got {points.dtype}")
+        self.is_cuda = True
+        self.device = points.device
+        self.points = points.contiguous()
+        self.dtype = points.dtype
+        self.tree_depth = max_tree_depth
+        self.leaf_size = leaf_size
+        self._handle = None
+        L = _lib.lib()
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            rc = L.cagr_tree_build(
+                _ptr(self.points), self.points.shape[0],
+                _lib.CAGR_F64 if self.dtype == torch.float64 else _lib.CAGR_F32,
+                max_tree_depth, leaf_size, _stream(self.device), ctypes.byref(h))
+        check(rc, "cagr_tree_build")
+        self._handle = h
+        n, m, nl, d, ln = (ctypes.c_int64() for _ in range(5))
+        check(L.cagr_tree_info(h, ctypes.byref(n), ctypes.byref(m), ctypes.byref(nl),
+                               ctypes.byref(d), ctypes.byref(ln)), "cagr_tree_info")
+        self.num_nodes, self.num_leaves = m.value, nl.value
+        self.depth, self.n2p_len = d.value, ln.value
+        self._layout = None
+
+    # ---- lifetime -----------------------------------------------------------
+    def close(self) -> None:
+        if self._handle is not None and self._handle.value:
+            torch.cuda.synchronize(self.device)
+            _lib.lib().cagr_tree_destroy(self._handle)
+        self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        if self._handle is None:
+            raise RuntimeError("tree has been closed")
+        return self._handle
+
+    # ---- reference-layout tree tensors (wn_treecode_func.py:28-43) ------------
+    def _export_layout(self):
+        if self._layout is None:
+            M, Ln, dev = self.num_nodes, self.n2p_len, self.device
+            i64 = dict(dtype=torch.int64, device=dev)
+            parent = torch.empty(M, **i64)
+            children = torch.empty(M, 8, **i64)
+            is_leaf = torch.empty(M, dtype=torch.bool, device=dev)
+            half_w = torch.empty(M, dtype=self.dtype, device=dev)
+            npts = torch.empty(M, **i64)
+            n2p = torch.empty(Ln, **i64)
+            n2p_start = torch.empty(M, **i64)
+            with torch.cuda.device(dev):
+                check(_lib.lib().cagr_tree_export(
+                    self.handle, _ptr(parent), _ptr(children), _ptr(is_leaf), _ptr(half_w),
+                    _ptr(npts), _ptr(n2p), _ptr(n2p_start), _stream(dev)), "cagr_tree_export")
+            self._layout = (parent, children, is_leaf, half_w, npts, n2p, n2p_start)
+        return self._layout
+
+    node_parent_list = property(lambda self: self._export_layout()[0])
+    node_children_list = property(lambda self: self._export_layout()[1])
+    node_is_leaf_list = property(lambda self: self._export_layout()[2])
+    node_half_w_list = property(lambda self: self._export_layout()[3])
+    num_points_in_node = property(lambda self: self._export_layout()[4])
+    node2point_index = property(lambda self: self._export_layout()[5])
+    node2point_indexstart = property(lambda self: self._export_layout()[6])
+
+    def morton_order(self) -> torch.Tensor:
+        """Sorted position -> original point index (int32 [N])."""
+        perm = torch.empty(self.points.shape[0], dtype=torch.int32, device=self.device)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().cagr_tree_morton_order(self.handle, _ptr(perm), _stream(self.device)),
+                  "cagr_tree_morton_order")
+        return perm
+
+    # ---- generic calls --------------------------------------------------------
+    def _check_values(self, x: torch.Tensor, name: str) -> torch.Tensor:
+        if not x.is_cuda or x.device != self.device:
+            raise RuntimeError(f"{name} must be a CUDA tensor on {self.device}")
+        if x.dtype != self.dtype:
+            raise RuntimeError(f"{name} must have dtype {self.dtype}, got {x.dtype}")
+        return x.contiguous()
+
+    def _widths(self, widths, n: int):
+        """(tensor or None, scalar) for the C call."""
+        if isinstance(widths, (int, float)):
+            return None, float(widths)
+        assert len(widths.shape) == 1
+        assert widths.shape[0] == n
+        return self._check_values(widths, "widths"), 0.0
+
+    def scatter(self, values: torch.Tensor, slot: int = 0, weights: torch.Tensor | None = None):
+        """Node moments of per-point values ([N,1] or [N,3]) into a moment slot."""
+        values = self._check_values(values, "values")
+        w = None if weights is None else self._check_values(weights, "weights")
+        with torch.cuda.device(self.device):
+            check(_lib.lib().cagr_scatter(self.handle, slot, _ptr(values), values.shape[1],
+                                          _ptr(w), _stream(self.device)), "cagr_scatter")
+
+    def scatter_export(self, slot: int = 0, attr_dim: int = 3):
+        """Reference-layout node moments (node_attrs, node_reppoints, node_weights) of a slot,
+        as scatter_point_attrs_to_nodes returns them (wn_treecode_cuda_torch_interface.cu:133)."""
+        M, dev = self.num_nodes, self.device
+        a = torch.empty(M, attr_dim, dtype=self.dtype, device=dev)
+        r = torch.empty(M, 3, dtype=self.dtype, device=dev)
+        w = torch.empty(M, dtype=self.dtype, device=dev)
+        with torch.cuda.device(dev):
+            check(_lib.lib().cagr_scatter_export(self.handle, slot, _ptr(a), _ptr(r), _ptr(w),
+                                                 _stream(dev)), "cagr_scatter_export")
+        return [a, r, w]
+
+    def multiply(self, op: str, widths, queries: torch.Tensor | None = None,
+                 query_order: torch.Tensor | None = None, continuous: bool = False,
+                 out: torch.Tensor | None = None) -> torch.Tensor:
+        """Traversal with the moments currently in slot 0 (after ``scatter``)."""
+        n = self.points.shape[0] if queries is None else queries.shape[0]
+        if queries is not None:
+            assert len(queries.shape) == 2 and queries.shape[1] == 3
+            queries = self._check_values(queries, "queries")
+        if query_order is not None:
+            if query_order.dtype != torch.int32 or query_order.shape != (n,):
+                raise RuntimeError("query_order must be int32 [num_queries]")
+            query_order = query_order.contiguous()
+        wt, ws = self._widths(widths, n)
+        if out is None:
+            out = torch.empty(n, OUT_DIM[op], dtype=self.dtype, device=self.device)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().cagr_multiply(
+                self.handle, OPS[op], _ptr(queries), _ptr(query_order), n, _ptr(wt), ws,
+                int(continuous), _ptr(out), out.stride(0), _stream(self.device)),
+                f"cagr_multiply({op})")
+        return out
+
+    def _forward(self, op: str, values: torch.Tensor, widths, continuous: bool = False,
+                 queries: torch.Tensor | None = None) -> torch.Tensor:
+        values = self._check_values(values, "values")
+        assert values.shape[1] == ATTR_DIM[op]
+        self.scatter(values)
+        return self.multiply(op, widths, queries=queries, continuous=continuous)
+
+    # ---- the reference's forward_* (wn_treecode_func.py:45-392) ----------------
+    def _assert_normals(self, normals, widths):
+        assert self.points.shape == normals.shape
+        if not isinstance(widths, (int, float)):
+            assert len(widths.shape) == 1
+            assert self.points.shape[0] == widths.shape[0]
+
+    def _assert_values(self, values, widths):
+        assert len(values.shape) == 2
+        assert values.shape[0] == self.points.shape[0]
+        assert values.shape[1] == 1
+        if not isinstance(widths, (int, float)):
+            assert len(widths.shape) == 1
+            assert self.points.shape[0] == widths.shape[0]
+
+    def forward_A(self, normals, widths):
+        """normals: [N, 3], widths: [N,] -> [N, 1] (wn_treecode_func.py:45-79)."""
+        self._assert_normals(normals, widths)
+        return self._forward("A", normals, widths)
+
+    def forward_AT(self, values, widths):
+        """values: [N, 1], widths: [N,] -> [N, 3] (wn_treecode_func.py:81-120)."""
+        self._assert_values(values, widths)
+        return self._forward("AT", values, widths)
+
+    def forward_A21(self, normals, widths):
+        self._assert_normals(normals, widths)
+        return self._forward("A21", normals, widths)
+
+    def forward_A22(self, normals, widths):
+        self._assert_normals(normals, widths)
+        return self._forward("A22", normals, widths)
+
+    def forward_A23(self, normals, widths):
+        self._assert_normals(normals, widths)
+        return self._forward("A23", normals, widths)
+
+    def forward_A2T1(self, values, widths):
+        self._assert_values(values, widths)
+        return self._forward("A2T1", values, widths)
+
+    def forward_A2T2(self, values, widths):
+        self._assert_values(values, widths)
+        return self._forward("A2T2", values, widths)
+
+    def forward_A2T3(self, values, widths):
+        self._assert_values(values, widths)
+        return self._forward("A2T3", values, widths)
+
+    def forward_G(self, normals, widths):
+        """normals: [N, 3] -> [N, 3] (wn_treecode_func.py:353-392)."""
+        self._assert_normals(normals, widths)
+        return self._forward("G", normals, widths)
+
+    # ---- additions ---------------------------------------------------------------
+    def forward_A2(self, normals, widths, continuous: bool = False):
+        """[A21 | A22 | A23](normals) -> [N, 3], one traversal."""
+        self._assert_normals(normals, widths)
+        return self._forward("A2_FUSED", normals, widths, continuous)
+
+    def forward_A3(self, normals, widths, queries: torch.Tensor | None = None,
+                   continuous: bool = True):
+        """(A21 + A22 + A23) / 3 at `queries` (default: the points) -> [N', 1]; the
+        field operator of the GaussRecon driver (main_GaussRecon_cuda.cu:427-466),
+        which uses the continuous kernel."""
+        assert self.points.shape == normals.shape
+        return self._forward("A3", normals, widths, continuous, queries)
+
+    def forward_A2T_sum(self, values3, widths):
+        """sum_k A2Tk(values3[:, k]) -> [N, 3]: the reference composition
+        A2T1(s1) + A2T2(s2) + A2T3(s3) (main_CAGR.py:110), three traversals with
+        each direction's own node moments."""
+        assert len(values3.shape) == 2 and values3.shape[1] == 3
+        out = None
+        for k, op in enumerate(("A2T1", "A2T2", "A2T3")):
+            y = self._forward(op, values3[:, k:k + 1].contiguous(), widths)
+            out = y if out is None else out.add_(y)
+        return out

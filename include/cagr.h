@@ -1,0 +1,145 @@
+/*
+ * cagr.h -- C ABI of the B200 treecode library (libcagr_b200.so).
+ *
+ * Drop-in boundary for the hot path of mayueji/CAGR: the Barnes-Hut treecode
+ * evaluation of the convection-augmented Gauss operator A.mu and its
+ * transpose-form A^T.w.  Every pointer argument named *_dev is a device
+ * pointer on the current CUDA device; `stream` is a cudaStream_t (NULL = the
+ * legacy default stream).  No entry point synchronises the stream unless it
+ * says so.  Outputs are caller-owned; the tree handle owns its own device
+ * memory.  Every function returns a cagr_status; on failure
+ * cagr_last_error() gives a message (thread-local).
+ *
+ * Reference interfaces replaced (paths inside mayueji/CAGR):
+ *   build_tree ............ CUDA-based/ext/wn_treecode/wn_treecode_cpu/
+ *                           wn_treecode_cpu_torch_interface.cpp:104-118 (-> :42-102)
+ *   scatter_point_attrs_to_nodes
+ *                           CUDA-based/ext/wn_treecode/wn_treecode_cuda/
+ *                           wn_treecode_cuda_torch_interface.cu:41-134
+ *   multiply_by_{A,AT,A3,A21,A22,A23,A2T1,A2T2,A2T3,G}
+ *                           wn_treecode_cuda_torch_interface.cu:137-777
+ *                           (pybind names at :779-793)
+ *   WindingNumberTreecode.forward_*
+ *                           CUDA-based/ext/wn_treecode/wn_treecode_func.py:45-392
+ */
+#ifndef CAGR_H
+#define CAGR_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cagr_tree cagr_tree;
+
+/* Status codes. */
+enum {
+    CAGR_OK = 0,
+    CAGR_ERR_INVALID = 1,  /* bad argument (null pointer, size, dtype, op) */
+    CAGR_ERR_CUDA = 2,     /* a CUDA call or kernel launch failed */
+    CAGR_ERR_ALLOC = 3,    /* device allocation failed */
+    CAGR_ERR_OVERFLOW = 4, /* a size exceeds the 32-bit index range of the tree */
+    CAGR_ERR_STATE = 5     /* call order: e.g. multiply before scatter */
+};
+
+/* Element types (the reference dispatches float and double,
+ * AT_DISPATCH_FLOATING_TYPES in wn_treecode_cuda_torch_interface.cu). */
+enum { CAGR_F32 = 0, CAGR_F64 = 1 };
+
+/* Operators.  Reference kernels in wn_treecode_cuda_kernels.cu:
+ *   A    :556-621   [N',1]   sum d.mu / r^3 (CUDA sign)
+ *   AT   :623-692   [N',3]   sum d s / r^3
+ *   A3   :694-763   [N',1]   (A21 + A22 + A23) / 3
+ *   A21..A23 :843-1042 [N',1] sum exp(d_k/2) (d.mu / r^3 + mu_k / (2r))
+ *   A2T1..A2T3 :1046-1257 [N',3] sum exp(d_k/2) (d s / r^3 + e_k s / (2r))
+ *   G    :1259-1322 [N',3]   sum mu / r^3 - 3 d (d.mu) / r^5
+ * A2_FUSED has no reference counterpart: A21, A22, A23 from one traversal,
+ * written as the three columns of an [N',3] output. */
+enum {
+    CAGR_OP_A = 0,
+    CAGR_OP_AT = 1,
+    CAGR_OP_A3 = 2,
+    CAGR_OP_A21 = 3,
+    CAGR_OP_A22 = 4,
+    CAGR_OP_A23 = 5,
+    CAGR_OP_A2T1 = 6,
+    CAGR_OP_A2T2 = 7,
+    CAGR_OP_A2T3 = 8,
+    CAGR_OP_G = 9,
+    CAGR_OP_A2_FUSED = 10
+};
+
+/* Library identification. */
+int cagr_version(void);
+const char* cagr_status_string(int status);
+const char* cagr_last_error(void);
+
+/* Builds the octree of `n` points (points_dev: [n,3], dtype) on the device.
+ * Same tree as the reference build_tree (root centre 0, half-width 1, octant
+ * code x>=cx | y>=cy<<1 | z>=cz<<2, leaf at max_depth or <= leaf_size points,
+ * preorder node ids); the reference hard-codes leaf_size 1
+ * (wn_treecode_cpu_torch_interface.cpp:60) and callers pass max_depth 15.
+ * Replaces build_tree, wn_treecode_cpu_torch_interface.cpp:104-118.
+ * Synchronises `stream` (node counts are needed on the host). */
+int cagr_tree_build(const void* points_dev, int64_t n, int dtype, int max_depth, int leaf_size,
+                    void* stream, cagr_tree** out_tree);
+
+/* Frees the tree and all its device memory (after the device is idle for it). */
+int cagr_tree_destroy(cagr_tree* tree);
+
+/* Sizes of a built tree.  Any output pointer may be NULL. */
+int cagr_tree_info(const cagr_tree* tree, int64_t* num_points, int64_t* num_nodes,
+                   int64_t* num_leaves, int64_t* depth, int64_t* n2p_len);
+
+/* Writes the tree in the reference layout (build_tree's seven tensors,
+ * wn_treecode_cpu_torch_interface.cpp:73-101): parent[M] i64 (-1 root),
+ * children[M,8] i64 (-1 none), is_leaf[M] u8, half_w[M] (tree dtype),
+ * npts[M] i64, n2p[L] i64, n2p_start[M] i64.  Any output may be NULL. */
+int cagr_tree_export(const cagr_tree* tree, int64_t* parent_dev, int64_t* children_dev,
+                     uint8_t* is_leaf_dev, void* half_w_dev, int64_t* npts_dev, int64_t* n2p_dev,
+                     int64_t* n2p_start_dev, void* stream);
+
+/* Copies the Morton order (sorted position -> original index, int32[n]). */
+int cagr_tree_morton_order(const cagr_tree* tree, int32_t* perm_dev, void* stream);
+
+/* Node moments of per-point attributes (attrs_dev: [n, attr_dim], attr_dim 1
+ * or 3, original point order) into moment slot `slot` (0..2) of the tree:
+ * node attribute sums, weights (sum of weights_dev, or of |attr| when
+ * weights_dev is NULL, as wn_treecode_func.py:131 computes them) and weighted
+ * centroids.  Replaces scatter_point_attrs_to_nodes,
+ * wn_treecode_cuda_torch_interface.cu:41-134; results are bit-identical to
+ * the reference kernels :419-553 evaluated in IEEE arithmetic. */
+int cagr_scatter(cagr_tree* tree, int slot, const void* attrs_dev, int attr_dim,
+                 const void* weights_dev, void* stream);
+
+/* Copies slot `slot` out in the reference layout: node_attrs [M, attr_dim],
+ * reppoints [M,3], node_weights [M] (any may be NULL). */
+int cagr_scatter_export(const cagr_tree* tree, int slot, void* node_attrs_dev,
+                        void* reppoints_dev, void* node_weights_dev, void* stream);
+
+/* Evaluates operator `op` with the moments in slot 0 (attr_dim 3 for
+ * A/A3/A2x/G/A2_FUSED, 1 for AT/A2Tx).  Queries: queries_dev [nq,3], or NULL
+ * for the tree's own points (then nq is ignored and outputs follow the
+ * original point order).  query_order_dev (int32[nq], optional) gives the
+ * order in which queries are processed (Morton order is fastest); outputs
+ * always land at the query's own row.  Width per query: widths_dev [nq] or,
+ * when NULL, the scalar `width`.  continuous: the reference's continuous
+ * kernel flag (A, A3, A2x).  out_dev: [nq, out_stride] with out_stride 0 =
+ * the operator's output width.  Replaces multiply_by_*,
+ * wn_treecode_cuda_torch_interface.cu:137-777. */
+int cagr_multiply(const cagr_tree* tree, int op, const void* queries_dev,
+                  const int32_t* query_order_dev, int64_t nq, const void* widths_dev,
+                  double width, int continuous, void* out_dev, int64_t out_stride, void* stream);
+
+/* One WindingNumberTreecode.forward_* call (wn_treecode_func.py:45-392):
+ * node moments of values_dev ([n,3] for A/A3/A2x/G/A2_FUSED, [n,1] for
+ * AT/A2Tx) into slot 0, then `op` at the tree's own points. */
+int cagr_forward(cagr_tree* tree, int op, const void* values_dev, const void* widths_dev,
+                 double width, int continuous, void* out_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CAGR_H */

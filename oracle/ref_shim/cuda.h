@@ -1,0 +1,1 @@
+/* Empty stand-in used when the reference CUDA kernel file is compiled as host C++ (oracle/Makefile). */

@@ -1,0 +1,176 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+Integer/index work (the octree) must be bit-exact; node moments are computed
+in the reference's operation order and must be bit-exact too; operator
+values are floating point and must agree within the stated tolerances
+(FP32: relative L2 <= 2e-5 and max error <= 2e-4 of max |ref|, set by
+rsqrt/exp rounding and a different summation order over identical pair
+sets; FP64: 1e-12 / 1e-11).
+"""
+import numpy as np
+import pytest
+
+from tests._cases import edge_cloud, random_values, rel_errors, smooth_normals, sphere_cloud
+
+pytestmark = pytest.mark.gpu
+
+TOL = {np.float32: (2e-5, 2e-4), np.float64: (1e-12, 1e-11)}
+VALUE_OPS = ["AT", "A2T1", "A2T2", "A2T3"]
+NORMAL_OPS = ["A", "A3", "A21", "A22", "A23", "G"]
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _tree(points, max_depth=15, leaf_size=1):
+    torch = _torch()
+    from cagr_b200 import WindingNumberTreecode
+    return WindingNumberTreecode(torch.from_numpy(points).cuda(), max_tree_depth=max_depth,
+                                 leaf_size=leaf_size)
+
+
+TREE_CASES = [
+    ("sphere3000", lambda: sphere_cloud(3000), 15, 1),
+    ("edge", lambda: edge_cloud(), 15, 1),
+    ("sphere_f64", lambda: sphere_cloud(2500, seed=5, dtype=np.float64), 15, 1),
+    ("leaf16_depth8", lambda: sphere_cloud(5000, seed=6), 8, 16),
+    ("leaf4_depth6_edge", lambda: edge_cloud(seed=7), 6, 4),
+    ("depth0", lambda: sphere_cloud(50, seed=8), 0, 1),
+    ("one_point", lambda: sphere_cloud(1, seed=9), 15, 1),
+    ("all_duplicates", lambda: np.repeat(sphere_cloud(3, seed=10), 40, axis=0), 15, 1),
+    ("depth21", lambda: edge_cloud(seed=11), 21, 1),
+]
+
+
+@pytest.mark.parametrize("name,make,max_depth,leaf_size", TREE_CASES, ids=[c[0] for c in TREE_CASES])
+def test_tree_bit_exact(cuda_lib, oracle, name, make, max_depth, leaf_size):
+    pts = make()
+    tr = oracle.build_tree(pts, max_depth=max_depth, leaf_size=leaf_size)
+    wn = _tree(pts, max_depth, leaf_size)
+    got = [t.cpu().numpy() for t in (wn.node_parent_list, wn.node_children_list,
+                                     wn.node_is_leaf_list, wn.node_half_w_list,
+                                     wn.num_points_in_node, wn.node2point_index,
+                                     wn.node2point_indexstart)]
+    names = ["parent", "children", "is_leaf", "half_w", "npts", "n2p", "n2p_start"]
+    for g, r, nm in zip(got, tr.as_tuple(), names):
+        assert g.shape == r.shape, (nm, g.shape, r.shape)
+        assert g.dtype == r.dtype, (nm, g.dtype, r.dtype)
+        assert np.array_equal(g, r), nm
+    assert wn.depth == tr.depth
+    assert wn.num_leaves == tr.num_leaves
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("dim", [3, 1])
+def test_moments_bit_exact(cuda_lib, oracle, dtype, dim):
+    torch = _torch()
+    from oracle.oracle import point_weights
+    pts = edge_cloud(dtype=dtype)
+    wn = _tree(pts)
+    tr = oracle.build_tree(pts)
+    vals = smooth_normals(pts, zero_frac=0.2) if dim == 3 else random_values(len(pts), 1, dtype=dtype)
+    if dim == 1:
+        vals[::7] = 0
+    mom = oracle.moments(tr, pts, point_weights(vals), vals)
+    wn.scatter(torch.from_numpy(vals).cuda())
+    a, r, w = (t.cpu().numpy() for t in wn.scatter_export(0, dim))
+    assert np.array_equal(w, mom.weights)
+    assert np.array_equal(r, mom.rep)
+    assert np.array_equal(a, mom.attrs)
+
+
+def _ref_op(oracle, op, pts, vals, widths, queries=None, cont=False):
+    tr = oracle.build_tree(pts)
+    return oracle.forward(op, tr, pts, vals, widths, queries=queries, continuous=cont)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("op", NORMAL_OPS + VALUE_OPS)
+def test_operator_parity(cuda_lib, oracle, op, dtype):
+    torch = _torch()
+    pts = sphere_cloud(4000, seed=12, dtype=dtype)
+    rng = np.random.default_rng(13)
+    widths = rng.uniform(0.005, 0.03, size=len(pts)).astype(dtype)
+    if op in VALUE_OPS:
+        vals = random_values(len(pts), 1, seed=14, dtype=dtype)
+    else:
+        vals = smooth_normals(pts, seed=15)
+    ref = _ref_op(oracle, op, pts, vals, widths)
+    wn = _tree(pts)
+    fn = getattr(wn, f"forward_{op}")
+    got = fn(torch.from_numpy(vals).cuda(), torch.from_numpy(widths).cuda()).cpu().numpy()
+    assert got.shape == ref.shape
+    l2, mx = rel_errors(got, ref)
+    tl2, tmx = TOL[dtype]
+    assert l2 <= tl2 and mx <= tmx, (op, l2, mx)
+
+
+@pytest.mark.parametrize("op", ["A", "A3", "A21", "A22", "A23"])
+def test_continuous_kernel_at_queries(cuda_lib, oracle, op):
+    """Continuous kernel at external query points (the GaussRecon field
+    evaluation shape: grid corners + the samples themselves)."""
+    torch = _torch()
+    pts = sphere_cloud(3000, seed=16)
+    vals = smooth_normals(pts, seed=17)
+    rng = np.random.default_rng(18)
+    q = np.concatenate([rng.uniform(-1.0, 1.0, size=(3000, 3)), pts[:500]]).astype(np.float32)
+    w = np.full(len(q), 0.02, np.float32)
+    ref = _ref_op(oracle, op, pts, vals, w, queries=q, cont=True)
+    wn = _tree(pts)
+    wn.scatter(torch.from_numpy(vals).cuda())
+    got = wn.multiply(op, torch.from_numpy(w).cuda(), queries=torch.from_numpy(q).cuda(),
+                      continuous=True).cpu().numpy()
+    l2, mx = rel_errors(got, ref)
+    assert l2 <= 2e-5 and mx <= 2e-4, (op, l2, mx)
+
+
+def test_fused_forward_matches_single_direction(cuda_lib):
+    torch = _torch()
+    pts = sphere_cloud(5000, seed=19)
+    vals = torch.from_numpy(smooth_normals(pts, seed=20)).cuda()
+    wn = _tree(pts)
+    fused = wn.forward_A2(vals, 0.01)
+    for k, op in enumerate(("A21", "A22", "A23")):
+        single = getattr(wn, f"forward_{op}")(vals, 0.01)
+        assert torch.equal(fused[:, k:k + 1], single), op
+
+
+def test_scalar_width_equals_width_tensor(cuda_lib):
+    torch = _torch()
+    pts = sphere_cloud(3000, seed=21)
+    vals = torch.from_numpy(smooth_normals(pts, seed=22)).cuda()
+    wn = _tree(pts)
+    a = wn.forward_A21(vals, 0.015)
+    b = wn.forward_A21(vals, torch.full((len(pts),), 0.015, device="cuda"))
+    assert torch.equal(a, b)
+
+
+def test_a2t_sum_matches_reference_composition(cuda_lib, oracle):
+    torch = _torch()
+    pts = sphere_cloud(3000, seed=23)
+    s = random_values(len(pts), 3, seed=24)
+    w = np.full(len(pts), 0.01, np.float32)
+    tr = oracle.build_tree(pts)
+    ref = sum(oracle.forward(op, tr, pts, s[:, k:k + 1], w)
+              for k, op in enumerate(("A2T1", "A2T2", "A2T3")))
+    wn = _tree(pts)
+    got = wn.forward_A2T_sum(torch.from_numpy(s).cuda(), 0.01).cpu().numpy()
+    l2, mx = rel_errors(got, ref)
+    assert l2 <= 2e-5 and mx <= 2e-4, (l2, mx)
+
+
+def test_errors_are_raised(cuda_lib):
+    torch = _torch()
+    from cagr_b200 import WindingNumberTreecode
+    from cagr_b200._lib import CagrError
+    with pytest.raises(RuntimeError):
+        WindingNumberTreecode(torch.zeros(10, 3))  # CPU tensor: no CPU path
+    with pytest.raises(CagrError):
+        WindingNumberTreecode(torch.zeros(10, 3, device="cuda"), max_tree_depth=40)
+    wn = _tree(sphere_cloud(100))
+    with pytest.raises(CagrError):
+        wn.multiply("A21", 0.01)  # no moments computed yet
+    with pytest.raises(AssertionError):
+        wn.forward_A21(torch.zeros(99, 3, device="cuda"), 0.01)
