@@ -1,0 +1,428 @@
+#!/usr/bin/env python
+"""Benchmark of the CAGR treecode hot path on B200.
+
+One step = one convection-augmented Gauss operator pair at 1M points, as the
+CAGR normal solve applies it (main_CAGR.py:107-116):
+  A.mu   -- node moments of mu + A21/A22/A23 in one fused traversal
+  A^T.w  -- sum_k A2Tk(w_k): for each k node moments of w_k + one traversal
+            (the reference's three calls with their own node moments)
+Workload: 1,000,000 points on the union of 8 seeded primitives (normalised as
+main_CAGR.py does), octree leaf 1 / depth 15 (the reference defaults), per-point
+width 1.5 x the mean distance to the 10 nearest neighbours.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  For N > 1 (torchrun) every rank runs an
+independent replica (the operator does not shard on one GPU's worth of work;
+see DESIGN.md) and times are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "treecode A·μ+Aᵀ·w ms and end-to-end s @1M pts, FP32/adjoint vs FP64 form"
+UNIT = "ms"
+# FP32 work per pair term, counted from the kernel source (cagr_b200/csrc/traverse.cu,
+# pair_term; an FMA counts 2): d (3) + |d|^2 without contraction (5) + r^-3 (2)
+# + d.mu (5) + d.mu r^-3 (1) + r^-1/2 (1), then per direction 2 FMA (4):
+FLOPS_A2_FUSED = 29      # three directions
+FLOPS_A2T = 22           # d (3) + |d|^2 (5) + r^-3 (2) + e s r^-3 (2) + 3 FMA (6) + e s r^-1/2 (3) + add (1)
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="union8")
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="queries per operator timed on the CPU (0 = auto)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- workload ----
+
+def knn_widths(p: np.ndarray, k: int = 10, scale: float = 1.5) -> np.ndarray:
+    from scipy.spatial import cKDTree
+    d, _ = cKDTree(p).query(p, k=k + 1, workers=-1)
+    return (scale * d[:, 1:].mean(1)).astype(p.dtype)
+
+
+def make_workload(name: str, n: int, seed: int = 2):
+    from cagr_b200 import synthetic as S
+    raw = S.make(name, n, seed)
+    p = S.normalize(raw).astype(np.float32)
+    widths = knn_widths(p)
+    # mu: area-weighted outward normals of the cloud (the magnitude CAGR's mu has)
+    c = p.astype(np.float64) - p.mean(0)
+    mu = (c / np.maximum(np.linalg.norm(c, axis=1, keepdims=True), 1e-12) * (4.0 / n))
+    return p, widths, mu.astype(np.float32)
+
+
+def workload_config(args, width_mean: float) -> dict:
+    return {
+        "workload": (f"{args.workload}: {args.n:,} points on the union of 8 seeded primitives "
+                     "(seed 2, noise 1e-3), normalised as main_CAGR.py; octree leaf 1, depth 15; "
+                     "per-point width 1.5x mean 10-NN distance"),
+        "points": args.n,
+        "step": ("A.mu (moments of mu + one A21/A22/A23 traversal) + A^T.w (moments of w_1, "
+                 "w_2, w_3 + one traversal summing A2T1(w_1) + A2T2(w_2) + A2T3(w_3), each "
+                 "direction with its own moments and acceptance decisions)"),
+        "width_mean": round(width_mean, 6),
+        "l2": "flushed between timed steps (256 MiB write)",
+        "parallelism": "replicas" if args.gpus > 1 else "single",
+    }
+
+
+# ------------------------------------------------------------------ clocks ----
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "20"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------- CPU legs -------
+
+def cpu_reference_step_ms(p, widths, mu, wvals, sample: int, threads: int):
+    """The reference's own CPU-side algorithm for one step on a bounded sample:
+    the reference CUDA kernels compiled for the host (oracle/_ref) when present,
+    else the C restatement.  Per A21/A22/A23/A2T1/A2T2/A2T3 call: |value|
+    weights, full node moments, traversal of `sample` queries; traversal time
+    is scaled to all queries.  Returns (ms per full step, kind, description)."""
+    from oracle.oracle import Oracle, RefOracle, point_weights
+    try:
+        impl, kind = RefOracle(), "reference"
+    except (FileNotFoundError, OSError):
+        impl, kind = Oracle(), "port"
+    n = p.shape[0]
+    tree = impl.build_tree(p)
+    rng = np.random.default_rng(7)
+    sel = np.sort(rng.choice(n, size=min(sample, n), replace=False))
+    q, wq = p[sel], widths[sel]
+    t_scatter = t_trav = 0.0
+    for op, vals in (("A21", mu), ("A22", mu), ("A23", mu), ("A2T1", wvals[:, 0:1]),
+                     ("A2T2", wvals[:, 1:2]), ("A2T3", wvals[:, 2:3])):
+        vals = np.ascontiguousarray(vals)
+        t0 = time.perf_counter()
+        mom = impl.moments(tree, p, point_weights(vals), vals)
+        t1 = time.perf_counter()
+        impl.multiply(op, q, wq, p, vals, tree, mom)
+        t2 = time.perf_counter()
+        t_scatter += t1 - t0
+        t_trav += t2 - t1
+    ms = (t_scatter + t_trav * (n / len(sel))) * 1e3
+    desc = (f"{len(sel):,} of {n:,} queries per operator (traversal time scaled by "
+            f"{n / len(sel):.1f}); node moments over all {tree.num_nodes:,} nodes; 6 operator "
+            f"calls (A21, A22, A23, A2T1, A2T2, A2T3) as main_CAGR.py makes them; "
+            f"{threads} OpenMP threads")
+    return ms, kind, desc
+
+
+def run_reference_arm(args, rank: int):
+    if rank != 0:
+        return
+    import multiprocessing
+    threads = multiprocessing.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    p, widths, mu = make_workload(args.workload, args.n)
+    rng = np.random.default_rng(5)
+    wvals = rng.normal(size=(args.n, 3)).astype(np.float32) * 1e-3
+    sample = args.cpu_sample or 100_000
+    times = []
+    kind = desc = None
+    for i in range(args.warmup + args.steps):
+        ms, kind, desc = cpu_reference_step_ms(p, widths, mu, wvals, sample, threads)
+        if i >= args.warmup:
+            times.append(ms)
+    v = float(np.mean(times))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(v, 3), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(args, float(widths.mean())),
+        "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": desc},
+        "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm ---
+
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+
+    from cagr_b200 import WindingNumberTreecode, _lib
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    p, widths, mu = make_workload(args.workload, args.n)
+    P = torch.from_numpy(p).to(dev)
+    W = torch.from_numpy(widths).to(dev)
+    MU = torch.from_numpy(mu).to(dev)
+    wn = WindingNumberTreecode(P)
+    # adjoint input: the forward result, as the solve feeds A2k(mu) back (main_CAGR.py:107-110)
+    WV = (-wn.forward_A2(MU, W)).contiguous()
+    out_a = torch.empty(args.n, 3, device=dev)
+    out_t = torch.empty(args.n, 3, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, device=dev)
+    wcols = [WV[:, k:k + 1].contiguous() for k in range(3)]
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def step(marks=None):
+        # A.mu: moments of mu, then A21/A22/A23 in one traversal
+        if marks is not None:
+            marks[0].record(stream)
+        wn.scatter(MU)
+        if marks is not None:
+            marks[1].record(stream)
+        wn.multiply("A2_FUSED", W, out=out_a)
+        if marks is not None:
+            marks[2].record(stream)
+        # A^T.w: moments of w_1, w_2, w_3 (one launch), then sum_k A2Tk(w_k) in one traversal
+        wn.scatter3(WV)
+        if marks is not None:
+            marks[3].record(stream)
+        wn.multiply("A2T_SUM", W, out=out_t)
+        if marks is not None:
+            marks[4].record(stream)
+
+    launches_per_step = 4
+
+    # pair-term counts of every traversal in a step (algorithmic work): each
+    # direction of the adjoint counted with its own moments
+    wn.scatter(MU)
+    terms_a2 = float(wn.multiply("COUNT", W).sum().item())
+    terms_t = []
+    for k in range(3):
+        wn.scatter(wcols[k])
+        terms_t.append(float(wn.multiply("COUNT", W).sum().item()))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    step_ms, a2_ms, a2t_ms, mom_ms = [], [], [], []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        marks = [ev() for _ in range(5)]
+        step(marks)
+        torch.cuda.synchronize(dev)
+        step_ms.append(marks[0].elapsed_time(marks[4]))
+        mom_ms.append(marks[0].elapsed_time(marks[1]) + marks[2].elapsed_time(marks[3]))
+        a2_ms.append(marks[1].elapsed_time(marks[2]))
+        a2t_ms.append(marks[3].elapsed_time(marks[4]))
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+
+    # end to end through the public API with host buffers
+    h_mu = torch.from_numpy(mu).pin_memory()
+    h_w = WV.cpu().pin_memory()
+    h_oa = torch.empty(args.n, 3).pin_memory()
+    h_ot = torch.empty(args.n, 3).pin_memory()
+    d_mu = torch.empty_like(MU)
+    d_w = torch.empty_like(WV)
+
+    def e2e_step():
+        d_mu.copy_(h_mu, non_blocking=True)
+        d_w.copy_(h_w, non_blocking=True)
+        oa = wn.forward_A2(d_mu, W)
+        ot = wn.forward_A2T_sum(d_w, W)
+        h_oa.copy_(oa, non_blocking=True)
+        h_ot.copy_(ot, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    e2e_ms = []
+    for _ in range(max(3, args.steps // 2)):
+        flush.fill_(1.0)
+        a, b = ev(), ev()
+        a.record(stream)
+        e2e_step()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        e2e_ms.append(a.elapsed_time(b))
+
+    # FP64 form of the same step (the plain FP64-accumulate comparison)
+    fp64_ms = None
+    if not args.no_fp64:
+        wn64 = WindingNumberTreecode(P.double())
+        W64, MU64, WV64 = W.double(), MU.double(), WV.double()
+        for _ in range(2):
+            wn64.forward_A2(MU64, W64)
+            wn64.forward_A2T_sum(WV64, W64)
+        torch.cuda.synchronize(dev)
+        t = []
+        for _ in range(3):
+            flush.fill_(1.0)
+            a, b = ev(), ev()
+            a.record(stream)
+            wn64.forward_A2(MU64, W64)
+            wn64.forward_A2T_sum(WV64, W64)
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            t.append(a.elapsed_time(b))
+        fp64_ms = float(np.mean(t))
+        wn64.close()
+
+    # measured FP32 FMA peak (roofline denominator)
+    gf = ctypes.c_double()
+    _lib.check(_lib.lib().cagr_probe_fp32_peak(20000, ctypes.byref(gf),
+                                               ctypes.c_void_p(stream.cuda_stream)),
+               "cagr_probe_fp32_peak")
+    peak_tflops = gf.value / 1e3
+
+    T = float(np.mean(step_ms))
+    E = float(np.mean(e2e_ms))
+    if world > 1:
+        t = torch.tensor([T, E], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        T, E = float(t[0]), float(t[1])
+    if rank != 0:
+        return
+
+    # dominant kernel: the traversal with the most time per step
+    a2_avg = float(np.mean(a2_ms))
+    a2t_avg = float(np.mean(a2t_ms))
+    if a2t_avg >= a2_avg:
+        dom, dur = "k_traverse_a2t<3 slots> (A2T_SUM)", a2t_avg
+        terms_dom, fpt = float(sum(terms_t)), FLOPS_A2T
+    else:
+        dom, dur = "k_traverse<A2_FUSED>", a2_avg
+        terms_dom, fpt = terms_a2, FLOPS_A2_FUSED
+    achieved = terms_dom * fpt / (dur * 1e-3) / 1e12
+    cpu = None
+    if not args.no_cpu_baseline:
+        import multiprocessing
+        threads = multiprocessing.cpu_count()
+        rng = np.random.default_rng(5)
+        wv_host = WV.cpu().numpy()
+        ms, kind, desc = cpu_reference_step_ms(p, widths, mu, wv_host,
+                                               args.cpu_sample or 200_000, threads)
+        cpu = {"value": round(ms, 3), "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": desc}
+        del rng
+    bi = (MU.numel() + WV.numel()) * 4
+    bo = (out_a.numel() + out_t.numel()) * 4
+    line = {
+        "metric": METRIC, "value": round(T / world, 4), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(T, 4),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": workload_config(args, float(widths.mean())),
+        "e2e": {"value": round(E / world, 4), "unit": UNIT, "h2d_bytes_per_step": bi,
+                "d2h_bytes_per_step": bo},
+        "gpu_launches": launches_per_step * args.steps,
+        "roofline": {"bound": "fp32", "kernel": dom, "achieved": round(achieved, 3),
+                     "peak": round(peak_tflops, 3), "unit": "TFLOP/s",
+                     "frac": round(achieved / peak_tflops, 4), "traffic": None,
+                     "peak_source": "measured FP32 FMA probe (cagr_probe_fp32_peak)",
+                     "pair_terms_per_launch": round(terms_dom), "flops_per_term": fpt},
+        "kernels_ms": {"moments_per_step": round(float(np.mean(mom_ms)), 4),
+                       "A2_FUSED": round(a2_avg, 4), "A2T_SUM": round(a2t_avg, 4)},
+        "pair_terms": {"A2_FUSED": round(terms_a2), "A2T1": round(terms_t[0]),
+                       "A2T2": round(terms_t[1]), "A2T3": round(terms_t[2])},
+        "fp64_ms_per_step": None if fp64_ms is None else round(fp64_ms, 3),
+        "clocks": clk,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -45,6 +45,9 @@ int op_attr_dim(int op) {
         case CAGR_OP_A23:
         case CAGR_OP_G:
         case CAGR_OP_A2_FUSED: return 3;
+        case CAGR_OP_A2T_SUM: return 3;         // three scalar columns, one per slot
+        case CAGR_OP_A2T_SUM_SHARED: return 1;  // one scalar column shared by the three
+        case CAGR_OP_COUNT: return -1;  // any: counts with whatever slot 0 holds
         default: return 0;
     }
 }
@@ -122,6 +125,11 @@ int cagr_scatter(cagr_tree* tree, int slot, const void* attrs_dev, int attr_dim,
     return cagr::moments(tree->t, slot, attrs_dev, attr_dim, weights_dev, as_stream(stream));
 }
 
+int cagr_scatter3(cagr_tree* tree, const void* values3_dev, void* stream) {
+    if (int rc = check_tree(tree)) return rc;
+    return cagr::moments3(tree->t, values3_dev, as_stream(stream));
+}
+
 int cagr_scatter_export(const cagr_tree* tree, int slot, void* node_attrs_dev,
                         void* reppoints_dev, void* node_weights_dev, void* stream) {
     if (int rc = check_tree(tree)) return rc;
@@ -131,14 +139,21 @@ int cagr_scatter_export(const cagr_tree* tree, int slot, void* node_attrs_dev,
 
 int cagr_multiply(const cagr_tree* tree, int op, const void* queries_dev,
                   const int32_t* query_order_dev, int64_t nq, const void* widths_dev,
-                  double width, int continuous, void* out_dev, int64_t out_stride, void* stream) {
+                  double width, int flags, void* out_dev, int64_t out_stride, void* stream) {
     if (int rc = check_tree(tree)) return rc;
     if (op_attr_dim(op) == 0) return set_error(CAGR_ERR_INVALID, "unknown operator");
+    if (flags & ~(CAGR_FLAG_CONTINUOUS | CAGR_FLAG_ACCUMULATE))
+        return set_error(CAGR_ERR_INVALID, "unknown flag bits");
     if (out_stride < 0 || out_stride > (1 << 20))
         return set_error(CAGR_ERR_INVALID, "out_stride out of range");
     cagr::TraverseArgs a;
     a.op = op;
-    a.continuous = continuous;
+    if (op == CAGR_OP_A2T_SUM || op == CAGR_OP_A2T_SUM_SHARED) {
+        a.op = cagr::kOpA2TFused;
+        a.slots = op == CAGR_OP_A2T_SUM ? 3 : 1;
+    }
+    a.continuous = (flags & CAGR_FLAG_CONTINUOUS) ? 1 : 0;
+    a.accumulate = (flags & CAGR_FLAG_ACCUMULATE) ? 1 : 0;
     a.queries = queries_dev;
     a.qorder = query_order_dev;
     a.nq = nq;
@@ -150,12 +165,16 @@ int cagr_multiply(const cagr_tree* tree, int op, const void* queries_dev,
 }
 
 int cagr_forward(cagr_tree* tree, int op, const void* values_dev, const void* widths_dev,
-                 double width, int continuous, void* out_dev, void* stream) {
+                 double width, int flags, void* out_dev, void* stream) {
     if (int rc = check_tree(tree)) return rc;
     const int dim = op_attr_dim(op);
-    if (dim == 0) return set_error(CAGR_ERR_INVALID, "unknown operator");
-    if (int rc = cagr::moments(tree->t, 0, values_dev, dim, nullptr, as_stream(stream))) return rc;
-    return cagr_multiply(tree, op, nullptr, nullptr, 0, widths_dev, width, continuous, out_dev, 0,
+    if (dim <= 0) return set_error(CAGR_ERR_INVALID, "unknown operator for cagr_forward");
+    if (op == CAGR_OP_A2T_SUM) {
+        if (int rc = cagr::moments3(tree->t, values_dev, as_stream(stream))) return rc;
+    } else if (int rc = cagr::moments(tree->t, 0, values_dev, dim, nullptr, as_stream(stream))) {
+        return rc;
+    }
+    return cagr_multiply(tree, op, nullptr, nullptr, 0, widths_dev, width, flags, out_dev, 0,
                          stream);
 }
 

@@ -7,12 +7,16 @@
 //                          position covered), npts (points under the node),
 //                          depth | is_leaf << 8 | nchild << 16}
 //   parent[M]      int32  parent id (-1 for the root)
+//   children[M*8]  int32  child ids in octant order (-1 = none)
 //   leaf_ids[NL]   int32  leaf node ids in preorder
-//   rec[(M+N)*12]  T      source records: [0, M) node records (centroid,
-//                          exp(-c/2), attribute sums, weight), [M, M+N)
-//                          point records in Morton order (position,
-//                          exp(-y/2), attribute) -- rewritten by every
-//                          moment pass.
+//   rec[(M+N)*12]  T      source records, three 4-vectors each:
+//                          node  i < M  : (cx, cy, cz, (4 half_w)^2)
+//                                         (e1, e2, e3, a0) (a1, a2, W, 0)
+//                          point M + s  : (x, y, z, 0) (e1, e2, e3, a0) (a1, a2, w, 0)
+//                          with c the weighted centroid, e_k = exp(-c_k / 2)
+//                          (resp. exp(-y_k / 2)), a the attribute (sum) and W / w
+//                          the weight; points in Morton order.  Rewritten by every
+//                          moment pass; one array per moment slot.
 //   counters[M]    uint32 arrival counters for the bottom-up moment pass
 //                          (self-resetting).
 #pragma once
@@ -22,18 +26,6 @@
 
 #define CAGR_MAX_DEPTH 21
 #define CAGR_REC_STRIDE 12  // scalars per source record
-
-// Record slots (in units of T) inside one record of CAGR_REC_STRIDE scalars.
-#define REC_X 0
-#define REC_Y 1
-#define REC_Z 2
-#define REC_E1 3
-#define REC_E2 4
-#define REC_E3 5
-#define REC_A0 6
-#define REC_A1 7
-#define REC_A2 8
-#define REC_W 9
 
 namespace cagr {
 
@@ -50,6 +42,44 @@ enum Status : int {
 __host__ __device__ inline int meta_depth(int w) { return w & 0xff; }
 __host__ __device__ inline bool meta_leaf(int w) { return (w >> 8) & 1; }
 __host__ __device__ inline int meta_nchild(int w) { return (w >> 16) & 0xff; }
+
+// 4-vector of T and aligned loads of one record component.
+template <typename T>
+struct Vec4Of;
+template <>
+struct Vec4Of<float> {
+    using type = float4;
+};
+template <>
+struct Vec4Of<double> {
+    using type = double4;
+};
+template <typename T>
+using Vec4 = typename Vec4Of<T>::type;
+
+template <typename T>
+__device__ __forceinline__ Vec4<T> ld4(const T* p) {
+    return *reinterpret_cast<const Vec4<T>*>(p);
+}
+template <typename T>
+__device__ __forceinline__ void st4(T* p, Vec4<T> v) {
+    *reinterpret_cast<Vec4<T>*>(p) = v;
+}
+// L2-coherent load (data written by other threads of the same launch)
+__device__ __forceinline__ float4 ld4_cg(const float* p) {
+    return __ldcg(reinterpret_cast<const float4*>(p));
+}
+__device__ __forceinline__ double4 ld4_cg(const double* p) {
+    const double2 a = __ldcg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float4 make4(float a, float b, float c, float d) {
+    return make_float4(a, b, c, d);
+}
+__device__ __forceinline__ double4 make4(double a, double b, double c, double d) {
+    return make_double4(a, b, c, d);
+}
 
 // Squared distance in the reference's operation order: d = x - c per axis,
 // then ((dx*dx + dy*dy) + dz*dz), each step rounded (no FMA contraction), so
@@ -102,7 +132,7 @@ __device__ __forceinline__ T width_threshold(T w) {
 // acceptance threshold `pow(4 * half_w, 2)` (wn_treecode_cuda_kernels.cu:595),
 // exact in both precisions.
 template <typename T>
-__device__ __forceinline__ T mac_radius2(int depth) {
+__host__ __device__ __forceinline__ T mac_radius2(int depth) {
     return T(16.0) * ldexp(T(1.0), -2 * depth);
 }
 

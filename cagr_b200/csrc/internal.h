@@ -60,6 +60,9 @@ int tree_export(const Tree* t, int64_t* parent, int64_t* children, uint8_t* is_l
 // tree dtype (original point order); weights: [N] or null (then |attr|).
 int moments(Tree* t, int slot, const void* attrs, int dim, const void* weights,
             cudaStream_t stream);
+// Three scalar attributes at once (values3: [N, 3], column k -> slot k, weights |v_k|):
+// the node moments of the reference's three A2Tk calls, in one launch.
+int moments3(Tree* t, const void* values3, cudaStream_t stream);
 // Copy node moments of a slot out in the reference layout:
 // node_attrs [M, dim], reppoints [M, 3], weights [M].
 int moments_export(const Tree* t, int slot, void* node_attrs, void* reppoints, void* weights,
@@ -78,12 +81,15 @@ enum Op : int {
     kOpA2T3 = 8,
     kOpG = 9,
     kOpA2Fused = 10,    // (A21, A22, A23) in one traversal -> [N', 3]
-    kOpA2TFused = 11,   // sum_k A2Tk(s_k), slots 0..2 -> [N', 3]
+    kOpA2TFused = 11,   // sum_k A2Tk(s_k) with slot k holding s_k -> [N', 3]
+    kOpCount = 12,      // pair terms per query with the slot-0 moments -> [N', 1]
 };
 
 struct TraverseArgs {
     int op = 0;
     int continuous = 0;
+    int accumulate = 0;
+    int slots = 1;                     // kOpA2TFused: 3 = slot k holds s_k, 1 = shared slot 0
     const void* queries = nullptr;     // [nq, 3] T or null (= the tree's points)
     const int32_t* qorder = nullptr;   // [nq] processing order or null
     int64_t nq = 0;

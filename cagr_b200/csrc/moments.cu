@@ -8,14 +8,18 @@
 // child (atomic arrival counter, reset by the thread that completes the node)
 // computes the parent from its children in octant order.  The floating-point
 // operation order is the reference's, so node sums, weights and centroids are
-// bit-identical to the reference's host build:
+// bit-identical to the reference kernels evaluated in IEEE arithmetic:
 //   leaf:     for points in node2point order  W += w;  A += a;  R += y*w;  P += y
 //   internal: for children in octant order    W += Wc; A += Ac; R += Rc*Wc; P += Rc
 //   centroid: W > 0 ? R * (1/W) : P * (1/npts)            (:456-461, :510-517)
-// The same launch writes the Morton-ordered point records the traversal reads,
-// and every record carries exp(-c/2) per axis so the traversal can form the
-// convection factor exp((x-c)_k/2) as exp(x_k/2) * exp(-c_k/2) without a
-// transcendental per pair.
+// The same launch writes the Morton-ordered point records the traversal reads.
+// Every record carries exp(-c/2) per axis so the traversal forms the
+// convection factor exp((x-c)_k/2) as exp(x_k/2) * exp(-c_k/2), and node
+// records carry the acceptance radius (4 half_w)^2.
+//
+// NS = 3 computes three independent scalar attributes (the three inputs of
+// the reference's A2T1/A2T2/A2T3 calls, each with its own |s_k| weights and
+// centroids) in one launch and one climb.
 #include <string>
 
 #include "internal.h"
@@ -31,111 +35,156 @@ __device__ __forceinline__ T weight_of(const T* a, int dim) {
     return sqrt_rn(add_rn(add_rn(mul_rn(a[0], a[0]), mul_rn(a[1], a[1])), mul_rn(a[2], a[2])));
 }
 
-template <typename T>
-__device__ __forceinline__ void write_record(T* r, const T* pos, const T* acc, int dim, T W) {
-    r[REC_X] = pos[0];
-    r[REC_Y] = pos[1];
-    r[REC_Z] = pos[2];
-    r[REC_E1] = exp_t(pos[0] * T(-0.5));
-    r[REC_E2] = exp_t(pos[1] * T(-0.5));
-    r[REC_E3] = exp_t(pos[2] * T(-0.5));
-    r[REC_A0] = acc[0];
-    r[REC_A1] = dim == 3 ? acc[1] : T(0);
-    r[REC_A2] = dim == 3 ? acc[2] : T(0);
-    r[REC_W] = W;
-    r[10] = T(0);
-    r[11] = T(0);
+// r0 = (x, y, z, r0w), r1 = (e1, e2, e3, a0), r2 = (a1, a2, W, 0)
+template <typename T, int DIM>
+__device__ __forceinline__ void write_record(T* r, const T* pos, const T* e, const T* a, T W,
+                                             T r0w) {
+    st4<T>(r, make4(pos[0], pos[1], pos[2], r0w));
+    st4<T>(r + 4, make4(e[0], e[1], e[2], a[0]));
+    st4<T>(r + 8, make4(DIM == 3 ? a[1] : T(0), DIM == 3 ? a[2] : T(0), W, T(0)));
 }
 
-template <typename T, int DIM>
-__global__ void __launch_bounds__(kBlock)
-    k_moments(int64_t num_leaves, int64_t M, const int32_t* __restrict__ leaf_ids,
-              const int4* __restrict__ meta, const int32_t* __restrict__ parent,
-              const int32_t* __restrict__ perm, const int32_t* __restrict__ invperm,
-              const int32_t* __restrict__ n2p, const int64_t* __restrict__ n2p_start,
-              const T* __restrict__ spos, const T* __restrict__ attrs,
-              const T* __restrict__ weights, uint32_t* __restrict__ counters, T* __restrict__ rec) {
+template <typename T>
+__device__ __forceinline__ void exps(const T* c, T* e) {
+    e[0] = exp_t(c[0] * T(-0.5));
+    e[1] = exp_t(c[1] * T(-0.5));
+    e[2] = exp_t(c[2] * T(-0.5));
+}
+
+template <typename T, int DIM, int NS>
+struct MomParams {
+    int64_t num_leaves = 0, M = 0;
+    const int32_t* leaf_ids = nullptr;
+    const int4* meta = nullptr;
+    const int32_t* parent = nullptr;
+    const int32_t* children = nullptr;
+    const int32_t* perm = nullptr;
+    const int32_t* invperm = nullptr;
+    const int32_t* n2p = nullptr;
+    const int64_t* n2p_start = nullptr;
+    const T* spos = nullptr;
+    const T* attrs = nullptr;    // row stride astride; slot k reads columns [k*DIM, k*DIM+DIM)
+    int astride = DIM;
+    const T* weights = nullptr;  // NS == 1 only; null = |attr|
+    uint32_t* counters = nullptr;
+    T* rec[NS];
+};
+
+template <typename T, int DIM, int NS>
+__global__ void __launch_bounds__(kBlock) k_moments(const MomParams<T, DIM, NS> p) {
     const int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (li >= num_leaves) return;
-    int node = leaf_ids[li];
-    const int4 lm = meta[node];
+    if (li >= p.num_leaves) return;
+    const int64_t M = p.M;
+    int node = p.leaf_ids[li];
+    const int4 lm = p.meta[node];
     const int pstart = lm.y, np = lm.z;
 
     // point records for the leaf's Morton range
     for (int j = 0; j < np; j++) {
         const int s = pstart + j;
-        const int p = perm[s];
-        T pos[3] = {spos[3 * s], spos[3 * s + 1], spos[3 * s + 2]};
-        T a[3] = {T(0), T(0), T(0)};
-        for (int c = 0; c < DIM; c++) a[c] = attrs[(int64_t)p * DIM + c];
-        const T w = weights ? weights[p] : weight_of(a, DIM);
-        write_record(rec + (M + s) * CAGR_REC_STRIDE, pos, a, DIM, w);
+        const int pt = p.perm[s];
+        const T pos[3] = {p.spos[3 * s], p.spos[3 * s + 1], p.spos[3 * s + 2]};
+        T e[3];
+        exps(pos, e);
+#pragma unroll
+        for (int k = 0; k < NS; k++) {
+            T a[3] = {T(0), T(0), T(0)};
+#pragma unroll
+            for (int c = 0; c < DIM; c++) a[c] = p.attrs[(int64_t)pt * p.astride + k * DIM + c];
+            const T w = (NS == 1 && p.weights) ? p.weights[pt] : weight_of(a, DIM);
+            write_record<T, DIM>(p.rec[k] + (M + s) * CAGR_REC_STRIDE, pos, e, a, w, T(0));
+        }
     }
 
     // leaf moments, points in node2point (ascending original index) order
-    T W = T(0), A[3] = {T(0), T(0), T(0)}, R[3] = {T(0), T(0), T(0)}, P[3] = {T(0), T(0), T(0)};
+    T W[NS], A[NS][3], R[NS][3], P[NS][3];
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+        W[k] = T(0);
+        for (int d = 0; d < 3; d++) A[k][d] = R[k][d] = P[k][d] = T(0);
+    }
     {
-        const int64_t base = n2p_start[node];
+        const int64_t base = p.n2p_start[node];
         for (int j = 0; j < np; j++) {
-            const int p = (np == 1) ? perm[pstart] : n2p[base + j];
-            const int s = (np == 1) ? pstart : invperm[p];
-            T a[3] = {T(0), T(0), T(0)};
-            for (int c = 0; c < DIM; c++) a[c] = attrs[(int64_t)p * DIM + c];
-            const T w = weights ? weights[p] : weight_of(a, DIM);
-            W = add_rn(W, w);
-            for (int c = 0; c < DIM; c++) A[c] = add_rn(A[c], a[c]);
-            for (int d = 0; d < 3; d++) {
-                const T y = spos[3 * s + d];
-                R[d] = add_rn(R[d], mul_rn(y, w));
-                P[d] = add_rn(P[d], y);
+            const int pt = (np == 1) ? p.perm[pstart] : p.n2p[base + j];
+            const int s = (np == 1) ? pstart : p.invperm[pt];
+            const T y[3] = {p.spos[3 * s], p.spos[3 * s + 1], p.spos[3 * s + 2]};
+#pragma unroll
+            for (int k = 0; k < NS; k++) {
+                T a[3] = {T(0), T(0), T(0)};
+#pragma unroll
+                for (int c = 0; c < DIM; c++)
+                    a[c] = p.attrs[(int64_t)pt * p.astride + k * DIM + c];
+                const T w = (NS == 1 && p.weights) ? p.weights[pt] : weight_of(a, DIM);
+                W[k] = add_rn(W[k], w);
+                for (int c = 0; c < DIM; c++) A[k][c] = add_rn(A[k][c], a[c]);
+                for (int d = 0; d < 3; d++) {
+                    R[k][d] = add_rn(R[k][d], mul_rn(y[d], w));
+                    P[k][d] = add_rn(P[k][d], y[d]);
+                }
             }
         }
     }
 
-    int count = np;  // points under `node`: the zero-weight centroid divides by it
+    int count = np;          // points under `node`: the zero-weight centroid divides by it
+    int depth = meta_depth(lm.w);
     while (true) {
-        T c[3];
-        if (W > T(0)) {
-            const T inv = div_rn(T(1), W);
-            for (int d = 0; d < 3; d++) c[d] = mul_rn(R[d], inv);
-        } else {
-            // (wn_treecode_cuda_kernels.cu:459-460 for leaves, :515-517 for internal
-            // nodes, where it divides a sum of child centroids by the point count)
-            const T inv = div_rn(T(1), T(count));
-            for (int d = 0; d < 3; d++) c[d] = mul_rn(P[d], inv);
+#pragma unroll
+        for (int k = 0; k < NS; k++) {
+            T c[3], e[3];
+            if (W[k] > T(0)) {
+                const T inv = div_rn(T(1), W[k]);
+                for (int d = 0; d < 3; d++) c[d] = mul_rn(R[k][d], inv);
+            } else {
+                // (wn_treecode_cuda_kernels.cu:459-460 for leaves, :515-517 for internal
+                // nodes, where it divides a sum of child centroids by the point count)
+                const T inv = div_rn(T(1), T(count));
+                for (int d = 0; d < 3; d++) c[d] = mul_rn(P[k][d], inv);
+            }
+            exps(c, e);
+            write_record<T, DIM>(p.rec[k] + (int64_t)node * CAGR_REC_STRIDE, c, e, A[k], W[k],
+                                 mac_radius2<T>(depth));
         }
-        write_record(rec + (int64_t)node * CAGR_REC_STRIDE, c, A, DIM, W);
         if (node == 0) return;
         // publish this node, then arrive at the parent
         __threadfence();
-        const int par = parent[node];
-        const int4 pm = meta[par];
-        const uint32_t arrived = atomicAdd(&counters[par], 1u);
+        const int par = p.parent[node];
+        const int4 pm = p.meta[par];
+        const uint32_t arrived = atomicAdd(&p.counters[par], 1u);
         if (arrived + 1u != (uint32_t)meta_nchild(pm.w)) return;
-        counters[par] = 0u;  // every child has arrived: ready for the next pass
+        p.counters[par] = 0u;  // every child has arrived: ready for the next pass
         __threadfence();
         node = par;
         count = pm.z;
-        W = T(0);
-        for (int d = 0; d < 3; d++) {
-            A[d] = T(0);
-            R[d] = T(0);
-            P[d] = T(0);
+        depth = meta_depth(pm.w);
+#pragma unroll
+        for (int k = 0; k < NS; k++) {
+            W[k] = T(0);
+            for (int d = 0; d < 3; d++) A[k][d] = R[k][d] = P[k][d] = T(0);
         }
-        // children of `node` in octant order = preorder: node+1, then skip pointers;
-        // read through L2 (other threads wrote them during this launch)
-        const int end = pm.x;
-        for (int ch = node + 1; ch < end;) {
-            const T* r = rec + (int64_t)ch * CAGR_REC_STRIDE;
-            const T wc = __ldcg(r + REC_W);
-            W = add_rn(W, wc);
-            for (int cc = 0; cc < DIM; cc++) A[cc] = add_rn(A[cc], __ldcg(r + REC_A0 + cc));
-            for (int d = 0; d < 3; d++) {
-                const T rc = __ldcg(r + REC_X + d);
-                R[d] = add_rn(R[d], mul_rn(rc, wc));
-                P[d] = add_rn(P[d], rc);
+        // children in octant order, read through L2 (written during this launch)
+        const int4 c0 = reinterpret_cast<const int4*>(p.children)[2 * (int64_t)node];
+        const int4 c1 = reinterpret_cast<const int4*>(p.children)[2 * (int64_t)node + 1];
+        const int ch[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            if (ch[q] < 0) continue;
+#pragma unroll
+            for (int k = 0; k < NS; k++) {
+                const T* r = p.rec[k] + (int64_t)ch[q] * CAGR_REC_STRIDE;
+                const Vec4<T> r0 = ld4_cg(r);
+                const Vec4<T> r1 = ld4_cg(r + 4);
+                const Vec4<T> r2 = ld4_cg(r + 8);
+                const T wc = r2.z;
+                const T ac[3] = {r1.w, r2.x, r2.y};
+                const T rc[3] = {r0.x, r0.y, r0.z};
+                W[k] = add_rn(W[k], wc);
+                for (int c = 0; c < DIM; c++) A[k][c] = add_rn(A[k][c], ac[c]);
+                for (int d = 0; d < 3; d++) {
+                    R[k][d] = add_rn(R[k][d], mul_rn(rc[d], wc));
+                    P[k][d] = add_rn(P[k][d], rc[d]);
+                }
             }
-            ch = meta[ch].x;
         }
     }
 }
@@ -146,37 +195,74 @@ __global__ void k_export_moments(const T* __restrict__ rec, int64_t M, T* __rest
     const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= M) return;
     const T* r = rec + n * CAGR_REC_STRIDE;
+    const T a[3] = {r[7], r[8], r[9]};
     if (node_attrs)
-        for (int c = 0; c < DIM; c++) node_attrs[n * DIM + c] = r[REC_A0 + c];
+        for (int c = 0; c < DIM; c++) node_attrs[n * DIM + c] = a[c];
     if (reppoints)
-        for (int d = 0; d < 3; d++) reppoints[n * 3 + d] = r[REC_X + d];
-    if (weights) weights[n] = r[REC_W];
+        for (int d = 0; d < 3; d++) reppoints[n * 3 + d] = r[d];
+    if (weights) weights[n] = r[10];
+}
+
+int ensure_slot(Tree* t, int slot, size_t elem) {
+    if (t->rec[slot]) return kOk;
+    cudaError_t e = cudaMalloc(&t->rec[slot], elem * (size_t)(t->m + t->n) * CAGR_REC_STRIDE);
+    if (e != cudaSuccess) {
+        t->rec[slot] = nullptr;
+        return set_error(kErrAlloc, std::string("record allocation: ") + cudaGetErrorString(e));
+    }
+    return kOk;
+}
+
+template <typename T, int DIM, int NS>
+MomParams<T, DIM, NS> params(Tree* t, const void* attrs, int astride, const void* weights) {
+    MomParams<T, DIM, NS> p;
+    p.num_leaves = t->num_leaves;
+    p.M = t->m;
+    p.leaf_ids = t->leaf_ids;
+    p.meta = t->meta;
+    p.parent = t->parent;
+    p.children = t->children;
+    p.perm = t->perm;
+    p.invperm = t->invperm;
+    p.n2p = t->n2p;
+    p.n2p_start = t->n2p_start;
+    p.spos = (const T*)t->spos;
+    p.attrs = (const T*)attrs;
+    p.astride = astride;
+    p.weights = (const T*)weights;
+    p.counters = t->counters;
+    return p;
 }
 
 template <typename T>
 int launch_moments(Tree* t, int slot, const void* attrs, int dim, const void* weights,
                    cudaStream_t s) {
-    if (!t->rec[slot]) {
-        cudaError_t e =
-            cudaMalloc(&t->rec[slot], sizeof(T) * (size_t)(t->m + t->n) * CAGR_REC_STRIDE);
-        if (e != cudaSuccess) {
-            t->rec[slot] = nullptr;
-            return set_error(kErrAlloc, std::string("record allocation: ") + cudaGetErrorString(e));
-        }
-    }
+    if (int rc = ensure_slot(t, slot, sizeof(T))) return rc;
     const unsigned grid = (unsigned)((t->num_leaves + kBlock - 1) / kBlock);
-    if (dim == 3)
-        k_moments<T, 3><<<grid, kBlock, 0, s>>>(t->num_leaves, t->m, t->leaf_ids, t->meta,
-                                                t->parent, t->perm, t->invperm, t->n2p,
-                                                t->n2p_start, (const T*)t->spos, (const T*)attrs,
-                                                (const T*)weights, t->counters, (T*)t->rec[slot]);
-    else
-        k_moments<T, 1><<<grid, kBlock, 0, s>>>(t->num_leaves, t->m, t->leaf_ids, t->meta,
-                                                t->parent, t->perm, t->invperm, t->n2p,
-                                                t->n2p_start, (const T*)t->spos, (const T*)attrs,
-                                                (const T*)weights, t->counters, (T*)t->rec[slot]);
+    if (dim == 3) {
+        auto p = params<T, 3, 1>(t, attrs, 3, weights);
+        p.rec[0] = (T*)t->rec[slot];
+        k_moments<T, 3, 1><<<grid, kBlock, 0, s>>>(p);
+    } else {
+        auto p = params<T, 1, 1>(t, attrs, 1, weights);
+        p.rec[0] = (T*)t->rec[slot];
+        k_moments<T, 1, 1><<<grid, kBlock, 0, s>>>(p);
+    }
     CAGR_CUDA(cudaGetLastError());
     t->rec_dim[slot] = dim;
+    return kOk;
+}
+
+template <typename T>
+int launch_moments3(Tree* t, const void* values3, cudaStream_t s) {
+    for (int k = 0; k < 3; k++)
+        if (int rc = ensure_slot(t, k, sizeof(T))) return rc;
+    const unsigned grid = (unsigned)((t->num_leaves + kBlock - 1) / kBlock);
+    auto p = params<T, 1, 3>(t, values3, 3, nullptr);
+    for (int k = 0; k < 3; k++) p.rec[k] = (T*)t->rec[k];
+    k_moments<T, 1, 3><<<grid, kBlock, 0, s>>>(p);
+    CAGR_CUDA(cudaGetLastError());
+    for (int k = 0; k < 3; k++) t->rec_dim[k] = 1;
     return kOk;
 }
 
@@ -189,6 +275,12 @@ int moments(Tree* t, int slot, const void* attrs, int dim, const void* weights,
     if (!attrs) return set_error(kErrInvalid, "attrs is null");
     return t->dtype == 0 ? launch_moments<float>(t, slot, attrs, dim, weights, stream)
                          : launch_moments<double>(t, slot, attrs, dim, weights, stream);
+}
+
+int moments3(Tree* t, const void* values3, cudaStream_t stream) {
+    if (!values3) return set_error(kErrInvalid, "values is null");
+    return t->dtype == 0 ? launch_moments3<float>(t, values3, stream)
+                         : launch_moments3<double>(t, values3, stream);
 }
 
 int moments_export(const Tree* t, int slot, void* node_attrs, void* reppoints, void* weights,

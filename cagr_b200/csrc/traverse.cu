@@ -10,21 +10,28 @@
 // B200 formulation: one WARP walks the tree for 32 Morton-consecutive queries.
 //  * The walk is stackless: nodes are in preorder, so "descend" is n+1 and
 //    "skip the subtree" is meta.next.  Every node load is warp-uniform (one
-//    L1 wavefront), and control flow stays uniform across the warp.
-//  * Each query keeps exactly its own reference acceptance decisions through a
-//    per-depth lane mask in shared memory: mask[d+1] = the lanes that opened the
-//    depth-d ancestor.  A lane contributes at a node only if it is in the mask
-//    for that depth; far lanes add the node term, near lanes descend, and at a
-//    leaf near lanes add the leaf's points.  The set of pair terms per query is
-//    therefore the reference's set; only the summation order differs.
-//  * Acceptance and width tests use the reference's rounding (see common.cuh),
-//    so they are decided bit-identically; the inner loop compares squared
-//    distances and needs one rsqrt per pair.
+//    L1 wavefront) and the loop control is uniform across the warp.
+//  * Each query keeps exactly its own reference decisions with one integer:
+//    kd = the deepest depth at which the query is still "active" (has opened
+//    every ancestor).  At a node of depth d an active lane (d <= kd) sets
+//    kd = d + 1 if it opens an internal node and kd = d otherwise.  Because
+//    the walk only ever moves to the first child (depth d + 1) or to the next
+//    node after a subtree (depth <= d), "active at the next node" is exactly
+//    "depth <= kd".  The warp descends when any lane opened the node.  So the
+//    set of pair terms of every query is the reference's set; only the
+//    summation order differs.
+//  * Acceptance and width tests use the reference's rounding (common.cuh) and
+//    are decided bit-identically; the inner loop compares squared distances
+//    and needs one rsqrt per pair.  The width rule is a select, not a branch.
 //  * exp((x-y)_k/2) = exp(x_k/2) * exp(-y_k/2): the second factor is stored in
-//    every source record, the first is per query and applied once at the end,
-//    so a pair term costs no transcendental beyond the rsqrt.
-//  * A2Fused evaluates A21, A22, A23 in one walk (they share node moments and
-//    acceptance decisions in the reference, which walks three times).
+//    every source record, the first is per query, so a pair term costs no
+//    transcendental beyond the rsqrt.
+//  * A2Fused evaluates A21, A22, A23 in one walk (one set of node moments and
+//    acceptance decisions, as in the reference, which walks three times).
+//  * k_traverse_a2t walks once for sum_k A2Tk(s_k): with three moment slots
+//    (the reference's three calls, each with its own |s_k|-weighted centroids
+//    and therefore its own acceptance decisions, tracked by three kd's), or
+//    with one shared slot when s_1 = s_2 = s_3 (the constant right-hand side).
 #include <string>
 
 #include "internal.h"
@@ -39,9 +46,7 @@ template <typename T>
 struct TravParams {
     int64_t M = 0, N = 0, nq = 0;
     const int4* meta = nullptr;
-    const T* rec = nullptr;
-    const T* rec1 = nullptr;   // A2TFused: slot 1
-    const T* rec2 = nullptr;   // A2TFused: slot 2
+    const T* rec[3] = {nullptr, nullptr, nullptr};
     const T* spos = nullptr;   // sorted tree points (queries == points)
     const int32_t* perm = nullptr;
     const T* queries = nullptr;
@@ -50,7 +55,13 @@ struct TravParams {
     T width = T(0);
     T* out = nullptr;
     int out_stride = 1;
+    int accumulate = 0;  // add into `out` instead of overwriting it
 };
+
+template <typename T>
+__device__ __forceinline__ void put(T* o, int j, T v, int accumulate) {
+    o[j] = accumulate ? o[j] + v : v;
+}
 
 template <int OP>
 struct OpInfo {
@@ -58,11 +69,15 @@ struct OpInfo {
                                OP == kOpA2Fused;
     static constexpr bool a2t = OP == kOpA2T1 || OP == kOpA2T2 || OP == kOpA2T3;
     static constexpr bool uses_exp = a2 || a2t;
+    static constexpr bool dim3 = a2 || OP == kOpA || OP == kOpG;
     // which convection direction a single-direction operator uses
     static constexpr int k [[maybe_unused]] = (OP == kOpA21 || OP == kOpA2T1)   ? 0
-                             : (OP == kOpA22 || OP == kOpA2T2) ? 1
-                             : (OP == kOpA23 || OP == kOpA2T3) ? 2
-                                                               : -1;
+                                              : (OP == kOpA22 || OP == kOpA2T2) ? 1
+                                              : (OP == kOpA23 || OP == kOpA2T3) ? 2
+                                                                                : -1;
+    static constexpr bool sums0 = k == 0 || OP == kOpA3 || OP == kOpA2Fused;
+    static constexpr bool sums1 = k == 1 || OP == kOpA3 || OP == kOpA2Fused;
+    static constexpr bool sums2 = k == 2 || OP == kOpA3 || OP == kOpA2Fused;
 };
 
 // Per-lane state of one query.
@@ -79,63 +94,60 @@ struct Lane {
 template <typename T, int OP, bool CONT>
 __device__ __forceinline__ void pair_term(Lane<T>& L, const T* __restrict__ src, T dx, T dy, T dz,
                                           T d2) {
-    const bool outside = d2 >= L.tw;
-    const T rinv = rsqrt_t(d2);
-    const T rinv3 = rinv * rinv * rinv;
-    if constexpr (OP == kOpA || OpInfo<OP>::a2 || OP == kOpG) {
-        const T m0 = src[REC_A0], m1 = src[REC_A1], m2 = src[REC_A2];
-        const T dm = dx * m0 + dy * m1 + dz * m2;
-        if constexpr (OP == kOpA) {
-            if (outside) L.acc0 += dm * rinv3;
-            else if (CONT) L.in0 += dm * L.iw3;
-        } else if constexpr (OP == kOpG) {
-            if (outside) {
+    if constexpr (OP == kOpCount) {
+        L.acc0 += T(1);  // one pair term, whichever branch the reference takes
+        return;
+    } else {
+        const bool outside = d2 >= L.tw;
+        const T rinv = outside ? rsqrt_t(d2) : T(0);  // zero: the pair contributes nothing
+        const T rinv3 = rinv * rinv * rinv;
+        const Vec4<T> r1 = ld4(src + 4);  // (e1, e2, e3, a0)
+        if constexpr (OpInfo<OP>::dim3) {
+            const Vec4<T> r2 = ld4(src + 8);  // (a1, a2, W, 0)
+            const T m0 = r1.w, m1 = r2.x, m2 = r2.y;
+            const T dm = dx * m0 + dy * m1 + dz * m2;
+            if constexpr (OP == kOpA) {
+                L.acc0 += dm * rinv3;
+                if (CONT && !outside) L.in0 += dm * L.iw3;
+            } else if constexpr (OP == kOpG) {
                 const T rinv5 = rinv3 * rinv * rinv;
                 const T c = T(3) * dm * rinv5;
                 L.acc0 += m0 * rinv3 - dx * c;
                 L.acc1 += m1 * rinv3 - dy * c;
                 L.acc2 += m2 * rinv3 - dz * c;
-            }
-        } else {
-            // A2k: exp(d_k/2) (dm / r^3 + m_k / (2r)); continuous inside:
-            // exp(w) (dm / w^3 + m_k / (2w))
-            if (outside) {
+            } else {
+                // A2k: exp(d_k/2) (dm / r^3 + m_k / (2r))
                 const T t = dm * rinv3;
                 const T h = T(0.5) * rinv;
-                constexpr int k = OpInfo<OP>::k;
-                if constexpr (k == 0 || OP == kOpA3 || OP == kOpA2Fused)
-                    L.acc0 += src[REC_E1] * (t + h * m0);
-                if constexpr (k == 1 || OP == kOpA3 || OP == kOpA2Fused)
-                    L.acc1 += src[REC_E2] * (t + h * m1);
-                if constexpr (k == 2 || OP == kOpA3 || OP == kOpA2Fused)
-                    L.acc2 += src[REC_E3] * (t + h * m2);
-            } else if (CONT) {
-                const T t = dm * L.iw3;
-                const T h = T(0.5) * L.iw;
-                constexpr int k = OpInfo<OP>::k;
-                if constexpr (k == 0 || OP == kOpA3 || OP == kOpA2Fused) L.in0 += t + h * m0;
-                if constexpr (k == 1 || OP == kOpA3 || OP == kOpA2Fused) L.in1 += t + h * m1;
-                if constexpr (k == 2 || OP == kOpA3 || OP == kOpA2Fused) L.in2 += t + h * m2;
+                if constexpr (OpInfo<OP>::sums0) L.acc0 += r1.x * (t + h * m0);
+                if constexpr (OpInfo<OP>::sums1) L.acc1 += r1.y * (t + h * m1);
+                if constexpr (OpInfo<OP>::sums2) L.acc2 += r1.z * (t + h * m2);
+                if constexpr (CONT) {
+                    // continuous, inside the width: exp(w) (dm / w^3 + m_k / (2w))
+                    if (!outside) {
+                        const T ti = dm * L.iw3;
+                        const T hi = T(0.5) * L.iw;
+                        if constexpr (OpInfo<OP>::sums0) L.in0 += ti + hi * m0;
+                        if constexpr (OpInfo<OP>::sums1) L.in1 += ti + hi * m1;
+                        if constexpr (OpInfo<OP>::sums2) L.in2 += ti + hi * m2;
+                    }
+                }
             }
-        }
-    } else if constexpr (OP == kOpAT) {
-        if (outside) {
-            const T c = src[REC_A0] * rinv3;
+        } else if constexpr (OP == kOpAT) {
+            const T c = r1.w * rinv3;
             L.acc0 += dx * c;
             L.acc1 += dy * c;
             L.acc2 += dz * c;
-        }
-    } else if constexpr (OpInfo<OP>::a2t) {
-        // exp(d_k/2) (d s / r^3 + e_k s / (2r)); no continuous branch (:293-299)
-        if (outside) {
+        } else if constexpr (OpInfo<OP>::a2t) {
+            // exp(d_k/2) (d s / r^3 + e_k s / (2r)); no continuous branch (:293-299)
             constexpr int k = OpInfo<OP>::k;
-            const T s = src[REC_A0];
-            const T e = src[REC_E1 + k];
-            const T c = e * s * rinv3;
+            const T e = k == 0 ? r1.x : (k == 1 ? r1.y : r1.z);
+            const T g = e * r1.w;
+            const T c = g * rinv3;
             L.acc0 += dx * c;
             L.acc1 += dy * c;
             L.acc2 += dz * c;
-            const T h = e * s * T(0.5) * rinv;
+            const T h = g * T(0.5) * rinv;
             if constexpr (k == 0) L.acc0 += h;
             if constexpr (k == 1) L.acc1 += h;
             if constexpr (k == 2) L.acc2 += h;
@@ -143,21 +155,14 @@ __device__ __forceinline__ void pair_term(Lane<T>& L, const T* __restrict__ src,
     }
 }
 
-template <typename T, int OP, bool CONT>
-__global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p) {
-    __shared__ unsigned smask[kWarps][CAGR_MAX_DEPTH + 2];
-    const int lane = threadIdx.x & 31;
-    const int wid = threadIdx.x >> 5;
-    const int64_t qi = ((int64_t)blockIdx.x * kWarps + wid) * 32 + lane;
-    const bool valid = qi < p.nq;
-    const unsigned vmask = __ballot_sync(kFull, valid);
-    if (vmask == 0) return;  // whole warp past the end
-
-    // this lane's query
-    int64_t oidx = 0;
-    Lane<T> L;
-    T w = p.width;
+// Loads this lane's query; returns false past the end.
+template <typename T>
+__device__ __forceinline__ bool load_query(const TravParams<T>& p, int64_t qi, Lane<T>& L,
+                                           int64_t& oidx, T& w) {
+    w = p.width;
+    oidx = 0;
     L.q0 = L.q1 = L.q2 = T(0);
+    const bool valid = qi < p.nq;
     if (valid) {
         if (p.queries == nullptr) {
             oidx = p.perm[qi];
@@ -177,35 +182,47 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p)
     L.iw3 = T(1) / (w * w * w);
     L.acc0 = L.acc1 = L.acc2 = T(0);
     L.in0 = L.in1 = L.in2 = T(0);
+    return valid;
+}
 
-    unsigned* sm = smask[wid];
-    if (lane == 0) sm[0] = vmask;
-    __syncwarp();
+template <typename T, int OP, bool CONT>
+__global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p) {
+    const int lane = threadIdx.x & 31;
+    const int64_t qi = ((int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32 + lane;
+    if (__all_sync(kFull, qi >= p.nq)) return;  // whole warp past the end
+    Lane<T> L;
+    int64_t oidx;
+    T w;
+    const bool valid = load_query(p, qi, L, oidx, w);
 
-    const int64_t M = p.M;
-    const T* __restrict__ rec = p.rec;
+    const int M = (int)p.M;
+    const T* __restrict__ rec = p.rec[0];
+    int kd = valid ? 0 : -1;  // active at depth d  <=>  d <= kd
     int n = 0;
     while (n < M) {
-        const int4 mt = p.meta[n];
-        const int depth = meta_depth(mt.w);
+        const int4 mt = __ldg(p.meta + n);
+        const int d = meta_depth(mt.w);
         const bool leaf = meta_leaf(mt.w);
-        const bool active = (sm[depth] >> lane) & 1u;
         const T* r = rec + (int64_t)n * CAGR_REC_STRIDE;
-        T dx = sub_rn(L.q0, r[REC_X]);
-        T dy = sub_rn(L.q1, r[REC_Y]);
-        T dz = sub_rn(L.q2, r[REC_Z]);
+        const Vec4<T> r0 = ld4(r);  // (cx, cy, cz, (4 half_w)^2)
+        T dx = sub_rn(L.q0, r0.x);
+        T dy = sub_rn(L.q1, r0.y);
+        T dz = sub_rn(L.q2, r0.z);
         T d2 = dist2_exact(dx, dy, dz);
-        const bool far = d2 > mac_radius2<T>(depth);
+        const bool active = d <= kd;
+        const bool far = d2 > r0.w;
         const bool open = active && !far;
-        const unsigned omask = __ballot_sync(kFull, open);
+        if (active) kd = (open && !leaf) ? d + 1 : d;
+        const bool any_open = __any_sync(kFull, open);
         if (leaf && mt.z == 1) {
-            // single-point leaf: far lanes use the node term, near lanes the point
+            // single-point leaf: far lanes take the node term, near lanes the point
             const T* src = r;
             if (open) {
-                src = rec + (M + mt.y) * CAGR_REC_STRIDE;
-                dx = sub_rn(L.q0, src[REC_X]);
-                dy = sub_rn(L.q1, src[REC_Y]);
-                dz = sub_rn(L.q2, src[REC_Z]);
+                src = rec + ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
+                const Vec4<T> s0 = ld4(src);
+                dx = sub_rn(L.q0, s0.x);
+                dy = sub_rn(L.q1, s0.y);
+                dz = sub_rn(L.q2, s0.z);
                 d2 = dist2_exact(dx, dy, dz);
             }
             if (active) pair_term<T, OP, CONT>(L, src, dx, dy, dz, d2);
@@ -214,69 +231,193 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p)
         }
         if (active && far) pair_term<T, OP, CONT>(L, r, dx, dy, dz, d2);
         if (leaf) {
-            if (omask) {
-                const T* pr = rec + (M + mt.y) * CAGR_REC_STRIDE;
+            if (any_open) {
+                const T* pr = rec + ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
                 for (int j = 0; j < mt.z; j++, pr += CAGR_REC_STRIDE) {
                     if (open) {
-                        const T ex = sub_rn(L.q0, pr[REC_X]);
-                        const T ey = sub_rn(L.q1, pr[REC_Y]);
-                        const T ez = sub_rn(L.q2, pr[REC_Z]);
+                        const Vec4<T> s0 = ld4(pr);
+                        const T ex = sub_rn(L.q0, s0.x);
+                        const T ey = sub_rn(L.q1, s0.y);
+                        const T ez = sub_rn(L.q2, s0.z);
                         pair_term<T, OP, CONT>(L, pr, ex, ey, ez, dist2_exact(ex, ey, ez));
                     }
                 }
             }
             n = mt.x;
-        } else if (omask) {
-            if (lane == 0) sm[depth + 1] = omask;
-            __syncwarp();
-            n = n + 1;
         } else {
-            n = mt.x;
+            n = any_open ? n + 1 : mt.x;
         }
     }
 
     if (!valid) return;
     T* o = p.out + oidx * (int64_t)p.out_stride;
+    const int acc = p.accumulate;
     if constexpr (OpInfo<OP>::uses_exp) {
         const T ex0 = exp_t(L.q0 * T(0.5)), ex1 = exp_t(L.q1 * T(0.5)), ex2 = exp_t(L.q2 * T(0.5));
         const T ew = CONT ? exp_t(w) : T(0);
         const T v0 = ex0 * L.acc0 + ew * L.in0;
         const T v1 = ex1 * L.acc1 + ew * L.in1;
         const T v2 = ex2 * L.acc2 + ew * L.in2;
-        if constexpr (OP == kOpA21) o[0] = v0;
-        if constexpr (OP == kOpA22) o[0] = v1;
-        if constexpr (OP == kOpA23) o[0] = v2;
-        if constexpr (OP == kOpA3) o[0] = (v0 + v1 + v2) / T(3);
+        if constexpr (OP == kOpA21) put(o, 0, v0, acc);
+        if constexpr (OP == kOpA22) put(o, 0, v1, acc);
+        if constexpr (OP == kOpA23) put(o, 0, v2, acc);
+        if constexpr (OP == kOpA3) put(o, 0, (v0 + v1 + v2) / T(3), acc);
         if constexpr (OP == kOpA2Fused) {
-            o[0] = v0;
-            o[1] = v1;
-            o[2] = v2;
+            put(o, 0, v0, acc);
+            put(o, 1, v1, acc);
+            put(o, 2, v2, acc);
         }
         if constexpr (OpInfo<OP>::a2t) {
             constexpr int k = OpInfo<OP>::k;
             const T ek = k == 0 ? ex0 : (k == 1 ? ex1 : ex2);
-            o[0] = ek * L.acc0;
-            o[1] = ek * L.acc1;
-            o[2] = ek * L.acc2;
+            put(o, 0, ek * L.acc0, acc);
+            put(o, 1, ek * L.acc1, acc);
+            put(o, 2, ek * L.acc2, acc);
         }
     } else if constexpr (OP == kOpA) {
-        o[0] = L.acc0 + L.in0;
+        put(o, 0, L.acc0 + L.in0, acc);
+    } else if constexpr (OP == kOpCount) {
+        put(o, 0, L.acc0, acc);
     } else {
-        o[0] = L.acc0;
-        o[1] = L.acc1;
-        o[2] = L.acc2;
+        put(o, 0, L.acc0, acc);
+        put(o, 1, L.acc1, acc);
+        put(o, 2, L.acc2, acc);
     }
 }
 
+// One A2T term of the directions [klo, khi) with weight s:
+//   acc += sum_k g_k (d / r^3 + e_k / (2r)),  g_k = exp(x_k/2) e_k(y) s,
+// where e(y) = exp(-y/2) comes from the record (folded per term so that the
+// three directions, which may use different sources, share one accumulator).
+template <typename T>
+__device__ __forceinline__ void a2t_term(Lane<T>& L, const T* ex, const T* e, T s, T dx, T dy,
+                                         T dz, T d2, int klo, int khi) {
+    const bool outside = d2 >= L.tw;
+    const T rinv = outside ? rsqrt_t(d2) : T(0);
+    const T rinv3 = rinv * rinv * rinv;
+    const T hr = T(0.5) * rinv;
+    T gsum = T(0);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        if (k < klo || k >= khi) continue;
+        const T g = ex[k] * e[k] * s;
+        gsum += g;
+        if (k == 0) L.acc0 += g * hr;
+        if (k == 1) L.acc1 += g * hr;
+        if (k == 2) L.acc2 += g * hr;
+    }
+    const T c = gsum * rinv3;
+    L.acc0 += dx * c;
+    L.acc1 += dy * c;
+    L.acc2 += dz * c;
+}
+
+// sum_k A2Tk(s_k) in one walk.  NS = 3: slot k holds the moments of s_k (own
+// centroids, own acceptance decisions, own kd).  NS = 1: one slot shared by
+// the three directions (s_1 = s_2 = s_3).
+template <typename T, int NS>
+__global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t(const TravParams<T> p) {
+    const int lane = threadIdx.x & 31;
+    const int64_t qi = ((int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32 + lane;
+    if (__all_sync(kFull, qi >= p.nq)) return;
+    Lane<T> L;
+    int64_t oidx;
+    T w;
+    const bool valid = load_query(p, qi, L, oidx, w);
+    const T ex[3] = {exp_t(L.q0 * T(0.5)), exp_t(L.q1 * T(0.5)), exp_t(L.q2 * T(0.5))};
+
+    const int M = (int)p.M;
+    int kd[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) kd[k] = valid ? 0 : -1;
+
+    int n = 0;
+    while (n < M) {
+        const int4 mt = __ldg(p.meta + n);
+        const int d = meta_depth(mt.w);
+        const bool leaf = meta_leaf(mt.w);
+        bool far[NS], open[NS], active[NS];
+        T gx[NS], gy[NS], gz[NS], g2[NS];
+        bool open_any = false;
+#pragma unroll
+        for (int k = 0; k < NS; k++) {
+            const Vec4<T> r0 = ld4(p.rec[k] + (int64_t)n * CAGR_REC_STRIDE);
+            gx[k] = sub_rn(L.q0, r0.x);
+            gy[k] = sub_rn(L.q1, r0.y);
+            gz[k] = sub_rn(L.q2, r0.z);
+            g2[k] = dist2_exact(gx[k], gy[k], gz[k]);
+            active[k] = d <= kd[k];
+            far[k] = g2[k] > r0.w;
+            open[k] = active[k] && !far[k];
+            if (active[k]) kd[k] = (open[k] && !leaf) ? d + 1 : d;
+            open_any = open_any || open[k];
+        }
+        const bool any_open = __any_sync(kFull, open_any);
+        // node terms, each slot with its own centroid
+#pragma unroll
+        for (int k = 0; k < NS; k++) {
+            if (active[k] && far[k]) {
+                const Vec4<T> r1 = ld4(p.rec[k] + (int64_t)n * CAGR_REC_STRIDE + 4);
+                const T e[3] = {r1.x, r1.y, r1.z};
+                a2t_term(L, ex, e, r1.w, gx[k], gy[k], gz[k], g2[k], NS == 1 ? 0 : k,
+                         NS == 1 ? 3 : k + 1);
+            }
+        }
+        if (leaf) {
+            if (any_open) {
+                const int64_t base = ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
+                for (int j = 0; j < mt.z; j++) {
+                    if (open_any) {
+                        // one point: shared position and exp factors, s_k per slot
+                        const int64_t off = base + (int64_t)j * CAGR_REC_STRIDE;
+                        const Vec4<T> s0 = ld4(p.rec[0] + off);
+                        const Vec4<T> r1 = ld4(p.rec[0] + off + 4);
+                        const T e[3] = {r1.x, r1.y, r1.z};
+                        const T px = sub_rn(L.q0, s0.x);
+                        const T py = sub_rn(L.q1, s0.y);
+                        const T pz = sub_rn(L.q2, s0.z);
+                        const T dd = dist2_exact(px, py, pz);
+                        if (NS == 1) {
+                            a2t_term(L, ex, e, r1.w, px, py, pz, dd, 0, 3);
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < NS; k++) {
+                                if (!open[k]) continue;
+                                const T s = k == 0 ? r1.w : p.rec[k][off + 7];
+                                a2t_term(L, ex, e, s, px, py, pz, dd, k, k + 1);
+                            }
+                        }
+                    }
+                }
+            }
+            n = mt.x;
+        } else {
+            n = any_open ? n + 1 : mt.x;
+        }
+    }
+
+    if (!valid) return;
+    T* o = p.out + oidx * (int64_t)p.out_stride;
+    put(o, 0, L.acc0, p.accumulate);
+    put(o, 1, L.acc1, p.accumulate);
+    put(o, 2, L.acc2, p.accumulate);
+}
+
 template <typename T, int OP>
-int launch_op(const TravParams<T>& p, int cont, cudaStream_t s) {
+int launch_op(const TravParams<T>& p, int cont, int slots, cudaStream_t s) {
     const int64_t warps = (p.nq + 31) / 32;
     const int64_t blocks = (warps + kWarps - 1) / kWarps;
     if (blocks > 0x7fffffffLL) return set_error(kErrInvalid, "too many queries");
-    if (cont)
+    if constexpr (OP == kOpA2TFused) {
+        if (slots == 3)
+            k_traverse_a2t<T, 3><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
+        else
+            k_traverse_a2t<T, 1><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
+    } else if (cont) {
         k_traverse<T, OP, true><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
-    else
+    } else {
         k_traverse<T, OP, false><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
+    }
     CAGR_CUDA(cudaGetLastError());
     return kOk;
 }
@@ -295,30 +436,41 @@ int dispatch(const Tree* t, const TraverseArgs& a, cudaStream_t s) {
     p.widths = (const T*)a.widths;
     p.width = (T)a.width;
     p.out = (T*)a.out;
-    const bool vec_in = a.op == kOpAT || a.op == kOpA2T1 || a.op == kOpA2T2 || a.op == kOpA2T3;
-    const int need_dim = vec_in ? 1 : 3;
-    const int slot = 0;
-    if (!t->rec[slot] || t->rec_dim[slot] != need_dim)
+    p.accumulate = a.accumulate;
+    const bool scalar_in = a.op == kOpAT || a.op == kOpA2T1 || a.op == kOpA2T2 ||
+                           a.op == kOpA2T3 || a.op == kOpA2TFused;
+    const int need_dim = a.op == kOpCount ? t->rec_dim[0] : (scalar_in ? 1 : 3);
+    if (!t->rec[0] || t->rec_dim[0] == 0 || t->rec_dim[0] != need_dim)
         return set_error(kErrState, "node moments of the right attribute dim are not computed");
-    p.rec = (const T*)t->rec[slot];
-    int out_dim = (a.op == kOpA || a.op == kOpA3 || a.op == kOpA21 || a.op == kOpA22 ||
-                   a.op == kOpA23)
-                      ? 1
-                      : 3;
+    for (int k = 0; k < 3; k++) p.rec[k] = (const T*)t->rec[0];
+    const int slots = (a.op == kOpA2TFused && a.slots == 3) ? 3 : 1;
+    if (slots == 3) {
+        for (int k = 1; k < 3; k++) {
+            if (!t->rec[k] || t->rec_dim[k] != 1)
+                return set_error(kErrState, "A2T sum needs scalar moments in slots 0, 1 and 2");
+            p.rec[k] = (const T*)t->rec[k];
+        }
+    }
+    const int out_dim = (a.op == kOpA || a.op == kOpA3 || a.op == kOpA21 || a.op == kOpA22 ||
+                         a.op == kOpA23 || a.op == kOpCount)
+                            ? 1
+                            : 3;
     p.out_stride = a.out_stride > 0 ? a.out_stride : out_dim;
     if (p.nq == 0) return kOk;
     switch (a.op) {
-        case kOpA: return launch_op<T, kOpA>(p, a.continuous, s);
-        case kOpAT: return launch_op<T, kOpAT>(p, 0, s);
-        case kOpA3: return launch_op<T, kOpA3>(p, a.continuous, s);
-        case kOpA21: return launch_op<T, kOpA21>(p, a.continuous, s);
-        case kOpA22: return launch_op<T, kOpA22>(p, a.continuous, s);
-        case kOpA23: return launch_op<T, kOpA23>(p, a.continuous, s);
-        case kOpA2T1: return launch_op<T, kOpA2T1>(p, 0, s);
-        case kOpA2T2: return launch_op<T, kOpA2T2>(p, 0, s);
-        case kOpA2T3: return launch_op<T, kOpA2T3>(p, 0, s);
-        case kOpG: return launch_op<T, kOpG>(p, 0, s);
-        case kOpA2Fused: return launch_op<T, kOpA2Fused>(p, a.continuous, s);
+        case kOpA: return launch_op<T, kOpA>(p, a.continuous, 1, s);
+        case kOpAT: return launch_op<T, kOpAT>(p, 0, 1, s);
+        case kOpA3: return launch_op<T, kOpA3>(p, a.continuous, 1, s);
+        case kOpA21: return launch_op<T, kOpA21>(p, a.continuous, 1, s);
+        case kOpA22: return launch_op<T, kOpA22>(p, a.continuous, 1, s);
+        case kOpA23: return launch_op<T, kOpA23>(p, a.continuous, 1, s);
+        case kOpA2T1: return launch_op<T, kOpA2T1>(p, 0, 1, s);
+        case kOpA2T2: return launch_op<T, kOpA2T2>(p, 0, 1, s);
+        case kOpA2T3: return launch_op<T, kOpA2T3>(p, 0, 1, s);
+        case kOpG: return launch_op<T, kOpG>(p, 0, 1, s);
+        case kOpA2Fused: return launch_op<T, kOpA2Fused>(p, a.continuous, 1, s);
+        case kOpA2TFused: return launch_op<T, kOpA2TFused>(p, 0, slots, s);
+        case kOpCount: return launch_op<T, kOpCount>(p, 0, 1, s);
         default: return set_error(kErrInvalid, "unknown operator " + std::to_string(a.op));
     }
 }
@@ -329,6 +481,8 @@ int traverse(const Tree* t, const TraverseArgs& a, cudaStream_t stream) {
     if (!a.out) return set_error(kErrInvalid, "output is null");
     if (a.queries && a.nq < 0) return set_error(kErrInvalid, "negative query count");
     if (!a.widths && !(a.width == a.width)) return set_error(kErrInvalid, "width is NaN");
+    if (a.qorder && !a.queries)
+        return set_error(kErrInvalid, "a query order needs explicit queries");
     return t->dtype == 0 ? dispatch<float>(t, a, stream) : dispatch<double>(t, a, stream);
 }
 

@@ -1,0 +1,151 @@
+"""Device-resident CAGR normal solve (the caller of the treecode hot path).
+
+Restates main_CAGR.py (mayueji/CAGR, CUDA-based/main_CAGR.py:40-187):
+normalise the cloud into the [-1/1.1, 1/1.1]^3 box, then 40 iterations with a
+width schedule that shrinks linearly from wsmax to wsmin (:103) -- 31
+steepest-descent-type steps (:105-118), a residual restart at i == 30
+(:119-125), 9 CG-type steps (:126-144) -- and 8 WNNC G steps (:167-174).
+Every operator application goes through the C ABI (A2k fused into one
+traversal; A2Tk as the reference composes them).  The iteration stays on the
+GPU: step lengths are device tensors, nothing is copied to the host until the
+caller asks for the result.
+
+Precision: operators in FP32 (the reference's dtype); the Krylov dot
+products and norms accumulate in FP64 (the reference uses FP32 torch sums),
+and so does the WNNC renormalisation.  This changes results only at rounding
+level; parity with the reference is stated as normal-sign agreement.
+"""
+from __future__ import annotations
+
+import dataclasses
+import time
+
+import numpy as np
+import torch
+
+from .wn_treecode import WindingNumberTreecode
+
+# main_CAGR.py:74-82
+PRESET_WIDTHS = {
+    "l0": (0.002, 0.016),
+    "l1": (0.01, 0.04),
+    "l2": (0.02, 0.08),
+    "l3": (0.03, 0.12),
+    "l4": (0.04, 0.16),
+    "l5": (0.05, 0.2),
+}
+
+
+def normalize_points(points_unnormalized: np.ndarray, bbox_scale: float = 1.1) -> np.ndarray:
+    """main_CAGR.py:42-45 (float64), then cast to float32 as :47 does."""
+    p = np.asarray(points_unnormalized, np.float64)
+    center = (p.min(0) + p.max(0)) / 2.0
+    length = (p.max(0) - p.min(0)).max()
+    return ((p - center) * (2.0 / (length * bbox_scale))).astype(np.float32)
+
+
+@dataclasses.dataclass
+class SolveResult:
+    normals: torch.Tensor          # [N, 3] float32, the solved mu (area-weighted normals)
+    residual_norm: float           # |r| after the steepest-descent phase (main_CAGR.py:165)
+    rk_norm: float                 # |rk1| after the CG phase (main_CAGR.py:166)
+    time_tree_s: float
+    time_main_s: float
+    operator_calls: int
+
+
+def _dot(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+    return (a.double() * b.double()).sum()
+
+
+def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40,
+               n_sd: int = 30, lambda0: float = 0.0, wnnc_steps: int = 8,
+               widths: torch.Tensor | None = None, max_tree_depth: int = 15,
+               tree: WindingNumberTreecode | None = None) -> SolveResult:
+    """Solve for mu on normalised float32 CUDA points [N, 3].
+
+    widths: per-point base widths (main_CAGR.py:61 uses ones); each iteration
+    uses widths * width_scale."""
+    assert wsmin <= wsmax
+    dev = points.device
+    n = points.shape[0]
+    t0 = time.perf_counter()
+    wn = tree if tree is not None else WindingNumberTreecode(points, max_tree_depth)
+    torch.cuda.synchronize(dev)
+    t1 = time.perf_counter()
+    base = torch.ones(n, device=dev) if widths is None else widths
+    normals = torch.zeros(n, 3, device=dev)
+    b3 = torch.full((n, 3), 0.5, device=dev)   # b for each of the three A2Tk calls
+    calls = 0
+
+    def A2(x, w):   # [A21 | A22 | A23](x)
+        nonlocal calls
+        calls += 3
+        return wn.forward_A2(x, w)
+
+    def A2T(v3, w):  # A2T1(v1) + A2T2(v2) + A2T3(v3)
+        nonlocal calls
+        calls += 3
+        return wn.forward_A2T_sum(v3, w)
+
+    def scale(i):
+        return wsmin + ((iters - 1 - i) / (iters - 1)) * (wsmax - wsmin)
+
+    w = base * (wsmin + 0.5 * (wsmax - wsmin))
+    rk1 = A2T(b3, w)   # main_CAGR.py:98 (overwritten at i == n_sd)
+    pk = rk1
+    r = rk1
+    for i in range(iters):
+        w = base * scale(i)
+        if i <= n_sd:
+            A_mu = -A2(normals, w)
+            AT_A_mu = A2T(A_mu.contiguous(), w)
+            r = A2T(b3, w) - AT_A_mu - lambda0 * normals
+            A_r = -A2(r.contiguous(), w).sum(1, keepdim=True)
+            alpha = (_dot(r, r) / _dot(A_r, A_r)).float()
+            normals = normals + alpha * r
+            if i == n_sd:
+                A_mu = -A2(normals, w)
+                AT_A_mu = A2T(A_mu.contiguous(), w)
+                rk1 = A2T(b3, w) - AT_A_mu - lambda0 * normals
+                pk = rk1
+        else:
+            A_pk = -A2(pk.contiguous(), w)
+            AT_A_pk = A2T(A_pk.contiguous(), w)
+            den = _dot(AT_A_pk, pk) + lambda0 * _dot(pk, pk)
+            alpha = (_dot(rk1, rk1) / den).float()
+            normals = normals + alpha * pk
+            rk20 = rk1 - alpha * AT_A_pk - alpha * lambda0 * pk
+            beta = (_dot(rk20, rk20) / _dot(rk1, rk1)).float()
+            pk = rk20 + beta * pk
+            rk1 = rk20
+    r_norm = torch.linalg.norm(r.double())
+    rk_norm = torch.linalg.norm(rk1.double())
+    # WNNC refinement at the last width (main_CAGR.py:167-174)
+    for _ in range(wnnc_steps):
+        calls += 1
+        g = wn.forward_G(normals.contiguous(), w).double()
+        g = g / torch.clamp(torch.linalg.norm(g, dim=-1, keepdim=True), min=1e-12)
+        length = torch.linalg.norm(normals.double(), dim=-1, keepdim=True)
+        normals = (g * length).float().contiguous()
+    torch.cuda.synchronize(dev)
+    t2 = time.perf_counter()
+    return SolveResult(normals, float(r_norm), float(rk_norm), t1 - t0, t2 - t1, calls)
+
+
+def orient_file(path_in: str, width_config: str = "l0", wsmin: float | None = None,
+                wsmax: float | None = None, device: str = "cuda") -> tuple[np.ndarray, SolveResult]:
+    """main_CAGR.py end to end for an .xyz/.npy file: returns [xyz, mu] rows as the
+    reference writes them (:185-186)."""
+    if path_in.endswith(".npy"):
+        raw = np.load(path_in)[:, :3]
+    else:
+        raw = np.loadtxt(path_in)[:, :3]
+    if width_config == "custom":
+        lo, hi = wsmin, wsmax
+    else:
+        lo, hi = PRESET_WIDTHS[width_config]
+    pts = torch.from_numpy(normalize_points(raw)).to(device)
+    res = cagr_solve(pts, lo, hi)
+    out = np.concatenate([raw, res.normals.cpu().numpy().astype(np.float64)], 1)
+    return out, res

@@ -162,7 +162,7 @@ class WindingNumberTreecode:
 
     def multiply(self, op: str, widths, queries: torch.Tensor | None = None,
                  query_order: torch.Tensor | None = None, continuous: bool = False,
-                 out: torch.Tensor | None = None) -> torch.Tensor:
+                 out: torch.Tensor | None = None, accumulate: bool = False) -> torch.Tensor:
         """Traversal with the moments currently in slot 0 (after ``scatter``)."""
         n = self.points.shape[0] if queries is None else queries.shape[0]
         if queries is not None:
@@ -174,11 +174,19 @@ class WindingNumberTreecode:
             query_order = query_order.contiguous()
         wt, ws = self._widths(widths, n)
         if out is None:
+            if accumulate:
+                raise RuntimeError("accumulate needs an output tensor")
             out = torch.empty(n, OUT_DIM[op], dtype=self.dtype, device=self.device)
+        elif (not out.is_cuda or out.dtype != self.dtype or out.shape[0] != n
+              or out.dim() != 2 or out.shape[1] < OUT_DIM[op] or out.stride(1) != 1):
+            raise RuntimeError(f"out must be a {self.dtype} CUDA tensor [{n}, >= {OUT_DIM[op]}] "
+                               "with unit column stride")
         with torch.cuda.device(self.device):
             check(_lib.lib().cagr_multiply(
                 self.handle, OPS[op], _ptr(queries), _ptr(query_order), n, _ptr(wt), ws,
-                int(continuous), _ptr(out), out.stride(0), _stream(self.device)),
+                (_lib.FLAG_CONTINUOUS if continuous else 0) |
+                (_lib.FLAG_ACCUMULATE if accumulate else 0),
+                _ptr(out), out.stride(0), _stream(self.device)),
                 f"cagr_multiply({op})")
         return out
 
@@ -250,20 +258,37 @@ class WindingNumberTreecode:
         return self._forward("A2_FUSED", normals, widths, continuous)
 
     def forward_A3(self, normals, widths, queries: torch.Tensor | None = None,
-                   continuous: bool = True):
-        """(A21 + A22 + A23) / 3 at `queries` (default: the points) -> [N', 1]; the
-        field operator of the GaussRecon driver (main_GaussRecon_cuda.cu:427-466),
-        which uses the continuous kernel."""
+                   continuous: bool = False):
+        """(A21 + A22 + A23) / 3 at `queries` (default: the points) -> [N', 1].
+        The pybind multiply_by_A3 never passes the continuous flag (kernel default
+        false, wn_treecode_cuda_torch_interface.cu:228-243); the GaussRecon driver's
+        field evaluation passes true (main_GaussRecon_cuda.cu:442,465)."""
         assert self.points.shape == normals.shape
         return self._forward("A3", normals, widths, continuous, queries)
 
-    def forward_A2T_sum(self, values3, widths):
-        """sum_k A2Tk(values3[:, k]) -> [N, 3]: the reference composition
-        A2T1(s1) + A2T2(s2) + A2T3(s3) (main_CAGR.py:110), three traversals with
-        each direction's own node moments."""
+    def scatter3(self, values3: torch.Tensor):
+        """Node moments of the three columns of values3 ([N, 3]) into slots 0..2."""
+        values3 = self._check_values(values3, "values")
         assert len(values3.shape) == 2 and values3.shape[1] == 3
-        out = None
-        for k, op in enumerate(("A2T1", "A2T2", "A2T3")):
-            y = self._forward(op, values3[:, k:k + 1].contiguous(), widths)
-            out = y if out is None else out.add_(y)
-        return out
+        with torch.cuda.device(self.device):
+            check(_lib.lib().cagr_scatter3(self.handle, _ptr(values3), _stream(self.device)),
+                  "cagr_scatter3")
+
+    def forward_A2T_sum(self, values3, widths, out: torch.Tensor | None = None,
+                        accumulate: bool = False):
+        """sum_k A2Tk(values3[:, k]) -> [N, 3]: the reference composition
+        A2T1(s1) + A2T2(s2) + A2T3(s3) (main_CAGR.py:110,137-139) in one
+        traversal; each direction keeps its own node moments (its own
+        |s_k|-weighted centroids and acceptance decisions)."""
+        assert len(values3.shape) == 2 and values3.shape[1] == 3
+        assert values3.shape[0] == self.points.shape[0]
+        self.scatter3(values3)
+        return self.multiply("A2T_SUM", widths, out=out, accumulate=accumulate)
+
+    def forward_A2T_shared(self, values, widths, out: torch.Tensor | None = None,
+                           accumulate: bool = False):
+        """A2T1(s) + A2T2(s) + A2T3(s) -> [N, 3] for one scalar input s [N, 1]
+        (the right-hand side term of main_CAGR.py:98,108): one set of moments."""
+        self._assert_values(values, widths)
+        self.scatter(self._check_values(values, "values"))
+        return self.multiply("A2T_SUM_SHARED", widths, out=out, accumulate=accumulate)

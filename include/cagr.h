@@ -55,7 +55,16 @@ enum { CAGR_F32 = 0, CAGR_F64 = 1 };
  *   A2T1..A2T3 :1046-1257 [N',3] sum exp(d_k/2) (d s / r^3 + e_k s / (2r))
  *   G    :1259-1322 [N',3]   sum mu / r^3 - 3 d (d.mu) / r^5
  * A2_FUSED has no reference counterpart: A21, A22, A23 from one traversal,
- * written as the three columns of an [N',3] output. */
+ * written as the three columns of an [N',3] output.
+ * A2T_SUM replaces the reference composition A2T1(s1) + A2T2(s2) + A2T3(s3)
+ * (main_CAGR.py:110,137-139) with one traversal over the moments of s_k in
+ * slot k (cagr_scatter3): every direction keeps its own |s_k|-weighted
+ * centroids and acceptance decisions, as the three reference calls do.
+ * A2T_SUM_SHARED is the same sum when s1 = s2 = s3 = s (the right-hand side
+ * A2T1(b) + A2T2(b) + A2T3(b), main_CAGR.py:108): one slot, [N',3] output.
+ * COUNT has no reference counterpart (the reference has no instrumentation):
+ * the number of pair terms (accepted nodes + near leaf points) each query
+ * sums with the moments in slot 0 -- the algorithmic work of a traversal. */
 enum {
     CAGR_OP_A = 0,
     CAGR_OP_AT = 1,
@@ -67,7 +76,16 @@ enum {
     CAGR_OP_A2T2 = 7,
     CAGR_OP_A2T3 = 8,
     CAGR_OP_G = 9,
-    CAGR_OP_A2_FUSED = 10
+    CAGR_OP_A2_FUSED = 10,
+    CAGR_OP_A2T_SUM = 11,
+    CAGR_OP_COUNT = 12,
+    CAGR_OP_A2T_SUM_SHARED = 13
+};
+
+/* cagr_multiply / cagr_forward flags. */
+enum {
+    CAGR_FLAG_CONTINUOUS = 1, /* the reference's continuous_kernel argument (A, A3, A2x) */
+    CAGR_FLAG_ACCUMULATE = 2  /* add into out_dev instead of overwriting it */
 };
 
 /* Library identification. */
@@ -113,30 +131,45 @@ int cagr_tree_morton_order(const cagr_tree* tree, int32_t* perm_dev, void* strea
 int cagr_scatter(cagr_tree* tree, int slot, const void* attrs_dev, int attr_dim,
                  const void* weights_dev, void* stream);
 
+/* Node moments of three scalar attributes at once: column k of values3_dev
+ * ([n,3], original point order) goes to slot k with weights |v_k| -- the three
+ * scatter_point_attrs_to_nodes calls the reference makes before its A2T1,
+ * A2T2 and A2T3 kernels (wn_treecode_func.py:271-351), in one launch. */
+int cagr_scatter3(cagr_tree* tree, const void* values3_dev, void* stream);
+
 /* Copies slot `slot` out in the reference layout: node_attrs [M, attr_dim],
  * reppoints [M,3], node_weights [M] (any may be NULL). */
 int cagr_scatter_export(const cagr_tree* tree, int slot, void* node_attrs_dev,
                         void* reppoints_dev, void* node_weights_dev, void* stream);
 
 /* Evaluates operator `op` with the moments in slot 0 (attr_dim 3 for
- * A/A3/A2x/G/A2_FUSED, 1 for AT/A2Tx).  Queries: queries_dev [nq,3], or NULL
+ * A/A3/A2x/G/A2_FUSED, 1 for AT/A2Tx/A2T_SUM_SHARED; slots 0..2 for
+ * A2T_SUM).  Queries: queries_dev [nq,3], or NULL
  * for the tree's own points (then nq is ignored and outputs follow the
  * original point order).  query_order_dev (int32[nq], optional) gives the
  * order in which queries are processed (Morton order is fastest); outputs
  * always land at the query's own row.  Width per query: widths_dev [nq] or,
- * when NULL, the scalar `width`.  continuous: the reference's continuous
- * kernel flag (A, A3, A2x).  out_dev: [nq, out_stride] with out_stride 0 =
+ * when NULL, the scalar `width`.  flags: CAGR_FLAG_CONTINUOUS (the
+ * reference's continuous kernel, for A, A3, A2x) and CAGR_FLAG_ACCUMULATE
+ * (sum into out_dev).  out_dev: [nq, out_stride] with out_stride 0 =
  * the operator's output width.  Replaces multiply_by_*,
  * wn_treecode_cuda_torch_interface.cu:137-777. */
 int cagr_multiply(const cagr_tree* tree, int op, const void* queries_dev,
                   const int32_t* query_order_dev, int64_t nq, const void* widths_dev,
-                  double width, int continuous, void* out_dev, int64_t out_stride, void* stream);
+                  double width, int flags, void* out_dev, int64_t out_stride, void* stream);
 
 /* One WindingNumberTreecode.forward_* call (wn_treecode_func.py:45-392):
  * node moments of values_dev ([n,3] for A/A3/A2x/G/A2_FUSED, [n,1] for
- * AT/A2Tx) into slot 0, then `op` at the tree's own points. */
+ * AT/A2Tx/A2T_SUM_SHARED; [n,3] scalar columns for A2T_SUM, via
+ * cagr_scatter3), then `op` at the tree's own points. */
 int cagr_forward(cagr_tree* tree, int op, const void* values_dev, const void* widths_dev,
-                 double width, int continuous, void* out_dev, void* stream);
+                 double width, int flags, void* out_dev, void* stream);
+
+/* Diagnostic with no counterpart in the reference: measures this GPU's FP32
+ * FMA throughput (a long chain of independent fused multiply-adds on every
+ * SM) and writes it to *gflops.  The roofline denominator for the
+ * FP32-bound traversal kernels.  Synchronises `stream`. */
+int cagr_probe_fp32_peak(int64_t iters, double* gflops, void* stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,68 @@
+"""CPU: the C ABI library loads and exports every symbol include/cagr.h declares.
+
+No compute call is made here (there is no GPU); only host-side functions
+(version, status strings, argument validation that fails before any CUDA
+call) are exercised.
+"""
+import ctypes
+import os
+
+import pytest
+
+from cagr_b200 import _lib
+from cagr_b200 import build as B
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not os.path.exists(B.LIB_PATH):
+        B.build()
+    return _lib.lib()
+
+
+def test_header_declares_the_boundary():
+    names = _lib.header_symbols()
+    for expected in ("cagr_tree_build", "cagr_tree_destroy", "cagr_tree_export",
+                     "cagr_scatter", "cagr_multiply", "cagr_forward"):
+        assert expected in names
+
+
+def test_every_declared_symbol_is_exported(lib):
+    missing = [n for n in _lib.header_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_the_header():
+    declared = set(_lib.header_symbols())
+    bound = set(_lib._SIGNATURES)
+    assert declared == bound, (declared ^ bound)
+
+
+def test_version_and_status_strings(lib):
+    assert lib.cagr_version() >= 100
+    assert lib.cagr_status_string(0) == b"ok"
+    assert lib.cagr_status_string(1) == b"invalid argument"
+    assert lib.cagr_status_string(99) == b"unknown status"
+
+
+def test_invalid_arguments_fail_before_touching_the_device(lib):
+    h = ctypes.c_void_p()
+    assert lib.cagr_tree_build(None, 10, 0, 15, 1, None, ctypes.byref(h)) == 1
+    assert b"null" in lib.cagr_last_error()
+    assert lib.cagr_tree_build(ctypes.c_void_p(16), 0, 0, 15, 1, None, ctypes.byref(h)) == 1
+    assert lib.cagr_tree_build(ctypes.c_void_p(16), 10, 0, 22, 1, None, ctypes.byref(h)) == 1
+    assert b"max_depth" in lib.cagr_last_error()
+    assert lib.cagr_tree_build(ctypes.c_void_p(16), 10, 7, 15, 1, None, ctypes.byref(h)) == 1
+    assert lib.cagr_multiply(None, 3, None, None, 0, None, 0.01, 0, None, 0, None) == 1
+    assert lib.cagr_tree_destroy(None) == 0
+
+
+def test_no_cpu_fallback_in_the_product():
+    """The product package never imports the oracle."""
+    import cagr_b200
+    pkg = os.path.dirname(cagr_b200.__file__)
+    for root, _, files in os.walk(pkg):
+        for f in files:
+            if f.endswith(".py"):
+                text = open(os.path.join(root, f)).read()
+                assert "import oracle" not in text and "from oracle" not in text, f

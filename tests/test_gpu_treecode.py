@@ -161,6 +161,54 @@ def test_a2t_sum_matches_reference_composition(cuda_lib, oracle):
     assert l2 <= 2e-5 and mx <= 2e-4, (l2, mx)
 
 
+def test_a2t_shared_matches_reference_composition(cuda_lib, oracle):
+    """A2T1(b) + A2T2(b) + A2T3(b) with one input (the solve's right-hand side)."""
+    torch = _torch()
+    pts = sphere_cloud(3000, seed=25)
+    b = random_values(len(pts), 1, seed=26)
+    w = np.full(len(pts), 0.01, np.float32)
+    tr = oracle.build_tree(pts)
+    ref = sum(oracle.forward(op, tr, pts, b, w) for op in ("A2T1", "A2T2", "A2T3"))
+    wn = _tree(pts)
+    got = wn.forward_A2T_shared(torch.from_numpy(b).cuda(), 0.01).cpu().numpy()
+    l2, mx = rel_errors(got, ref)
+    assert l2 <= 2e-5 and mx <= 2e-4, (l2, mx)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_three_slot_moments_bit_exact(cuda_lib, oracle, dtype):
+    torch = _torch()
+    from oracle.oracle import point_weights
+    pts = edge_cloud(dtype=dtype)
+    wn = _tree(pts)
+    tr = oracle.build_tree(pts)
+    s = random_values(len(pts), 3, seed=27, dtype=dtype)
+    s[::5, 1] = 0
+    wn.scatter3(torch.from_numpy(s).cuda())
+    for k in range(3):
+        col = np.ascontiguousarray(s[:, k:k + 1])
+        mom = oracle.moments(tr, pts, point_weights(col), col)
+        a, r, w = (t.cpu().numpy() for t in wn.scatter_export(k, 1))
+        assert np.array_equal(w, mom.weights) and np.array_equal(r, mom.rep)
+        assert np.array_equal(a, mom.attrs)
+
+
+def test_pair_term_counts_match_oracle(cuda_lib, oracle):
+    """COUNT reproduces the reference traversal's term count per query."""
+    torch = _torch()
+    from oracle.oracle import point_weights
+    pts = sphere_cloud(4000, seed=28)
+    mu = smooth_normals(pts, seed=29)
+    w = np.full(len(pts), 0.01, np.float32)
+    tr = oracle.build_tree(pts)
+    mom = oracle.moments(tr, pts, point_weights(mu), mu)
+    _, terms, _ = oracle.multiply("A21", pts, w, pts, mu, tr, mom, counts=True)
+    wn = _tree(pts)
+    wn.scatter(torch.from_numpy(mu).cuda())
+    got = wn.multiply("COUNT", 0.01).cpu().numpy()[:, 0]
+    assert np.array_equal(got.astype(np.int64), terms)
+
+
 def test_errors_are_raised(cuda_lib):
     torch = _torch()
     from cagr_b200 import WindingNumberTreecode
