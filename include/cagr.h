@@ -165,6 +165,27 @@ int cagr_multiply(const cagr_tree* tree, int op, const void* queries_dev,
 int cagr_forward(cagr_tree* tree, int op, const void* values_dev, const void* widths_dev,
                  double width, int flags, void* out_dev, void* stream);
 
+/* No counterpart in the reference.  Node moments (the outputs of
+ * cagr_scatter_export) computed from tree arrays in the reference layout
+ * (parent, children, is_leaf, npts, n2p, n2p_start as cagr_tree_export
+ * writes them; num_nodes = M) WITHOUT ANY DEVICE ALLOCATION, for callers that
+ * cannot allocate at this point (inside a CUDA-graph capture, under a fixed
+ * memory budget owned by another allocator, or holding only the reference
+ * arrays and no tree handle).  Inputs (points [n,3], weights [n] or NULL for
+ * |attr|, attrs [n, attr_dim]) and outputs (node_attrs [M, attr_dim],
+ * reppoints [M,3], node_weights [M]) are the caller's; dtype CAGR_F32 or
+ * CAGR_F64.  The per-node scratch lives in one fixed device array of
+ * 2,097,152 nodes (8 MiB, held by every GPU that loads the library until
+ * exit); larger trees return CAGR_ERR_INVALID.  All calls share that array:
+ * calls that overlap on the GPU race, so order them on one stream.  The first
+ * call on a device looks the array up; make it before any stream capture. */
+int cagr_scatter_noalloc(const int64_t* parent_dev, const int64_t* children_dev,
+                         const uint8_t* is_leaf_dev, const int64_t* npts_dev,
+                         const int64_t* n2p_dev, const int64_t* n2p_start_dev, int64_t num_nodes,
+                         int dtype, const void* points_dev, const void* weights_dev,
+                         const void* attrs_dev, int attr_dim, void* node_attrs_dev,
+                         void* reppoints_dev, void* node_weights_dev, void* stream);
+
 /* Diagnostic with no counterpart in the reference: measures this GPU's FP32
  * FMA throughput (a long chain of independent fused multiply-adds on every
  * SM) and writes it to *gflops.  The roofline denominator for the
