@@ -75,7 +75,7 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
     t1 = time.perf_counter()
     base = torch.ones(n, device=dev) if widths is None else widths
     normals = torch.zeros(n, 3, device=dev)
-    b3 = torch.full((n, 3), 0.5, device=dev)   # b for each of the three A2Tk calls
+    b = torch.full((n, 1), 0.5, device=dev)   # main_CAGR.py:50
     calls = 0
 
     def A2(x, w):   # [A21 | A22 | A23](x)
@@ -88,11 +88,16 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
         calls += 3
         return wn.forward_A2T_sum(v3, w)
 
+    def A2Tb(w):     # A2T1(b) + A2T2(b) + A2T3(b): one input, one set of moments
+        nonlocal calls
+        calls += 3
+        return wn.forward_A2T_shared(b, w)
+
     def scale(i):
         return wsmin + ((iters - 1 - i) / (iters - 1)) * (wsmax - wsmin)
 
     w = base * (wsmin + 0.5 * (wsmax - wsmin))
-    rk1 = A2T(b3, w)   # main_CAGR.py:98 (overwritten at i == n_sd)
+    rk1 = A2Tb(w)   # main_CAGR.py:98 (overwritten at i == n_sd)
     pk = rk1
     r = rk1
     for i in range(iters):
@@ -100,14 +105,14 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
         if i <= n_sd:
             A_mu = -A2(normals, w)
             AT_A_mu = A2T(A_mu.contiguous(), w)
-            r = A2T(b3, w) - AT_A_mu - lambda0 * normals
+            r = A2Tb(w) - AT_A_mu - lambda0 * normals
             A_r = -A2(r.contiguous(), w).sum(1, keepdim=True)
             alpha = (_dot(r, r) / _dot(A_r, A_r)).float()
             normals = normals + alpha * r
             if i == n_sd:
                 A_mu = -A2(normals, w)
                 AT_A_mu = A2T(A_mu.contiguous(), w)
-                rk1 = A2T(b3, w) - AT_A_mu - lambda0 * normals
+                rk1 = A2Tb(w) - AT_A_mu - lambda0 * normals
                 pk = rk1
         else:
             A_pk = -A2(pk.contiguous(), w)
