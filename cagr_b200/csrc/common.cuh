@@ -4,8 +4,9 @@
 // exactly as the reference serialiser numbers them):
 //   perm[N]        int32  Morton-sorted position -> original point index
 //   meta[M]        int4   {next (preorder skip pointer), pstart (first sorted
-//                          position covered), npts (points under the node),
-//                          depth | is_leaf << 8 | nchild << 16}
+//                          position covered), npts (points under the node,
+//                          negated for a leaf), depth}
+//   nchild[M]      uint8  number of children
 //   parent[M]      int32  parent id (-1 for the root)
 //   children[M*8]  int32  child ids in octant order (-1 = none)
 //   leaf_ids[NL]   int32  leaf node ids in preorder
@@ -39,9 +40,9 @@ enum Status : int {
     kErrState = 5,
 };
 
-__host__ __device__ inline int meta_depth(int w) { return w & 0xff; }
-__host__ __device__ inline bool meta_leaf(int w) { return (w >> 8) & 1; }
-__host__ __device__ inline int meta_nchild(int w) { return (w >> 16) & 0xff; }
+__host__ __device__ inline bool node_leaf(const int4& m) { return m.z < 0; }
+__host__ __device__ inline int node_npts(const int4& m) { return m.z < 0 ? -m.z : m.z; }
+__host__ __device__ inline int node_depth(const int4& m) { return m.w; }
 
 // 4-vector of T and aligned loads of one record component.
 template <typename T>
@@ -134,6 +135,14 @@ __device__ __forceinline__ T width_threshold(T w) {
 template <typename T>
 __host__ __device__ __forceinline__ T mac_radius2(int depth) {
     return T(16.0) * ldexp(T(1.0), -2 * depth);
+}
+// The same power of two, 2^(4 - 2 depth), built directly from its exponent
+// field (valid for depth <= CAGR_MAX_DEPTH): two integer instructions.
+__device__ __forceinline__ float mac_radius2_bits(int depth, float) {
+    return __int_as_float((131 - 2 * depth) << 23);
+}
+__device__ __forceinline__ double mac_radius2_bits(int depth, double) {
+    return __longlong_as_double((long long)(1027 - 2 * depth) << 52);
 }
 
 }  // namespace cagr

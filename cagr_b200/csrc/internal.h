@@ -38,6 +38,7 @@ struct Tree {
     int32_t* perm = nullptr;       // [N] sorted position -> original index
     int32_t* invperm = nullptr;    // [N] original index -> sorted position
     int4* meta = nullptr;          // [M]
+    uint8_t* nchild = nullptr;     // [M]
     int32_t* parent = nullptr;     // [M]
     int32_t* children = nullptr;   // [M*8], -1 = none
     int32_t* leaf_ids = nullptr;   // [num_leaves]
@@ -47,6 +48,12 @@ struct Tree {
     uint32_t* counters = nullptr;  // [M], zero between moment passes
     void* rec[3] = {nullptr, nullptr, nullptr};  // [(M+N)*CAGR_REC_STRIDE] T per slot
     int rec_dim[3] = {0, 0, 0};    // attribute dim the slot was filled with (0 = empty)
+    // Packed records of the three-slot adjoint (written with slots 0..2 by moments3):
+    //   node  [M*12]: for k = 0..2  (c_k.x, c_k.y, c_k.z, exp(-c_k[k]/2) * s_k)
+    //   point [N*8] : (y.x, y.y, y.z, e_0 s_0), (e_1 s_1, e_2 s_2, 0, 0),  e_k = exp(-y_k/2)
+    void* adj_nodes = nullptr;
+    void* adj_points = nullptr;
+    bool adj_valid = false;
 };
 
 int tree_build(const void* points, int64_t n, int dtype, int max_depth, int leaf_size,

@@ -56,6 +56,7 @@ struct MomParams {
     int64_t num_leaves = 0, M = 0;
     const int32_t* leaf_ids = nullptr;
     const int4* meta = nullptr;
+    const uint8_t* nchild = nullptr;
     const int32_t* parent = nullptr;
     const int32_t* children = nullptr;
     const int32_t* perm = nullptr;
@@ -68,6 +69,8 @@ struct MomParams {
     const T* weights = nullptr;  // NS == 1 only; null = |attr|
     uint32_t* counters = nullptr;
     T* rec[NS];
+    T* adjn = nullptr;  // NS == 3: packed adjoint node records [M*12]
+    T* adjp = nullptr;  // NS == 3: packed adjoint point records [N*8]
 };
 
 template <typename T, int DIM, int NS>
@@ -77,7 +80,7 @@ __global__ void __launch_bounds__(kBlock) k_moments(const MomParams<T, DIM, NS> 
     const int64_t M = p.M;
     int node = p.leaf_ids[li];
     const int4 lm = p.meta[node];
-    const int pstart = lm.y, np = lm.z;
+    const int pstart = lm.y, np = node_npts(lm);
 
     // point records for the leaf's Morton range
     for (int j = 0; j < np; j++) {
@@ -86,6 +89,7 @@ __global__ void __launch_bounds__(kBlock) k_moments(const MomParams<T, DIM, NS> 
         const T pos[3] = {p.spos[3 * s], p.spos[3 * s + 1], p.spos[3 * s + 2]};
         T e[3];
         exps(pos, e);
+        T es[3] = {T(0), T(0), T(0)};
 #pragma unroll
         for (int k = 0; k < NS; k++) {
             T a[3] = {T(0), T(0), T(0)};
@@ -93,6 +97,11 @@ __global__ void __launch_bounds__(kBlock) k_moments(const MomParams<T, DIM, NS> 
             for (int c = 0; c < DIM; c++) a[c] = p.attrs[(int64_t)pt * p.astride + k * DIM + c];
             const T w = (NS == 1 && p.weights) ? p.weights[pt] : weight_of(a, DIM);
             write_record<T, DIM>(p.rec[k] + (M + s) * CAGR_REC_STRIDE, pos, e, a, w, T(0));
+            es[k] = e[k] * a[0];
+        }
+        if constexpr (NS == 3) {
+            st4<T>(p.adjp + (int64_t)s * 8, make4(pos[0], pos[1], pos[2], es[0]));
+            st4<T>(p.adjp + (int64_t)s * 8 + 4, make4(es[1], es[2], T(0), T(0)));
         }
     }
 
@@ -127,7 +136,7 @@ __global__ void __launch_bounds__(kBlock) k_moments(const MomParams<T, DIM, NS> 
     }
 
     int count = np;          // points under `node`: the zero-weight centroid divides by it
-    int depth = meta_depth(lm.w);
+    int depth = node_depth(lm);
     while (true) {
 #pragma unroll
         for (int k = 0; k < NS; k++) {
@@ -144,6 +153,8 @@ __global__ void __launch_bounds__(kBlock) k_moments(const MomParams<T, DIM, NS> 
             exps(c, e);
             write_record<T, DIM>(p.rec[k] + (int64_t)node * CAGR_REC_STRIDE, c, e, A[k], W[k],
                                  mac_radius2<T>(depth));
+            if constexpr (NS == 3)
+                st4<T>(p.adjn + (int64_t)node * 12 + 4 * k, make4(c[0], c[1], c[2], e[k] * A[k][0]));
         }
         if (node == 0) return;
         // publish this node, then arrive at the parent
@@ -151,12 +162,12 @@ __global__ void __launch_bounds__(kBlock) k_moments(const MomParams<T, DIM, NS> 
         const int par = p.parent[node];
         const int4 pm = p.meta[par];
         const uint32_t arrived = atomicAdd(&p.counters[par], 1u);
-        if (arrived + 1u != (uint32_t)meta_nchild(pm.w)) return;
+        if (arrived + 1u != (uint32_t)p.nchild[par]) return;
         p.counters[par] = 0u;  // every child has arrived: ready for the next pass
         __threadfence();
         node = par;
-        count = pm.z;
-        depth = meta_depth(pm.w);
+        count = node_npts(pm);
+        depth = node_depth(pm);
 #pragma unroll
         for (int k = 0; k < NS; k++) {
             W[k] = T(0);
@@ -220,6 +231,7 @@ MomParams<T, DIM, NS> params(Tree* t, const void* attrs, int astride, const void
     p.M = t->m;
     p.leaf_ids = t->leaf_ids;
     p.meta = t->meta;
+    p.nchild = t->nchild;
     p.parent = t->parent;
     p.children = t->children;
     p.perm = t->perm;
@@ -257,12 +269,21 @@ template <typename T>
 int launch_moments3(Tree* t, const void* values3, cudaStream_t s) {
     for (int k = 0; k < 3; k++)
         if (int rc = ensure_slot(t, k, sizeof(T))) return rc;
+    if (!t->adj_nodes) {
+        cudaError_t e = cudaMalloc(&t->adj_nodes, sizeof(T) * 12 * (size_t)t->m);
+        if (e == cudaSuccess) e = cudaMalloc(&t->adj_points, sizeof(T) * 8 * (size_t)t->n);
+        if (e != cudaSuccess)
+            return set_error(kErrAlloc, std::string("adjoint records: ") + cudaGetErrorString(e));
+    }
     const unsigned grid = (unsigned)((t->num_leaves + kBlock - 1) / kBlock);
     auto p = params<T, 1, 3>(t, values3, 3, nullptr);
     for (int k = 0; k < 3; k++) p.rec[k] = (T*)t->rec[k];
+    p.adjn = (T*)t->adj_nodes;
+    p.adjp = (T*)t->adj_points;
     k_moments<T, 1, 3><<<grid, kBlock, 0, s>>>(p);
     CAGR_CUDA(cudaGetLastError());
     for (int k = 0; k < 3; k++) t->rec_dim[k] = 1;
+    t->adj_valid = true;
     return kOk;
 }
 
@@ -273,6 +294,7 @@ int moments(Tree* t, int slot, const void* attrs, int dim, const void* weights,
     if (slot < 0 || slot > 2) return set_error(kErrInvalid, "moment slot must be 0, 1 or 2");
     if (dim != 1 && dim != 3) return set_error(kErrInvalid, "attribute dim must be 1 or 3");
     if (!attrs) return set_error(kErrInvalid, "attrs is null");
+    t->adj_valid = false;  // a single-slot pass overwrites one of the adjoint's slots
     return t->dtype == 0 ? launch_moments<float>(t, slot, attrs, dim, weights, stream)
                          : launch_moments<double>(t, slot, attrs, dim, weights, stream);
 }

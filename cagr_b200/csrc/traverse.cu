@@ -47,6 +47,8 @@ struct TravParams {
     int64_t M = 0, N = 0, nq = 0;
     const int4* meta = nullptr;
     const T* rec[3] = {nullptr, nullptr, nullptr};
+    const T* adjn = nullptr;   // packed adjoint records (k_traverse_a2t3)
+    const T* adjp = nullptr;
     const T* spos = nullptr;   // sorted tree points (queries == points)
     const int32_t* perm = nullptr;
     const T* queries = nullptr;
@@ -201,8 +203,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p)
     int n = 0;
     while (n < M) {
         const int4 mt = __ldg(p.meta + n);
-        const int d = meta_depth(mt.w);
-        const bool leaf = meta_leaf(mt.w);
+        const int d = node_depth(mt);
+        const bool leaf = node_leaf(mt);
         const T* r = rec + (int64_t)n * CAGR_REC_STRIDE;
         const Vec4<T> r0 = ld4(r);  // (cx, cy, cz, (4 half_w)^2)
         T dx = sub_rn(L.q0, r0.x);
@@ -214,26 +216,23 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p)
         const bool open = active && !far;
         if (active) kd = (open && !leaf) ? d + 1 : d;
         const bool any_open = __any_sync(kFull, open);
-        if (leaf && mt.z == 1) {
-            // single-point leaf: far lanes take the node term, near lanes the point
-            const T* src = r;
-            if (open) {
-                src = rec + ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
-                const Vec4<T> s0 = ld4(src);
-                dx = sub_rn(L.q0, s0.x);
-                dy = sub_rn(L.q1, s0.y);
-                dz = sub_rn(L.q2, s0.z);
-                d2 = dist2_exact(dx, dy, dz);
-            }
-            if (active) pair_term<T, OP, CONT>(L, src, dx, dy, dz, d2);
-            n = mt.x;
-            continue;
+        // one term per active lane: far lanes the node term, near lanes at a leaf
+        // its first point (the rest of a multi-point leaf follows below)
+        const T* src = r;
+        if (leaf && open) {
+            src = rec + ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
+            const Vec4<T> s0 = ld4(src);
+            dx = sub_rn(L.q0, s0.x);
+            dy = sub_rn(L.q1, s0.y);
+            dz = sub_rn(L.q2, s0.z);
+            d2 = dist2_exact(dx, dy, dz);
         }
-        if (active && far) pair_term<T, OP, CONT>(L, r, dx, dy, dz, d2);
+        if (active && (far || leaf)) pair_term<T, OP, CONT>(L, src, dx, dy, dz, d2);
         if (leaf) {
-            if (any_open) {
-                const T* pr = rec + ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
-                for (int j = 0; j < mt.z; j++, pr += CAGR_REC_STRIDE) {
+            const int np = -mt.z;
+            if (np > 1 && any_open) {
+                const T* pr = rec + ((int64_t)M + mt.y + 1) * CAGR_REC_STRIDE;
+                for (int j = 1; j < np; j++, pr += CAGR_REC_STRIDE) {
                     if (open) {
                         const Vec4<T> s0 = ld4(pr);
                         const T ex = sub_rn(L.q0, s0.x);
@@ -312,11 +311,11 @@ __device__ __forceinline__ void a2t_term(Lane<T>& L, const T* ex, const T* e, T 
     L.acc2 += dz * c;
 }
 
-// sum_k A2Tk(s_k) in one walk.  NS = 3: slot k holds the moments of s_k (own
-// centroids, own acceptance decisions, own kd).  NS = 1: one slot shared by
-// the three directions (s_1 = s_2 = s_3).
-template <typename T, int NS>
-__global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t(const TravParams<T> p) {
+// A2T1(s) + A2T2(s) + A2T3(s) in one walk for ONE input s (one slot, the three
+// directions share its centroids and acceptance decisions): the solve's
+// right-hand side A2T(b) (main_CAGR.py:98,108).
+template <typename T>
+__global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t_shared(const TravParams<T> p) {
     const int lane = threadIdx.x & 31;
     const int64_t qi = ((int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32 + lane;
     if (__all_sync(kFull, qi >= p.nq)) return;
@@ -325,68 +324,52 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t(const TravParams<T
     T w;
     const bool valid = load_query(p, qi, L, oidx, w);
     const T ex[3] = {exp_t(L.q0 * T(0.5)), exp_t(L.q1 * T(0.5)), exp_t(L.q2 * T(0.5))};
-
     const int M = (int)p.M;
-    int kd[NS];
-#pragma unroll
-    for (int k = 0; k < NS; k++) kd[k] = valid ? 0 : -1;
-
+    const T* __restrict__ rec = p.rec[0];
+    int kd = valid ? 0 : -1;
     int n = 0;
     while (n < M) {
         const int4 mt = __ldg(p.meta + n);
-        const int d = meta_depth(mt.w);
-        const bool leaf = meta_leaf(mt.w);
-        bool far[NS], open[NS], active[NS];
-        T gx[NS], gy[NS], gz[NS], g2[NS];
-        bool open_any = false;
-#pragma unroll
-        for (int k = 0; k < NS; k++) {
-            const Vec4<T> r0 = ld4(p.rec[k] + (int64_t)n * CAGR_REC_STRIDE);
-            gx[k] = sub_rn(L.q0, r0.x);
-            gy[k] = sub_rn(L.q1, r0.y);
-            gz[k] = sub_rn(L.q2, r0.z);
-            g2[k] = dist2_exact(gx[k], gy[k], gz[k]);
-            active[k] = d <= kd[k];
-            far[k] = g2[k] > r0.w;
-            open[k] = active[k] && !far[k];
-            if (active[k]) kd[k] = (open[k] && !leaf) ? d + 1 : d;
-            open_any = open_any || open[k];
+        const int d = node_depth(mt);
+        const bool leaf = node_leaf(mt);
+        const T* r = rec + (int64_t)n * CAGR_REC_STRIDE;
+        const Vec4<T> r0 = ld4(r);
+        T dx = sub_rn(L.q0, r0.x);
+        T dy = sub_rn(L.q1, r0.y);
+        T dz = sub_rn(L.q2, r0.z);
+        T d2 = dist2_exact(dx, dy, dz);
+        const bool active = d <= kd;
+        const bool far = d2 > r0.w;
+        const bool open = active && !far;
+        if (active) kd = (open && !leaf) ? d + 1 : d;
+        const bool any_open = __any_sync(kFull, open);
+        const T* src = r;
+        if (leaf && open) {
+            src = rec + ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
+            const Vec4<T> s0 = ld4(src);
+            dx = sub_rn(L.q0, s0.x);
+            dy = sub_rn(L.q1, s0.y);
+            dz = sub_rn(L.q2, s0.z);
+            d2 = dist2_exact(dx, dy, dz);
         }
-        const bool any_open = __any_sync(kFull, open_any);
-        // node terms, each slot with its own centroid
-#pragma unroll
-        for (int k = 0; k < NS; k++) {
-            if (active[k] && far[k]) {
-                const Vec4<T> r1 = ld4(p.rec[k] + (int64_t)n * CAGR_REC_STRIDE + 4);
-                const T e[3] = {r1.x, r1.y, r1.z};
-                a2t_term(L, ex, e, r1.w, gx[k], gy[k], gz[k], g2[k], NS == 1 ? 0 : k,
-                         NS == 1 ? 3 : k + 1);
-            }
+        if (active && (far || leaf)) {
+            const Vec4<T> r1 = ld4(src + 4);  // (e1, e2, e3, s)
+            const T e[3] = {r1.x, r1.y, r1.z};
+            a2t_term(L, ex, e, r1.w, dx, dy, dz, d2, 0, 3);
         }
         if (leaf) {
-            if (any_open) {
-                const int64_t base = ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
-                for (int j = 0; j < mt.z; j++) {
-                    if (open_any) {
-                        // one point: shared position and exp factors, s_k per slot
-                        const int64_t off = base + (int64_t)j * CAGR_REC_STRIDE;
-                        const Vec4<T> s0 = ld4(p.rec[0] + off);
-                        const Vec4<T> r1 = ld4(p.rec[0] + off + 4);
+            const int np = -mt.z;
+            if (np > 1 && any_open) {
+                const T* pr = rec + ((int64_t)M + mt.y + 1) * CAGR_REC_STRIDE;
+                for (int j = 1; j < np; j++, pr += CAGR_REC_STRIDE) {
+                    if (open) {
+                        const Vec4<T> s0 = ld4(pr);
+                        const Vec4<T> r1 = ld4(pr + 4);
                         const T e[3] = {r1.x, r1.y, r1.z};
                         const T px = sub_rn(L.q0, s0.x);
                         const T py = sub_rn(L.q1, s0.y);
                         const T pz = sub_rn(L.q2, s0.z);
-                        const T dd = dist2_exact(px, py, pz);
-                        if (NS == 1) {
-                            a2t_term(L, ex, e, r1.w, px, py, pz, dd, 0, 3);
-                        } else {
-#pragma unroll
-                            for (int k = 0; k < NS; k++) {
-                                if (!open[k]) continue;
-                                const T s = k == 0 ? r1.w : p.rec[k][off + 7];
-                                a2t_term(L, ex, e, s, px, py, pz, dd, k, k + 1);
-                            }
-                        }
+                        a2t_term(L, ex, e, r1.w, px, py, pz, dist2_exact(px, py, pz), 0, 3);
                     }
                 }
             }
@@ -395,7 +378,116 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t(const TravParams<T
             n = any_open ? n + 1 : mt.x;
         }
     }
+    if (!valid) return;
+    T* o = p.out + oidx * (int64_t)p.out_stride;
+    put(o, 0, L.acc0, p.accumulate);
+    put(o, 1, L.acc1, p.accumulate);
+    put(o, 2, L.acc2, p.accumulate);
+}
 
+// One direction-K A2T term with g = exp(x_K/2) exp(-y_K/2) s (premultiplied):
+//   acc += g (d / r^3 + e_K / (2r)).
+template <typename T, int K>
+__device__ __forceinline__ void a2t_term1(Lane<T>& L, T g, T dx, T dy, T dz, T d2) {
+    const bool outside = d2 >= L.tw;
+    const T rinv = outside ? rsqrt_t(d2) : T(0);
+    const T c = g * (rinv * rinv * rinv);
+    L.acc0 += dx * c;
+    L.acc1 += dy * c;
+    L.acc2 += dz * c;
+    const T h = g * T(0.5) * rinv;
+    if constexpr (K == 0) L.acc0 += h;
+    if constexpr (K == 1) L.acc1 += h;
+    if constexpr (K == 2) L.acc2 += h;
+}
+
+// Slot K of the three-slot adjoint walk: acceptance test against the slot's
+// own centroid and the lane's own active depth kd.
+template <typename T>
+struct SlotTest {
+    T dx, dy, dz, d2;
+    bool active, far, open;
+};
+template <typename T>
+__device__ __forceinline__ SlotTest<T> slot_test(const Lane<T>& L, const Vec4<T>& c, T R2, int d,
+                                                 bool leaf, int& kd) {
+    SlotTest<T> s;
+    s.dx = sub_rn(L.q0, c.x);
+    s.dy = sub_rn(L.q1, c.y);
+    s.dz = sub_rn(L.q2, c.z);
+    s.d2 = dist2_exact(s.dx, s.dy, s.dz);
+    s.active = d <= kd;
+    s.far = s.d2 > R2;
+    s.open = s.active && !s.far;
+    if (s.active) kd = (s.open && !leaf) ? d + 1 : d;
+    return s;
+}
+
+// sum_k A2Tk(s_k) in one walk over the packed adjoint records (Tree::adj_*):
+// slot k holds the moments of s_k with its own |s_k|-weighted centroids, hence
+// its own acceptance decisions, tracked by its own kd -- the three reference
+// calls A2T1(s1), A2T2(s2), A2T3(s3) with their own scatters.  A near point's
+// geometry is shared by the three directions.
+template <typename T>
+__global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t3(const TravParams<T> p) {
+    const int lane = threadIdx.x & 31;
+    const int64_t qi = ((int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32 + lane;
+    if (__all_sync(kFull, qi >= p.nq)) return;
+    Lane<T> L;
+    int64_t oidx;
+    T w;
+    const bool valid = load_query(p, qi, L, oidx, w);
+    const T ex0 = exp_t(L.q0 * T(0.5)), ex1 = exp_t(L.q1 * T(0.5)), ex2 = exp_t(L.q2 * T(0.5));
+    const int M = (int)p.M;
+    const T* __restrict__ an = p.adjn;
+    const T* __restrict__ ap = p.adjp;
+    int kd0 = valid ? 0 : -1, kd1 = kd0, kd2 = kd0;
+    int n = 0;
+    while (n < M) {
+        const int4 mt = __ldg(p.meta + n);
+        const int d = node_depth(mt);
+        const bool leaf = node_leaf(mt);
+        const T R2 = mac_radius2_bits(d, T(0));
+        const T* q = an + (int64_t)n * 12;
+        const Vec4<T> c0 = ld4(q), c1 = ld4(q + 4), c2 = ld4(q + 8);
+        const SlotTest<T> s0 = slot_test(L, c0, R2, d, leaf, kd0);
+        const SlotTest<T> s1 = slot_test(L, c1, R2, d, leaf, kd1);
+        const SlotTest<T> s2 = slot_test(L, c2, R2, d, leaf, kd2);
+        const bool open_any = s0.open || s1.open || s2.open;
+        const bool any_open = __any_sync(kFull, open_any);
+        if (s0.active && s0.far) a2t_term1<T, 0>(L, ex0 * c0.w, s0.dx, s0.dy, s0.dz, s0.d2);
+        if (s1.active && s1.far) a2t_term1<T, 1>(L, ex1 * c1.w, s1.dx, s1.dy, s1.dz, s1.d2);
+        if (s2.active && s2.far) a2t_term1<T, 2>(L, ex2 * c2.w, s2.dx, s2.dy, s2.dz, s2.d2);
+        if (leaf) {
+            if (any_open) {
+                const int np = -mt.z;
+                const T* pp = ap + (int64_t)mt.y * 8;
+                for (int j = 0; j < np; j++, pp += 8) {
+                    if (open_any) {
+                        const Vec4<T> P0 = ld4(pp);      // (y, e_0 s_0)
+                        const Vec4<T> P1 = ld4(pp + 4);  // (e_1 s_1, e_2 s_2, 0, 0)
+                        const T px = sub_rn(L.q0, P0.x);
+                        const T py = sub_rn(L.q1, P0.y);
+                        const T pz = sub_rn(L.q2, P0.z);
+                        const T dd = dist2_exact(px, py, pz);
+                        const bool outside = dd >= L.tw;
+                        const T rinv = outside ? rsqrt_t(dd) : T(0);
+                        const T hr = T(0.5) * rinv;
+                        const T g0 = s0.open ? ex0 * P0.w : T(0);
+                        const T g1 = s1.open ? ex1 * P1.x : T(0);
+                        const T g2 = s2.open ? ex2 * P1.y : T(0);
+                        const T c = (g0 + g1 + g2) * (rinv * rinv * rinv);
+                        L.acc0 += px * c + g0 * hr;
+                        L.acc1 += py * c + g1 * hr;
+                        L.acc2 += pz * c + g2 * hr;
+                    }
+                }
+            }
+            n = mt.x;
+        } else {
+            n = any_open ? n + 1 : mt.x;
+        }
+    }
     if (!valid) return;
     T* o = p.out + oidx * (int64_t)p.out_stride;
     put(o, 0, L.acc0, p.accumulate);
@@ -410,9 +502,9 @@ int launch_op(const TravParams<T>& p, int cont, int slots, cudaStream_t s) {
     if (blocks > 0x7fffffffLL) return set_error(kErrInvalid, "too many queries");
     if constexpr (OP == kOpA2TFused) {
         if (slots == 3)
-            k_traverse_a2t<T, 3><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
+            k_traverse_a2t3<T><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
         else
-            k_traverse_a2t<T, 1><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
+            k_traverse_a2t_shared<T><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
     } else if (cont) {
         k_traverse<T, OP, true><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
     } else {
@@ -445,11 +537,10 @@ int dispatch(const Tree* t, const TraverseArgs& a, cudaStream_t s) {
     for (int k = 0; k < 3; k++) p.rec[k] = (const T*)t->rec[0];
     const int slots = (a.op == kOpA2TFused && a.slots == 3) ? 3 : 1;
     if (slots == 3) {
-        for (int k = 1; k < 3; k++) {
-            if (!t->rec[k] || t->rec_dim[k] != 1)
-                return set_error(kErrState, "A2T sum needs scalar moments in slots 0, 1 and 2");
-            p.rec[k] = (const T*)t->rec[k];
-        }
+        if (!t->adj_valid || !t->adj_nodes)
+            return set_error(kErrState, "A2T sum needs the three-slot moments (cagr_scatter3)");
+        p.adjn = (const T*)t->adj_nodes;
+        p.adjp = (const T*)t->adj_points;
     }
     const int out_dim = (a.op == kOpA || a.op == kOpA3 || a.op == kOpA21 || a.op == kOpA22 ||
                          a.op == kOpA23 || a.op == kOpCount)

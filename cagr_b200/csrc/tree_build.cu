@@ -216,7 +216,8 @@ __global__ void k_emit(const uint64_t* __restrict__ sk, const int8_t* __restrict
             par = (int64_t)base[p] + (d - 1 - d0a[p]);
         }
         const bool leaf = (d == dlast);
-        meta[id] = make_int4((int)next, (int)i, (int)(end - i), d | ((leaf ? 1 : 0) << 8));
+        const int cnt = (int)(end - i);
+        meta[id] = make_int4((int)next, (int)i, leaf ? -cnt : cnt, d);
         parent[id] = (int32_t)par;
         npts64[id] = end - i;
         if (par >= 0) {
@@ -226,10 +227,10 @@ __global__ void k_emit(const uint64_t* __restrict__ sk, const int8_t* __restrict
     }
 }
 
-__global__ void k_pack(int4* __restrict__ meta, const int32_t* __restrict__ nchild, int64_t M) {
+__global__ void k_pack(uint8_t* __restrict__ out, const int32_t* __restrict__ nchild, int64_t M) {
     int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= M) return;
-    meta[id].w |= (nchild[id] & 0xff) << 16;
+    out[id] = (uint8_t)nchild[id];
 }
 
 __global__ void k_leaf_ids(const int32_t* __restrict__ nn, const int32_t* __restrict__ base,
@@ -276,9 +277,9 @@ __global__ void k_walk(const int32_t* __restrict__ invperm, const uint64_t* __re
             pair_pt[k + c] = (int32_t)p;
         }
         c++;
-        const int w = meta[node].w;
-        if (meta_leaf(w) || c > CAGR_MAX_DEPTH + 1) break;
-        node = children[node * 8 + digit_at(code, D, meta_depth(w))];
+        const int4 m = meta[node];
+        if (node_leaf(m) || c > CAGR_MAX_DEPTH + 1) break;
+        node = children[node * 8 + digit_at(code, D, node_depth(m))];
         if (node < 0) break;  // unreachable for a consistent tree; never index with -1
     }
     if (!WRITE) cnt[p] = c;
@@ -301,9 +302,9 @@ __global__ void k_export(const int4* __restrict__ meta, const int32_t* __restric
     if (o_parent) o_parent[id] = parent[id];
     if (o_children)
         for (int k = 0; k < 8; k++) o_children[id * 8 + k] = children[id * 8 + k];
-    if (o_leaf) o_leaf[id] = meta_leaf(mt.w) ? 1 : 0;
-    if (o_half_w) o_half_w[id] = ldexp(T(1), -meta_depth(mt.w));
-    if (o_npts) o_npts[id] = mt.z;
+    if (o_leaf) o_leaf[id] = node_leaf(mt) ? 1 : 0;
+    if (o_half_w) o_half_w[id] = ldexp(T(1), -node_depth(mt));
+    if (o_npts) o_npts[id] = node_npts(mt);
     if (o_n2ps) o_n2ps[id] = n2ps[id];
 }
 
@@ -410,6 +411,7 @@ int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) 
 
     // 4: nodes
     if (int rc = dev_alloc((void**)&t->meta, sizeof(int4) * M)) return rc;
+    if (int rc = dev_alloc((void**)&t->nchild, M)) return rc;
     if (int rc = dev_alloc((void**)&t->parent, sizeof(int32_t) * M)) return rc;
     if (int rc = dev_alloc((void**)&t->children, sizeof(int32_t) * M * 8)) return rc;
     if (int rc = dev_alloc((void**)&t->leaf_ids, sizeof(int32_t) * NL)) return rc;
@@ -425,7 +427,7 @@ int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) 
                                   (const int32_t*)base.p, (const int8_t*)d0a.p,
                                   (const int8_t*)dla.p, t->meta, t->parent, t->children,
                                   (int32_t*)nchild.p, (int64_t*)npts64.p);
-    k_pack<<<grid_for(M), kBlock, 0, st>>>(t->meta, (const int32_t*)nchild.p, M);
+    k_pack<<<grid_for(M), kBlock, 0, st>>>(t->nchild, (const int32_t*)nchild.p, M);
     k_leaf_ids<<<gN, kBlock, 0, st>>>((const int32_t*)nn.p, (const int32_t*)base.p,
                                       (const int8_t*)d0a.p, (const int8_t*)dla.p,
                                       (const int32_t*)leafrank.p, n, t->leaf_ids);
@@ -511,6 +513,7 @@ void tree_free(Tree* t) {
     cudaFree(t->perm);
     cudaFree(t->invperm);
     cudaFree(t->meta);
+    cudaFree(t->nchild);
     cudaFree(t->parent);
     cudaFree(t->children);
     cudaFree(t->leaf_ids);
@@ -519,6 +522,8 @@ void tree_free(Tree* t) {
     cudaFree(t->spos);
     cudaFree(t->counters);
     for (int k = 0; k < 3; k++) cudaFree(t->rec[k]);
+    cudaFree(t->adj_nodes);
+    cudaFree(t->adj_points);
     delete t;
 }
 

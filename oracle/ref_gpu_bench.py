@@ -81,6 +81,24 @@ def main():
         out[f"cagr_b200_{tag}_ms_per_step"] = round(float(np.mean(times["ours"])), 3)
         out[f"{tag}_rel_l2_A2"] = rel_l2(oa, ra)
         out[f"{tag}_rel_l2_A2T_sum"] = rel_l2(ot, rt)
+        if tag == "fp32":
+            # both GPU results against the reference algorithm in IEEE host arithmetic
+            # (the reference's kernels compiled for the host), on sampled queries
+            from oracle.oracle import RefOracle, point_weights
+            host = RefOracle()
+            pn = p.astype(np.float32)
+            tr = host.build_tree(pn)
+            mun = mu.astype(np.float32)
+            mom = host.moments(tr, pn, point_weights(mun), mun)
+            sel = np.random.default_rng(9).choice(args.n, size=min(50_000, args.n), replace=False)
+            h21 = host.multiply("A21", pn[sel], widths[sel], pn, mun, tr, mom)[:, 0]
+            g_ref = ra[:, 0].cpu().numpy()[sel]
+            g_our = oa[:, 0].cpu().numpy()[sel]
+            nrm = np.linalg.norm(h21)
+            out["A21_rel_l2_vs_host_reference"] = {
+                "reference_gpu": float(np.linalg.norm(g_ref - h21) / nrm),
+                "cagr_b200": float(np.linalg.norm(g_our - h21) / nrm),
+                "queries": int(len(sel))}
         wn.close()
     print(json.dumps(out), flush=True)
 
