@@ -71,11 +71,12 @@ def lib() -> ctypes.CDLL:
     """The loaded library (raises if it has not been built)."""
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
+        path = os.environ.get("CAGR_B200_LIB", LIB_PATH)  # an alternative build of the same ABI
+        if not os.path.exists(path):
             raise RuntimeError(
-                f"{LIB_PATH} is missing: build it with `python -m cagr_b200.build` "
+                f"{path} is missing: build it with `python -m cagr_b200.build` "
                 "(the treecode has no CPU fallback)")
-        L = ctypes.CDLL(LIB_PATH)
+        L = ctypes.CDLL(path)
         for name, (res, args) in _SIGNATURES.items():
             f = getattr(L, name)
             f.restype = res

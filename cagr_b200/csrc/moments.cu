@@ -2,24 +2,27 @@
 //
 // Reference: mayueji/CAGR CUDA-based/ext/wn_treecode/wn_treecode_cuda/
 // wn_treecode_cuda_torch_interface.cu:41-134 launches one leaf kernel and then
-// 2*tree_depth level kernels (wn_treecode_cuda_kernels.cu:419-553), each over
-// all M nodes.  Here one launch does the whole reduction: one thread per leaf
-// computes the leaf moments, then climbs; at every parent the last-arriving
-// child (atomic arrival counter, reset by the thread that completes the node)
-// computes the parent from its children in octant order.  The floating-point
-// operation order is the reference's, so node sums, weights and centroids are
-// bit-identical to the reference kernels evaluated in IEEE arithmetic:
+// 2*tree_depth kernels over ALL M nodes (find-next + nonleaf,
+// wn_treecode_cuda_kernels.cu:419-553).  Here one launch does the whole
+// reduction: one thread per leaf computes the leaf moments, then climbs; at
+// every parent the last-arriving child (atomic arrival counter, reset by the
+// thread that completes the node) computes the parent from its children in
+// octant order.  No thread ever waits for another.  (A level-synchronous
+// variant -- one launch per depth -- measured slower at 1M points: its ~15
+// dependent launches cost more than the arrival counters.)  The
+// floating-point operation order is the reference's, so node sums, weights and
+// centroids are bit-identical to the reference kernels evaluated in IEEE
+// arithmetic:
 //   leaf:     for points in node2point order  W += w;  A += a;  R += y*w;  P += y
 //   internal: for children in octant order    W += Wc; A += Ac; R += Rc*Wc; P += Rc
 //   centroid: W > 0 ? R * (1/W) : P * (1/npts)            (:456-461, :510-517)
-// The same launch writes the Morton-ordered point records the traversal reads.
-// Every record carries exp(-c/2) per axis so the traversal forms the
+// The same launch writes the Morton-ordered point records the traversal reads.  Every record carries exp(-c/2) per axis so the traversal forms the
 // convection factor exp((x-c)_k/2) as exp(x_k/2) * exp(-c_k/2), and node
 // records carry the acceptance radius (4 half_w)^2.
 //
 // NS = 3 computes three independent scalar attributes (the three inputs of
 // the reference's A2T1/A2T2/A2T3 calls, each with its own |s_k| weights and
-// centroids) in one launch and one climb.
+// centroids) in the same launch, and also writes the packed adjoint records.
 #include <string>
 
 #include "internal.h"
@@ -73,16 +76,26 @@ struct MomParams {
     T* adjp = nullptr;  // NS == 3: packed adjoint point records [N*8]
 };
 
-template <typename T, int DIM, int NS>
-__global__ void __launch_bounds__(kBlock) k_moments(const MomParams<T, DIM, NS> p) {
-    const int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (li >= p.num_leaves) return;
-    const int64_t M = p.M;
-    int node = p.leaf_ids[li];
-    const int4 lm = p.meta[node];
-    const int pstart = lm.y, np = node_npts(lm);
+// Running sums of one node, per slot.
+template <typename T, int NS>
+struct Sums {
+    T W[NS], A[NS][3], R[NS][3], P[NS][3];
+    __device__ __forceinline__ void clear() {
+#pragma unroll
+        for (int k = 0; k < NS; k++) {
+            W[k] = T(0);
+            for (int d = 0; d < 3; d++) A[k][d] = R[k][d] = P[k][d] = T(0);
+        }
+    }
+};
 
-    // point records for the leaf's Morton range
+// Point records of a leaf's Morton range, and the leaf sums over its points in
+// node2point (ascending original index) order.
+template <typename T, int DIM, int NS>
+__device__ __forceinline__ void leaf_pass(const MomParams<T, DIM, NS>& p, int node, const int4& lm,
+                                         Sums<T, NS>& S) {
+    const int64_t M = p.M;
+    const int pstart = lm.y, np = node_npts(lm);
     for (int j = 0; j < np; j++) {
         const int s = pstart + j;
         const int pt = p.perm[s];
@@ -104,99 +117,107 @@ __global__ void __launch_bounds__(kBlock) k_moments(const MomParams<T, DIM, NS> 
             st4<T>(p.adjp + (int64_t)s * 8 + 4, make4(es[1], es[2], T(0), T(0)));
         }
     }
-
-    // leaf moments, points in node2point (ascending original index) order
-    T W[NS], A[NS][3], R[NS][3], P[NS][3];
-#pragma unroll
-    for (int k = 0; k < NS; k++) {
-        W[k] = T(0);
-        for (int d = 0; d < 3; d++) A[k][d] = R[k][d] = P[k][d] = T(0);
-    }
-    {
-        const int64_t base = p.n2p_start[node];
-        for (int j = 0; j < np; j++) {
-            const int pt = (np == 1) ? p.perm[pstart] : p.n2p[base + j];
-            const int s = (np == 1) ? pstart : p.invperm[pt];
-            const T y[3] = {p.spos[3 * s], p.spos[3 * s + 1], p.spos[3 * s + 2]};
-#pragma unroll
-            for (int k = 0; k < NS; k++) {
-                T a[3] = {T(0), T(0), T(0)};
-#pragma unroll
-                for (int c = 0; c < DIM; c++)
-                    a[c] = p.attrs[(int64_t)pt * p.astride + k * DIM + c];
-                const T w = (NS == 1 && p.weights) ? p.weights[pt] : weight_of(a, DIM);
-                W[k] = add_rn(W[k], w);
-                for (int c = 0; c < DIM; c++) A[k][c] = add_rn(A[k][c], a[c]);
-                for (int d = 0; d < 3; d++) {
-                    R[k][d] = add_rn(R[k][d], mul_rn(y[d], w));
-                    P[k][d] = add_rn(P[k][d], y[d]);
-                }
-            }
-        }
-    }
-
-    int count = np;          // points under `node`: the zero-weight centroid divides by it
-    int depth = node_depth(lm);
-    while (true) {
+    S.clear();
+    const int64_t base = p.n2p_start[node];
+    for (int j = 0; j < np; j++) {
+        const int pt = (np == 1) ? p.perm[pstart] : p.n2p[base + j];
+        const int s = (np == 1) ? pstart : p.invperm[pt];
+        const T y[3] = {p.spos[3 * s], p.spos[3 * s + 1], p.spos[3 * s + 2]};
 #pragma unroll
         for (int k = 0; k < NS; k++) {
-            T c[3], e[3];
-            if (W[k] > T(0)) {
-                const T inv = div_rn(T(1), W[k]);
-                for (int d = 0; d < 3; d++) c[d] = mul_rn(R[k][d], inv);
-            } else {
-                // (wn_treecode_cuda_kernels.cu:459-460 for leaves, :515-517 for internal
-                // nodes, where it divides a sum of child centroids by the point count)
-                const T inv = div_rn(T(1), T(count));
-                for (int d = 0; d < 3; d++) c[d] = mul_rn(P[k][d], inv);
+            T a[3] = {T(0), T(0), T(0)};
+#pragma unroll
+            for (int c = 0; c < DIM; c++) a[c] = p.attrs[(int64_t)pt * p.astride + k * DIM + c];
+            const T w = (NS == 1 && p.weights) ? p.weights[pt] : weight_of(a, DIM);
+            S.W[k] = add_rn(S.W[k], w);
+            for (int c = 0; c < DIM; c++) S.A[k][c] = add_rn(S.A[k][c], a[c]);
+            for (int d = 0; d < 3; d++) {
+                S.R[k][d] = add_rn(S.R[k][d], mul_rn(y[d], w));
+                S.P[k][d] = add_rn(S.P[k][d], y[d]);
             }
-            exps(c, e);
-            write_record<T, DIM>(p.rec[k] + (int64_t)node * CAGR_REC_STRIDE, c, e, A[k], W[k],
-                                 mac_radius2<T>(depth));
-            if constexpr (NS == 3)
-                st4<T>(p.adjn + (int64_t)node * 12 + 4 * k, make4(c[0], c[1], c[2], e[k] * A[k][0]));
         }
+    }
+}
+
+// Sums over the children of `node` in octant order.  CG: read through L2
+// (children written by other threads of the same launch).
+template <bool CG, typename T, int DIM, int NS>
+__device__ __forceinline__ void children_pass(const MomParams<T, DIM, NS>& p, int node,
+                                              Sums<T, NS>& S) {
+    S.clear();
+    const int4 c0 = reinterpret_cast<const int4*>(p.children)[2 * (int64_t)node];
+    const int4 c1 = reinterpret_cast<const int4*>(p.children)[2 * (int64_t)node + 1];
+    const int ch[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        if (ch[q] < 0) continue;
+#pragma unroll
+        for (int k = 0; k < NS; k++) {
+            const T* r = p.rec[k] + (int64_t)ch[q] * CAGR_REC_STRIDE;
+            const Vec4<T> r0 = CG ? ld4_cg(r) : ld4(r);
+            const Vec4<T> r1 = CG ? ld4_cg(r + 4) : ld4(r + 4);
+            const Vec4<T> r2 = CG ? ld4_cg(r + 8) : ld4(r + 8);
+            const T wc = r2.z;
+            const T ac[3] = {r1.w, r2.x, r2.y};
+            const T rc[3] = {r0.x, r0.y, r0.z};
+            S.W[k] = add_rn(S.W[k], wc);
+            for (int c = 0; c < DIM; c++) S.A[k][c] = add_rn(S.A[k][c], ac[c]);
+            for (int d = 0; d < 3; d++) {
+                S.R[k][d] = add_rn(S.R[k][d], mul_rn(rc[d], wc));
+                S.P[k][d] = add_rn(S.P[k][d], rc[d]);
+            }
+        }
+    }
+}
+
+// Centroid (with the reference's zero-weight fallback) and node record(s).
+template <typename T, int DIM, int NS>
+__device__ __forceinline__ void finish_node(const MomParams<T, DIM, NS>& p, int node, int depth,
+                                            int count, const Sums<T, NS>& S) {
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+        T c[3], e[3];
+        if (S.W[k] > T(0)) {
+            const T inv = div_rn(T(1), S.W[k]);
+            for (int d = 0; d < 3; d++) c[d] = mul_rn(S.R[k][d], inv);
+        } else {
+            // (wn_treecode_cuda_kernels.cu:459-460 for leaves, :515-517 for internal
+            // nodes, where it divides a sum of child centroids by the point count)
+            const T inv = div_rn(T(1), T(count));
+            for (int d = 0; d < 3; d++) c[d] = mul_rn(S.P[k][d], inv);
+        }
+        exps(c, e);
+        write_record<T, DIM>(p.rec[k] + (int64_t)node * CAGR_REC_STRIDE, c, e, S.A[k], S.W[k],
+                             mac_radius2<T>(depth));
+        if constexpr (NS == 3)
+            st4<T>(p.adjn + (int64_t)node * 12 + 4 * k, make4(c[0], c[1], c[2], e[k] * S.A[k][0]));
+    }
+}
+
+// Each leaf thread climbs while it is the last child to arrive at the parent.
+template <typename T, int DIM, int NS>
+__global__ void __launch_bounds__(kBlock) k_moments_climb(const MomParams<T, DIM, NS> p) {
+    const int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= p.num_leaves) return;
+    int node = p.leaf_ids[li];
+    const int4 lm = p.meta[node];
+    Sums<T, NS> S;
+    leaf_pass(p, node, lm, S);
+    int count = node_npts(lm), depth = node_depth(lm);
+    while (true) {
+        finish_node(p, node, depth, count, S);
         if (node == 0) return;
-        // publish this node, then arrive at the parent
         __threadfence();
         const int par = p.parent[node];
-        const int4 pm = p.meta[par];
         const uint32_t arrived = atomicAdd(&p.counters[par], 1u);
         if (arrived + 1u != (uint32_t)p.nchild[par]) return;
-        p.counters[par] = 0u;  // every child has arrived: ready for the next pass
+        p.counters[par] = 0u;
         __threadfence();
+        const int4 pm = p.meta[par];
         node = par;
         count = node_npts(pm);
         depth = node_depth(pm);
-#pragma unroll
-        for (int k = 0; k < NS; k++) {
-            W[k] = T(0);
-            for (int d = 0; d < 3; d++) A[k][d] = R[k][d] = P[k][d] = T(0);
-        }
-        // children in octant order, read through L2 (written during this launch)
-        const int4 c0 = reinterpret_cast<const int4*>(p.children)[2 * (int64_t)node];
-        const int4 c1 = reinterpret_cast<const int4*>(p.children)[2 * (int64_t)node + 1];
-        const int ch[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-            if (ch[q] < 0) continue;
-#pragma unroll
-            for (int k = 0; k < NS; k++) {
-                const T* r = p.rec[k] + (int64_t)ch[q] * CAGR_REC_STRIDE;
-                const Vec4<T> r0 = ld4_cg(r);
-                const Vec4<T> r1 = ld4_cg(r + 4);
-                const Vec4<T> r2 = ld4_cg(r + 8);
-                const T wc = r2.z;
-                const T ac[3] = {r1.w, r2.x, r2.y};
-                const T rc[3] = {r0.x, r0.y, r0.z};
-                W[k] = add_rn(W[k], wc);
-                for (int c = 0; c < DIM; c++) A[k][c] = add_rn(A[k][c], ac[c]);
-                for (int d = 0; d < 3; d++) {
-                    R[k][d] = add_rn(R[k][d], mul_rn(rc[d], wc));
-                    P[k][d] = add_rn(P[k][d], rc[d]);
-                }
-            }
-        }
+        children_pass<true>(p, node, S);
     }
 }
 
@@ -225,8 +246,7 @@ int ensure_slot(Tree* t, int slot, size_t elem) {
 }
 
 template <typename T, int DIM, int NS>
-MomParams<T, DIM, NS> params(Tree* t, const void* attrs, int astride, const void* weights) {
-    MomParams<T, DIM, NS> p;
+int run(Tree* t, MomParams<T, DIM, NS> p, cudaStream_t s) {
     p.num_leaves = t->num_leaves;
     p.M = t->m;
     p.leaf_ids = t->leaf_ids;
@@ -239,28 +259,34 @@ MomParams<T, DIM, NS> params(Tree* t, const void* attrs, int astride, const void
     p.n2p = t->n2p;
     p.n2p_start = t->n2p_start;
     p.spos = (const T*)t->spos;
-    p.attrs = (const T*)attrs;
-    p.astride = astride;
-    p.weights = (const T*)weights;
     p.counters = t->counters;
-    return p;
+    const unsigned grid = (unsigned)((t->num_leaves + kBlock - 1) / kBlock);
+    k_moments_climb<T, DIM, NS><<<grid, kBlock, 0, s>>>(p);
+    CAGR_CUDA(cudaGetLastError());
+    return kOk;
 }
 
 template <typename T>
 int launch_moments(Tree* t, int slot, const void* attrs, int dim, const void* weights,
                    cudaStream_t s) {
     if (int rc = ensure_slot(t, slot, sizeof(T))) return rc;
-    const unsigned grid = (unsigned)((t->num_leaves + kBlock - 1) / kBlock);
+    int rc;
     if (dim == 3) {
-        auto p = params<T, 3, 1>(t, attrs, 3, weights);
+        MomParams<T, 3, 1> p;
+        p.attrs = (const T*)attrs;
+        p.astride = 3;
+        p.weights = (const T*)weights;
         p.rec[0] = (T*)t->rec[slot];
-        k_moments<T, 3, 1><<<grid, kBlock, 0, s>>>(p);
+        rc = run(t, p, s);
     } else {
-        auto p = params<T, 1, 1>(t, attrs, 1, weights);
+        MomParams<T, 1, 1> p;
+        p.attrs = (const T*)attrs;
+        p.astride = 1;
+        p.weights = (const T*)weights;
         p.rec[0] = (T*)t->rec[slot];
-        k_moments<T, 1, 1><<<grid, kBlock, 0, s>>>(p);
+        rc = run(t, p, s);
     }
-    CAGR_CUDA(cudaGetLastError());
+    if (rc) return rc;
     t->rec_dim[slot] = dim;
     return kOk;
 }
@@ -275,13 +301,13 @@ int launch_moments3(Tree* t, const void* values3, cudaStream_t s) {
         if (e != cudaSuccess)
             return set_error(kErrAlloc, std::string("adjoint records: ") + cudaGetErrorString(e));
     }
-    const unsigned grid = (unsigned)((t->num_leaves + kBlock - 1) / kBlock);
-    auto p = params<T, 1, 3>(t, values3, 3, nullptr);
+    MomParams<T, 1, 3> p;
+    p.attrs = (const T*)values3;
+    p.astride = 3;
     for (int k = 0; k < 3; k++) p.rec[k] = (T*)t->rec[k];
     p.adjn = (T*)t->adj_nodes;
     p.adjp = (T*)t->adj_points;
-    k_moments<T, 1, 3><<<grid, kBlock, 0, s>>>(p);
-    CAGR_CUDA(cudaGetLastError());
+    if (int rc = run(t, p, s)) return rc;
     for (int k = 0; k < 3; k++) t->rec_dim[k] = 1;
     t->adj_valid = true;
     return kOk;

@@ -39,7 +39,10 @@
 namespace cagr {
 namespace {
 
-constexpr int kWarps = 4;  // warps per block
+#ifndef CAGR_TRAV_WARPS
+#define CAGR_TRAV_WARPS 4
+#endif
+constexpr int kWarps = CAGR_TRAV_WARPS;  // warps (32 consecutive queries each) per block
 constexpr unsigned kFull = 0xffffffffu;
 
 template <typename T>
@@ -216,23 +219,27 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p)
         const bool open = active && !far;
         if (active) kd = (open && !leaf) ? d + 1 : d;
         const bool any_open = __any_sync(kFull, open);
-        // one term per active lane: far lanes the node term, near lanes at a leaf
-        // its first point (the rest of a multi-point leaf follows below)
-        const T* src = r;
-        if (leaf && open) {
-            src = rec + ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
-            const Vec4<T> s0 = ld4(src);
-            dx = sub_rn(L.q0, s0.x);
-            dy = sub_rn(L.q1, s0.y);
-            dz = sub_rn(L.q2, s0.z);
-            d2 = dist2_exact(dx, dy, dz);
+        if (mt.z == -1) {
+            // single-point leaf: far lanes take the node term, near lanes the point
+            const T* src = r;
+            if (open) {
+                src = rec + ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
+                const Vec4<T> s0 = ld4(src);
+                dx = sub_rn(L.q0, s0.x);
+                dy = sub_rn(L.q1, s0.y);
+                dz = sub_rn(L.q2, s0.z);
+                d2 = dist2_exact(dx, dy, dz);
+            }
+            if (active) pair_term<T, OP, CONT>(L, src, dx, dy, dz, d2);
+            n = mt.x;
+            continue;
         }
-        if (active && (far || leaf)) pair_term<T, OP, CONT>(L, src, dx, dy, dz, d2);
+        if (active && far) pair_term<T, OP, CONT>(L, r, dx, dy, dz, d2);
         if (leaf) {
             const int np = -mt.z;
-            if (np > 1 && any_open) {
-                const T* pr = rec + ((int64_t)M + mt.y + 1) * CAGR_REC_STRIDE;
-                for (int j = 1; j < np; j++, pr += CAGR_REC_STRIDE) {
+            if (any_open) {
+                const T* pr = rec + ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
+                for (int j = 0; j < np; j++, pr += CAGR_REC_STRIDE) {
                     if (open) {
                         const Vec4<T> s0 = ld4(pr);
                         const T ex = sub_rn(L.q0, s0.x);
@@ -388,8 +395,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t_shared(const TravP
 // One direction-K A2T term with g = exp(x_K/2) exp(-y_K/2) s (premultiplied):
 //   acc += g (d / r^3 + e_K / (2r)).
 template <typename T, int K>
-__device__ __forceinline__ void a2t_term1(Lane<T>& L, T g, T dx, T dy, T dz, T d2) {
-    const bool outside = d2 >= L.tw;
+__device__ __forceinline__ void a2t_term1(Lane<T>& L, bool take, T g, T dx, T dy, T dz, T d2) {
+    const bool outside = take && d2 >= L.tw;  // not taken: contributes exactly zero
     const T rinv = outside ? rsqrt_t(d2) : T(0);
     const T c = g * (rinv * rinv * rinv);
     L.acc0 += dx * c;
@@ -455,9 +462,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t3(const TravParams<
         const SlotTest<T> s2 = slot_test(L, c2, R2, d, leaf, kd2);
         const bool open_any = s0.open || s1.open || s2.open;
         const bool any_open = __any_sync(kFull, open_any);
-        if (s0.active && s0.far) a2t_term1<T, 0>(L, ex0 * c0.w, s0.dx, s0.dy, s0.dz, s0.d2);
-        if (s1.active && s1.far) a2t_term1<T, 1>(L, ex1 * c1.w, s1.dx, s1.dy, s1.dz, s1.d2);
-        if (s2.active && s2.far) a2t_term1<T, 2>(L, ex2 * c2.w, s2.dx, s2.dy, s2.dz, s2.d2);
+        // node terms, each slot against its own centroid
+        if (s0.active && s0.far) a2t_term1<T, 0>(L, true, ex0 * c0.w, s0.dx, s0.dy, s0.dz, s0.d2);
+        if (s1.active && s1.far) a2t_term1<T, 1>(L, true, ex1 * c1.w, s1.dx, s1.dy, s1.dz, s1.d2);
+        if (s2.active && s2.far) a2t_term1<T, 2>(L, true, ex2 * c2.w, s2.dx, s2.dy, s2.dz, s2.d2);
         if (leaf) {
             if (any_open) {
                 const int np = -mt.z;

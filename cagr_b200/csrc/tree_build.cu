@@ -503,6 +503,7 @@ int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) 
         maxd = h;
     }
     t->depth = maxd;
+
     return kOk;
 }
 
