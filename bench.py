@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--grid", type=int, default=512, help="field grid for the end-to-end run")
     ap.add_argument("--cpu-sample", type=int, default=0,
                     help="queries per operator timed on the CPU (0 = auto)")
     return ap.parse_args()
@@ -338,6 +340,31 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         fp64_ms = float(np.mean(t))
         wn64.close()
 
+    # end to end: the whole CAGR normal solve on this cloud (tree build + 40
+    # iterations + 8 G steps, main_CAGR.py's schedule, preset l0)
+    solve = None
+    if not args.no_solve:
+        from cagr_b200.solver import PRESET_WIDTHS, cagr_solve
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        res = cagr_solve(P, *PRESET_WIDTHS["l0"])
+        torch.cuda.synchronize(dev)
+        t_solve = time.perf_counter() - t0
+        from cagr_b200.mesh import reconstruct
+        t1 = time.perf_counter()
+        rec = reconstruct(P, res.normals, grid=args.grid)
+        torch.cuda.synchronize(dev)
+        t_rec = time.perf_counter() - t1
+        solve = {"total_s": round(t_solve + t_rec, 4), "solve_s": round(t_solve, 4),
+                 "tree_build_s": round(res.time_tree_s, 4),
+                 "iterations_s": round(res.time_main_s, 4),
+                 "operator_calls": res.operator_calls, "preset": "l0",
+                 "reconstruct_s": round(t_rec, 4), "grid": args.grid,
+                 "field_s": round(rec.seconds["field"], 4),
+                 "marching_cubes_s": round(rec.seconds["marching_cubes"], 4),
+                 "vertices": int(rec.vertices.shape[0]), "faces": int(rec.faces.shape[0])}
+        del rec
+
     # measured FP32 FMA peak (roofline denominator)
     gf = ctypes.c_double()
     _lib.check(_lib.lib().cagr_probe_fp32_peak(20000, ctypes.byref(gf),
@@ -395,6 +422,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "pair_terms": {"A2_FUSED": round(terms_a2), "A2T1": round(terms_t[0]),
                        "A2T2": round(terms_t[1]), "A2T3": round(terms_t[2])},
         "fp64_ms_per_step": None if fp64_ms is None else round(fp64_ms, 3),
+        "end_to_end": solve,
         "clocks": clk,
     }
     if cpu is not None:

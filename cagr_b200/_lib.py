@@ -51,6 +51,12 @@ _SIGNATURES = {
     "cagr_multiply": (_i32, [_p, _i32, _p, _p, _i64, _p, ctypes.c_double, _i32, _p, _i64, _p]),
     "cagr_forward": (_i32, [_p, _i32, _p, _p, ctypes.c_double, _i32, _p, _p]),
     "cagr_probe_fp32_peak": (_i32, [_i64, ctypes.POINTER(ctypes.c_double), _p]),
+    "cagr_field_grid": (_i32, [_p, _i32, _i32, _i32, _i32, ctypes.POINTER(ctypes.c_double),
+                               ctypes.c_double, _p, ctypes.c_double, _i32, _p, _p]),
+    "cagr_marching_cubes": (_i32, [_p, _i32, _i32, _i32, ctypes.POINTER(ctypes.c_double),
+                                   ctypes.c_double, ctypes.c_double, _p, _i64, _p, _i64, _pi64,
+                                   _pi64, _p]),
+    "cagr_mc_table": (_i32, [_p, _p]),
     "cagr_scatter_noalloc": (_i32, [_p] * 6 + [_i64, _i32, _p, _p, _p, _i32, _p, _p, _p, _p]),
 }
 

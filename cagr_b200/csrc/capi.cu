@@ -164,6 +164,43 @@ int cagr_multiply(const cagr_tree* tree, int op, const void* queries_dev,
     return cagr::traverse(tree->t, a, as_stream(stream));
 }
 
+int cagr_field_grid(const cagr_tree* tree, int op, int nx, int ny, int nz,
+                    const double* origin, double spacing, const void* widths_dev, double width,
+                    int flags, void* out_dev, void* stream) {
+    if (int rc = check_tree(tree)) return rc;
+    if (op_attr_dim(op) <= 0 || op == CAGR_OP_A2T_SUM || op == CAGR_OP_A2T_SUM_SHARED)
+        return set_error(CAGR_ERR_INVALID, "unsupported operator for grid queries");
+    if (!origin) return set_error(CAGR_ERR_INVALID, "origin is null");
+    if (flags & ~(CAGR_FLAG_CONTINUOUS | CAGR_FLAG_ACCUMULATE))
+        return set_error(CAGR_ERR_INVALID, "unknown flag bits");
+    cagr::TraverseArgs a;
+    a.op = op;
+    a.continuous = (flags & CAGR_FLAG_CONTINUOUS) ? 1 : 0;
+    a.accumulate = (flags & CAGR_FLAG_ACCUMULATE) ? 1 : 0;
+    a.grid = 1;
+    a.gx = nx;
+    a.gy = ny;
+    a.gz = nz;
+    for (int d = 0; d < 3; d++) a.gorigin[d] = origin[d];
+    a.gspacing = spacing;
+    a.widths = widths_dev;
+    a.width = width;
+    a.out = out_dev;
+    return cagr::traverse(tree->t, a, as_stream(stream));
+}
+
+int cagr_mc_table(int8_t* tri, uint8_t* ntri) { return cagr::mc_table(tri, ntri); }
+
+int cagr_marching_cubes(const float* values_dev, int nx, int ny, int nz, const double* origin,
+                        double spacing, double iso, float* vertices_dev, int64_t max_vertices,
+                        int32_t* faces_dev, int64_t max_faces, int64_t* num_vertices,
+                        int64_t* num_faces, void* stream) {
+    if (!origin) return set_error(CAGR_ERR_INVALID, "origin is null");
+    return cagr::marching_cubes(values_dev, nx, ny, nz, origin, spacing, iso, vertices_dev,
+                                max_vertices, faces_dev, max_faces, num_vertices, num_faces,
+                                as_stream(stream));
+}
+
 int cagr_forward(cagr_tree* tree, int op, const void* values_dev, const void* widths_dev,
                  double width, int flags, void* out_dev, void* stream) {
     if (int rc = check_tree(tree)) return rc;

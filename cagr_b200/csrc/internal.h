@@ -104,8 +104,21 @@ struct TraverseArgs {
     double width = 0.0;
     void* out = nullptr;               // [nq, out_dim] T
     int out_stride = 0;                // scalars between consecutive queries (0 = out_dim)
+    // regular-grid queries (instead of `queries`): node (i, j, k) at
+    // gorigin + (i, j, k) * gspacing, output row (k * gy + j) * gx + i
+    int grid = 0;
+    int gx = 0, gy = 0, gz = 0;
+    double gorigin[3] = {0, 0, 0};
+    double gspacing = 0;
 };
 
 int traverse(const Tree* t, const TraverseArgs& a, cudaStream_t stream);
+
+// Marching cubes (mcubes.cu).  The case table: tri[256][36] edge ids (12
+// triangles at most) and ntri[256].
+int mc_table(int8_t* tri, uint8_t* ntri);
+int marching_cubes(const float* values, int nx, int ny, int nz, const double* origin,
+                   double spacing, double iso, float* verts, int64_t max_verts, int32_t* faces,
+                   int64_t max_faces, int64_t* nverts, int64_t* nfaces, cudaStream_t s);
 
 }  // namespace cagr

@@ -1,0 +1,413 @@
+// Marching cubes on a regular grid of field values (the iso-surface step of the
+// reconstruction).
+//
+// Reference role: the GaussRecon driver evaluates the field at grid corners
+// and extracts the iso-surface at the median field value of the samples
+// (main_GaussRecon_cuda.cu:427-494) with PoissonRecon's adaptive marching
+// cubes (gaussrecon_src/Octree.cpp:852-1090).  The benchmark workloads ask for
+// a regular G^3 grid, which this module handles entirely on the device.
+//
+// Case table: generated here, not copied.  Cube corners c = x + 2y + 4z; edge
+// 4a + u + 2v runs along axis a with the other two coordinates (u, v) in
+// increasing axis order.  For each of the 256 inside/outside patterns:
+//  1. every face with 2 sign changes gets one segment between them; a face with
+//     4 (the ambiguous pattern) gets two segments, each cutting off one INSIDE
+//     corner -- a rule that depends only on that face's 4 corners, so the two
+//     cells sharing a face always agree and meshes are watertight;
+//  2. segments are chained into closed polygons (each crossed edge lies on two
+//     faces, so every polygon is a cycle);
+//  3. each polygon is oriented so that its area vector points along the sum of
+//     its edges' inside-to-outside directions (outward), then fan-triangulated.
+// A corner is inside when value > iso (NaN is outside).
+//
+// Device pipeline (three passes over grid points and cells, two scans):
+//   edges:  per grid point, its crossed +x/+y/+z edges (bit mask) and count
+//   verts:  one vertex per crossed edge, at the linear root along the edge
+//   cells:  per cell, its case and triangle count
+//   tris:   per cell, triangles as vertex indices (shared edges share vertices)
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <array>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/cagr.h"
+#include "internal.h"
+
+namespace cagr {
+namespace {
+
+constexpr int kMaxTri = 12;  // the generator checks the bound
+constexpr int kBlock = 256;
+
+struct McTable {
+    int8_t tri[256][3 * kMaxTri];
+    uint8_t ntri[256];
+};
+
+// corners at the two ends of edge e
+inline void edge_corners(int e, int& c0, int& c1) {
+    const int a = e >> 2, u = e & 1, v = (e >> 1) & 1;
+    int b[3];
+    // other axes in increasing order
+    int o0 = a == 0 ? 1 : 0, o1 = a == 2 ? 1 : 2;
+    b[a] = 0;
+    b[o0] = u;
+    b[o1] = v;
+    c0 = b[0] + 2 * b[1] + 4 * b[2];
+    b[a] = 1;
+    c1 = b[0] + 2 * b[1] + 4 * b[2];
+}
+
+inline int edge_between(int ca, int cb) {
+    for (int e = 0; e < 12; e++) {
+        int c0, c1;
+        edge_corners(e, c0, c1);
+        if ((c0 == ca && c1 == cb) || (c0 == cb && c1 == ca)) return e;
+    }
+    return -1;
+}
+
+bool build_table(McTable& T, std::string& err) {
+    std::memset(&T, 0, sizeof(T));
+    // the 6 faces as corner cycles (each consecutive pair shares an edge)
+    int faces[6][4];
+    for (int a = 0; a < 3; a++) {
+        const int o0 = a == 0 ? 1 : 0, o1 = a == 2 ? 1 : 2;
+        for (int s = 0; s < 2; s++) {
+            const int uv[4][2] = {{0, 0}, {1, 0}, {1, 1}, {0, 1}};
+            for (int q = 0; q < 4; q++) {
+                int b[3];
+                b[a] = s;
+                b[o0] = uv[q][0];
+                b[o1] = uv[q][1];
+                faces[2 * a + s][q] = b[0] + 2 * b[1] + 4 * b[2];
+            }
+        }
+    }
+    for (int cfg = 0; cfg < 256; cfg++) {
+        auto in = [&](int c) { return (cfg >> c) & 1; };
+        // segment graph over edges: each crossed edge gets two neighbours
+        std::vector<int> nb[12];
+        for (int f = 0; f < 6; f++) {
+            int ce[4], cc = 0;  // crossed face edges in cyclic order
+            for (int q = 0; q < 4; q++) {
+                const int a = faces[f][q], b = faces[f][(q + 1) & 3];
+                ce[q] = in(a) != in(b) ? edge_between(a, b) : -1;
+                cc += ce[q] >= 0;
+            }
+            if (cc == 2) {
+                int x = -1, y = -1;
+                for (int q = 0; q < 4; q++)
+                    if (ce[q] >= 0) (x < 0 ? x : y) = ce[q];
+                nb[x].push_back(y);
+                nb[y].push_back(x);
+            } else if (cc == 4) {
+                // cut off each inside corner q: join the face edges before and after it
+                for (int q = 0; q < 4; q++) {
+                    if (!in(faces[f][q])) continue;
+                    const int x = ce[(q + 3) & 3], y = ce[q];
+                    nb[x].push_back(y);
+                    nb[y].push_back(x);
+                }
+            } else if (cc != 0) {
+                err = "odd crossing count on a face";
+                return false;
+            }
+        }
+        bool used[12] = {false};
+        int nt = 0;
+        for (int start = 0; start < 12; start++) {
+            if (used[start] || nb[start].empty()) continue;
+            if (nb[start].size() != 2) {
+                err = "crossed edge without two neighbours";
+                return false;
+            }
+            std::vector<int> cyc;
+            int prev = -1, cur = start;
+            while (true) {
+                cyc.push_back(cur);
+                used[cur] = true;
+                const int nx = nb[cur][0] != prev ? nb[cur][0] : nb[cur][1];
+                prev = cur;
+                cur = nx;
+                if (cur == start) break;
+                if (used[cur] || cyc.size() > 12) {
+                    err = "segments do not close";
+                    return false;
+                }
+            }
+            // orientation from edge midpoints and inside->outside directions
+            double area[3] = {0, 0, 0}, g[3] = {0, 0, 0};
+            std::vector<std::array<double, 3>> mid(cyc.size());
+            for (size_t i = 0; i < cyc.size(); i++) {
+                int c0, c1;
+                edge_corners(cyc[i], c0, c1);
+                const double p0[3] = {double(c0 & 1), double((c0 >> 1) & 1), double(c0 >> 2)};
+                const double p1[3] = {double(c1 & 1), double((c1 >> 1) & 1), double(c1 >> 2)};
+                const double sgn = in(c0) ? 1.0 : -1.0;  // inside -> outside
+                for (int d = 0; d < 3; d++) {
+                    mid[i][d] = 0.5 * (p0[d] + p1[d]);
+                    g[d] += sgn * (p1[d] - p0[d]);
+                }
+            }
+            for (size_t i = 0; i < cyc.size(); i++) {
+                const auto& a = mid[i];
+                const auto& b = mid[(i + 1) % cyc.size()];
+                area[0] += a[1] * b[2] - a[2] * b[1];
+                area[1] += a[2] * b[0] - a[0] * b[2];
+                area[2] += a[0] * b[1] - a[1] * b[0];
+            }
+            if (area[0] * g[0] + area[1] * g[1] + area[2] * g[2] < 0)
+                std::reverse(cyc.begin(), cyc.end());
+            for (size_t i = 1; i + 1 < cyc.size(); i++) {
+                if (nt >= kMaxTri) {
+                    err = "too many triangles in one cell";
+                    return false;
+                }
+                T.tri[cfg][3 * nt + 0] = (int8_t)cyc[0];
+                T.tri[cfg][3 * nt + 1] = (int8_t)cyc[i];
+                T.tri[cfg][3 * nt + 2] = (int8_t)cyc[i + 1];
+                nt++;
+            }
+        }
+        T.ntri[cfg] = (uint8_t)nt;
+    }
+    return true;
+}
+
+const McTable* host_table(std::string& err) {
+    static McTable table;
+    static bool ok = false;
+    static std::string build_err;
+    static std::once_flag once;
+    std::call_once(once, [] { ok = build_table(table, build_err); });
+    if (!ok) {
+        err = build_err;
+        return nullptr;
+    }
+    return &table;
+}
+
+__constant__ int8_t c_tri[256][3 * kMaxTri];
+__constant__ uint8_t c_ntri[256];
+
+std::mutex g_upload_mutex;
+bool g_uploaded[64] = {};
+
+int upload_table() {
+    std::string err;
+    const McTable* T = host_table(err);
+    if (!T) return set_error(kErrState, "marching-cubes table: " + err);
+    int dev = 0;
+    CAGR_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(kErrInvalid, "device index too large");
+    std::lock_guard<std::mutex> lock(g_upload_mutex);
+    if (!g_uploaded[dev]) {
+        CAGR_CUDA(cudaMemcpyToSymbol(c_tri, T->tri, sizeof(T->tri)));
+        CAGR_CUDA(cudaMemcpyToSymbol(c_ntri, T->ntri, sizeof(T->ntri)));
+        g_uploaded[dev] = true;
+    }
+    return kOk;
+}
+
+struct Grid {
+    int nx, ny, nz;
+    float ox, oy, oz, h, iso;
+};
+
+__device__ __forceinline__ bool inside(float v, float iso) { return v > iso; }
+
+__device__ __forceinline__ int64_t gid(const Grid& g, int i, int j, int k) {
+    return ((int64_t)k * g.ny + j) * g.nx + i;
+}
+
+// crossed edges owned by each grid point (+x, +y, +z) and their count
+__global__ void k_mc_edges(const float* __restrict__ v, Grid g, uint8_t* __restrict__ mask,
+                           int32_t* __restrict__ cnt) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t total = (int64_t)g.nx * g.ny * g.nz;
+    if (p >= total) return;
+    const int i = (int)(p % g.nx), j = (int)((p / g.nx) % g.ny), k = (int)(p / ((int64_t)g.nx * g.ny));
+    const bool a = inside(v[p], g.iso);
+    uint8_t m = 0;
+    if (i + 1 < g.nx && inside(v[p + 1], g.iso) != a) m |= 1;
+    if (j + 1 < g.ny && inside(v[p + g.nx], g.iso) != a) m |= 2;
+    if (k + 1 < g.nz && inside(v[p + (int64_t)g.nx * g.ny], g.iso) != a) m |= 4;
+    mask[p] = m;
+    cnt[p] = __popc(m);
+}
+
+// root position on a crossed edge: t = (iso - v0) / (v1 - v0), reference rounding
+__device__ __forceinline__ float root_t(float v0, float v1, float iso) {
+    return __fdiv_rn(__fsub_rn(iso, v0), __fsub_rn(v1, v0));
+}
+
+__global__ void k_mc_verts(const float* __restrict__ v, Grid g, const uint8_t* __restrict__ mask,
+                           const int64_t* __restrict__ vbase, float* __restrict__ verts) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t total = (int64_t)g.nx * g.ny * g.nz;
+    if (p >= total) return;
+    const uint8_t m = mask[p];
+    if (!m) return;
+    const int i = (int)(p % g.nx), j = (int)((p / g.nx) % g.ny), k = (int)(p / ((int64_t)g.nx * g.ny));
+    const float x = __fmaf_rn(float(i), g.h, g.ox), y = __fmaf_rn(float(j), g.h, g.oy),
+                z = __fmaf_rn(float(k), g.h, g.oz);
+    int64_t o = vbase[p];
+    const int64_t step[3] = {1, g.nx, (int64_t)g.nx * g.ny};
+    for (int a = 0; a < 3; a++) {
+        if (!((m >> a) & 1)) continue;
+        const float t = root_t(v[p], v[p + step[a]], g.iso);
+        const float d = __fmul_rn(t, g.h);
+        verts[3 * o + 0] = a == 0 ? __fadd_rn(x, d) : x;
+        verts[3 * o + 1] = a == 1 ? __fadd_rn(y, d) : y;
+        verts[3 * o + 2] = a == 2 ? __fadd_rn(z, d) : z;
+        o++;
+    }
+}
+
+__device__ __forceinline__ int cell_case(const float* __restrict__ v, const Grid& g, int64_t p) {
+    const int64_t sx = 1, sy = g.nx, sz = (int64_t)g.nx * g.ny;
+    int c = 0;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        const int64_t o = (q & 1) * sx + ((q >> 1) & 1) * sy + (q >> 2) * sz;
+        c |= inside(v[p + o], g.iso) ? (1 << q) : 0;
+    }
+    return c;
+}
+
+__global__ void k_mc_cells(const float* __restrict__ v, Grid g, int32_t* __restrict__ tcnt) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int cx = g.nx - 1, cy = g.ny - 1, cz = g.nz - 1;
+    if (c >= (int64_t)cx * cy * cz) return;
+    const int i = (int)(c % cx), j = (int)((c / cx) % cy), k = (int)(c / ((int64_t)cx * cy));
+    tcnt[c] = c_ntri[cell_case(v, g, gid(g, i, j, k))];
+}
+
+__global__ void k_mc_tris(const float* __restrict__ v, Grid g, const uint8_t* __restrict__ mask,
+                          const int64_t* __restrict__ vbase, const int64_t* __restrict__ tbase,
+                          int32_t* __restrict__ faces) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int cx = g.nx - 1, cy = g.ny - 1, cz = g.nz - 1;
+    if (c >= (int64_t)cx * cy * cz) return;
+    const int i = (int)(c % cx), j = (int)((c / cx) % cy), k = (int)(c / ((int64_t)cx * cy));
+    const int64_t p = gid(g, i, j, k);
+    const int cs = cell_case(v, g, p);
+    const int nt = c_ntri[cs];
+    if (!nt) return;
+    int64_t o = tbase[c];
+    for (int t = 0; t < nt; t++) {
+        for (int s = 0; s < 3; s++) {
+            const int e = c_tri[cs][3 * t + s];
+            const int a = e >> 2, u = e & 1, w = (e >> 1) & 1;
+            int oi = i, oj = j, ok = k;  // the grid point owning edge e of this cell
+            if (a == 0) {
+                oj += u;
+                ok += w;
+            } else if (a == 1) {
+                oi += u;
+                ok += w;
+            } else {
+                oi += u;
+                oj += w;
+            }
+            const int64_t q = gid(g, oi, oj, ok);
+            const int rank = __popc(mask[q] & ((1u << a) - 1u));
+            faces[3 * (o + t) + s] = (int32_t)(vbase[q] + rank);
+        }
+    }
+}
+
+template <typename F>
+int cub_scan(F&& f, cudaStream_t s) {
+    size_t bytes = 0;
+    CAGR_CUDA(f(nullptr, bytes));
+    void* tmp = nullptr;
+    CAGR_CUDA(cudaMallocAsync(&tmp, bytes ? bytes : 16, s));
+    cudaError_t e = f(tmp, bytes);
+    cudaFreeAsync(tmp, s);
+    if (e != cudaSuccess) return set_error(kErrCuda, cudaGetErrorString(e));
+    return kOk;
+}
+
+}  // namespace
+
+int mc_table(int8_t* tri, uint8_t* ntri) {
+    std::string err;
+    const McTable* T = host_table(err);
+    if (!T) return set_error(kErrState, "marching-cubes table: " + err);
+    if (tri) std::memcpy(tri, T->tri, sizeof(T->tri));
+    if (ntri) std::memcpy(ntri, T->ntri, sizeof(T->ntri));
+    return kOk;
+}
+
+int marching_cubes(const float* values, int nx, int ny, int nz, const double* origin,
+                   double spacing, double iso, float* verts, int64_t max_verts, int32_t* faces,
+                   int64_t max_faces, int64_t* nverts, int64_t* nfaces, cudaStream_t s) {
+    if (!values || nx < 2 || ny < 2 || nz < 2 || !nverts || !nfaces)
+        return set_error(kErrInvalid, "marching cubes needs values on a grid of at least 2^3");
+    if ((int64_t)nx * ny * nz >= (int64_t(1) << 31))
+        return set_error(kErrOverflow, "grid too large for 32-bit vertex indices");
+    if (int rc = upload_table()) return rc;
+    Grid g{nx, ny, nz, (float)origin[0], (float)origin[1], (float)origin[2], (float)spacing,
+           (float)iso};
+    const int64_t P = (int64_t)nx * ny * nz, C = (int64_t)(nx - 1) * (ny - 1) * (nz - 1);
+    uint8_t* mask = nullptr;
+    int32_t *cnt = nullptr, *tcnt = nullptr;
+    int64_t *vbase = nullptr, *tbase = nullptr;
+    auto cleanup = [&] {
+        cudaFreeAsync(mask, s);
+        cudaFreeAsync(cnt, s);
+        cudaFreeAsync(tcnt, s);
+        cudaFreeAsync(vbase, s);
+        cudaFreeAsync(tbase, s);
+    };
+    if (cudaMallocAsync((void**)&mask, P, s) != cudaSuccess ||
+        cudaMallocAsync((void**)&cnt, 4 * (P + 1), s) != cudaSuccess ||
+        cudaMallocAsync((void**)&tcnt, 4 * (C + 1), s) != cudaSuccess ||
+        cudaMallocAsync((void**)&vbase, 8 * (P + 1), s) != cudaSuccess ||
+        cudaMallocAsync((void**)&tbase, 8 * (C + 1), s) != cudaSuccess) {
+        cleanup();
+        return set_error(kErrAlloc, "marching cubes scratch");
+    }
+    cudaMemsetAsync(cnt + P, 0, 4, s);
+    cudaMemsetAsync(tcnt + C, 0, 4, s);
+    k_mc_edges<<<(unsigned)((P + kBlock - 1) / kBlock), kBlock, 0, s>>>(values, g, mask, cnt);
+    k_mc_cells<<<(unsigned)((C + kBlock - 1) / kBlock), kBlock, 0, s>>>(values, g, tcnt);
+    int rc = cub_scan([&](void* t, size_t& b) {
+        return cub::DeviceScan::ExclusiveSum(t, b, cnt, vbase, P + 1, s);
+    }, s);
+    if (!rc)
+        rc = cub_scan([&](void* t, size_t& b) {
+            return cub::DeviceScan::ExclusiveSum(t, b, tcnt, tbase, C + 1, s);
+        }, s);
+    int64_t nv = 0, nf = 0;
+    if (!rc) {
+        cudaMemcpyAsync(&nv, vbase + P, 8, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&nf, tbase + C, 8, cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) rc = set_error(kErrCuda, "marching cubes counts");
+    }
+    if (!rc) {
+        *nverts = nv;
+        *nfaces = nf;
+        if (verts && faces) {
+            if (nv > max_verts || nf > max_faces) {
+                rc = set_error(kErrOverflow, "output buffers too small for the mesh");
+            } else {
+                k_mc_verts<<<(unsigned)((P + kBlock - 1) / kBlock), kBlock, 0, s>>>(values, g, mask,
+                                                                                   vbase, verts);
+                k_mc_tris<<<(unsigned)((C + kBlock - 1) / kBlock), kBlock, 0, s>>>(
+                    values, g, mask, vbase, tbase, faces);
+                if (cudaGetLastError() != cudaSuccess) rc = set_error(kErrCuda, "marching cubes launch");
+            }
+        }
+    }
+    cleanup();
+    return rc;
+}
+
+}  // namespace cagr

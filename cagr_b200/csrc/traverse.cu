@@ -58,6 +58,9 @@ struct TravParams {
     const int32_t* qorder = nullptr;
     const T* widths = nullptr;
     T width = T(0);
+    int grid = 0;              // queries are the nodes of a regular grid
+    int gx = 0, gy = 0, gz = 0;
+    T gox = T(0), goy = T(0), goz = T(0), gh = T(0);
     T* out = nullptr;
     int out_stride = 1;
     int accumulate = 0;  // add into `out` instead of overwriting it
@@ -160,15 +163,40 @@ __device__ __forceinline__ void pair_term(Lane<T>& L, const T* __restrict__ src,
     }
 }
 
-// Loads this lane's query; returns false past the end.
+// Inverse of the 3-way bit interleave: every third bit of x, packed.
+__device__ __forceinline__ uint32_t compact3(uint64_t x) {
+    x &= 0x1249249249249249ull;
+    x = (x ^ (x >> 2)) & 0x10c30c30c30c30c3ull;
+    x = (x ^ (x >> 4)) & 0x100f00f00f00f00full;
+    x = (x ^ (x >> 8)) & 0x1f0000ff0000ffull;
+    x = (x ^ (x >> 16)) & 0x1f00000000ffffull;
+    x = (x ^ (x >> 32)) & 0x1fffffull;
+    return (uint32_t)x;
+}
+
+// Loads this lane's query; returns false past the end.  Three query sources:
+// the tree's own points (Morton order), an explicit array (optional order), or
+// the nodes of a regular grid, visited in Morton order of (i, j, k) and
+// written at (k * gy + j) * gx + i.
 template <typename T>
 __device__ __forceinline__ bool load_query(const TravParams<T>& p, int64_t qi, Lane<T>& L,
                                            int64_t& oidx, T& w) {
     w = p.width;
     oidx = 0;
     L.q0 = L.q1 = L.q2 = T(0);
-    const bool valid = qi < p.nq;
-    if (valid) {
+    bool valid = qi < p.nq;
+    if (valid && p.grid) {
+        const uint32_t i = compact3((uint64_t)qi), j = compact3((uint64_t)qi >> 1),
+                       k = compact3((uint64_t)qi >> 2);
+        valid = i < (uint32_t)p.gx && j < (uint32_t)p.gy && k < (uint32_t)p.gz;
+        if (valid) {
+            oidx = ((int64_t)k * p.gy + j) * p.gx + i;
+            L.q0 = fma(T(i), p.gh, p.gox);  // one rounding: node = origin + index * spacing
+            L.q1 = fma(T(j), p.gh, p.goy);
+            L.q2 = fma(T(k), p.gh, p.goz);
+            if (p.widths) w = p.widths[oidx];
+        }
+    } else if (valid) {
         if (p.queries == nullptr) {
             oidx = p.perm[qi];
             L.q0 = p.spos[3 * qi];
@@ -528,6 +556,20 @@ int dispatch(const Tree* t, const TraverseArgs& a, cudaStream_t s) {
     p.M = t->m;
     p.N = t->n;
     p.nq = a.queries ? a.nq : t->n;
+    if (a.grid) {
+        // Morton indices over the smallest power-of-two cube holding the grid
+        int bits = 0;
+        while ((1 << bits) < a.gx || (1 << bits) < a.gy || (1 << bits) < a.gz) bits++;
+        p.grid = 1;
+        p.gx = a.gx;
+        p.gy = a.gy;
+        p.gz = a.gz;
+        p.gox = (T)a.gorigin[0];
+        p.goy = (T)a.gorigin[1];
+        p.goz = (T)a.gorigin[2];
+        p.gh = (T)a.gspacing;
+        p.nq = int64_t(1) << (3 * bits);
+    }
     p.meta = t->meta;
     p.spos = (const T*)t->spos;
     p.perm = t->perm;
@@ -580,6 +622,9 @@ int traverse(const Tree* t, const TraverseArgs& a, cudaStream_t stream) {
     if (!a.out) return set_error(kErrInvalid, "output is null");
     if (a.queries && a.nq < 0) return set_error(kErrInvalid, "negative query count");
     if (!a.widths && !(a.width == a.width)) return set_error(kErrInvalid, "width is NaN");
+    if (a.grid && (a.queries || a.qorder || a.gx <= 0 || a.gy <= 0 || a.gz <= 0 ||
+                   a.gx > (1 << 20) || a.gy > (1 << 20) || a.gz > (1 << 20)))
+        return set_error(kErrInvalid, "grid queries need positive dims <= 2^20 and no query array");
     if (a.qorder && !a.queries)
         return set_error(kErrInvalid, "a query order needs explicit queries");
     return t->dtype == 0 ? dispatch<float>(t, a, stream) : dispatch<double>(t, a, stream);

@@ -165,6 +165,39 @@ int cagr_multiply(const cagr_tree* tree, int op, const void* queries_dev,
 int cagr_forward(cagr_tree* tree, int op, const void* values_dev, const void* widths_dev,
                  double width, int flags, void* out_dev, void* stream);
 
+/* Evaluates `op` (A, A3, A2x, G, A2_FUSED, AT, A2Tx; moments in slot 0) at the
+ * nodes of a regular nx x ny x nz grid, node (i, j, k) at origin + (i, j, k) *
+ * spacing (origin: 3 doubles in host memory), written to out_dev row
+ * (k * ny + j) * nx + i; no query array is materialised.  Widths: widths_dev
+ * (grid-shaped) or the scalar `width`.  The field evaluation of the GaussRecon
+ * driver (multiply_by_A3 with the continuous kernel at grid corners,
+ * main_GaussRecon_cuda.cu:427-445) on a regular grid. */
+int cagr_field_grid(const cagr_tree* tree, int op, int nx, int ny, int nz, const double* origin,
+                    double spacing, const void* widths_dev, double width, int flags, void* out_dev,
+                    void* stream);
+
+/* Marching cubes on float32 field values of a regular grid (values_dev
+ * [nz, ny, nx], x fastest; node (i, j, k) at origin + (i, j, k) * spacing):
+ * the surface value = iso, corners with value > iso inside, triangles wound
+ * outward (toward decreasing values).  Writes *num_vertices / *num_faces; when
+ * vertices_dev and faces_dev are non-NULL also the mesh (vertices [V,3]
+ * float32, faces [F,3] int32 indices, vertices shared between cells), or
+ * CAGR_ERR_OVERFLOW if V or F exceed the given maxima.  Synchronises `stream`.
+ * The reference extracts the surface with PoissonRecon's adaptive octree MC
+ * (gaussrecon_src/Octree.cpp:852-1090, tables MarchingCubes.cpp:32-324); this
+ * uniform-grid MC uses its own generated case table (cagr_mc_table). */
+int cagr_marching_cubes(const float* values_dev, int nx, int ny, int nz, const double* origin,
+                        double spacing, double iso, float* vertices_dev, int64_t max_vertices,
+                        int32_t* faces_dev, int64_t max_faces, int64_t* num_vertices,
+                        int64_t* num_faces, void* stream);
+
+/* The marching-cubes case table (host memory): tri[256 * 36] edge ids, three
+ * per triangle, and ntri[256] triangle counts.  Corner c = x + 2y + 4z; edge
+ * 4a + u + 2v runs along axis a with the other two coordinates (u, v) in
+ * increasing axis order.  No counterpart in the reference (its tables use
+ * PoissonRecon's numbering). */
+int cagr_mc_table(int8_t* tri, uint8_t* ntri);
+
 /* No counterpart in the reference.  Node moments (the outputs of
  * cagr_scatter_export) computed from tree arrays in the reference layout
  * (parent, children, is_leaf, npts, n2p, n2p_start as cagr_tree_export

@@ -457,3 +457,97 @@ int oracle_direct_f64(int op, const double* q, const double* qw, idx_t nq, const
     }
     return 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Marching cubes on a regular grid (checker for cagr_marching_cubes)         */
+/* ------------------------------------------------------------------------ */
+
+/* Values v[(k*ny + j)*nx + i]; node (i,j,k) at origin + (i,j,k)*h in float as
+ * fmaf(i, h, o).  A corner is inside when v > iso.  Vertices: one per crossed
+ * grid edge, grid points in index order and axes x, y, z, at
+ * o + i*h + ((iso - v0) / (v1 - v0)) * h along the edge.  Triangles: cells in
+ * index order, each with the case table's triangles (tri[256][36] edge ids,
+ * ntri[256]); edge 4a + u + 2w of cell (i,j,k) starts at the grid point offset
+ * by (u, w) along the two other axes in increasing order.  With NULL outputs
+ * only the counts are returned. */
+int oracle_marching_cubes(const float* v, int nx, int ny, int nz, double ox, double oy, double oz,
+                          double h, float iso, const signed char* tri, const unsigned char* ntri,
+                          float* verts, idx_t maxv, int* faces, idx_t maxf, idx_t* nv_out,
+                          idx_t* nf_out) {
+    const idx_t P = (idx_t)nx * ny * nz;
+    unsigned char* mask = calloc(P, 1);
+    idx_t* vbase = malloc(sizeof(idx_t) * (P + 1));
+    if (!mask || !vbase) {
+        free(mask);
+        free(vbase);
+        return -1;
+    }
+    const float fh = (float)h, fox = (float)ox, foy = (float)oy, foz = (float)oz;
+    idx_t nv = 0;
+    for (idx_t p = 0; p < P; p++) {
+        const int i = (int)(p % nx), j = (int)((p / nx) % ny), k = (int)(p / ((idx_t)nx * ny));
+        const int a = v[p] > iso;
+        unsigned char m = 0;
+        if (i + 1 < nx && (v[p + 1] > iso) != a) m |= 1;
+        if (j + 1 < ny && (v[p + nx] > iso) != a) m |= 2;
+        if (k + 1 < nz && (v[p + (idx_t)nx * ny] > iso) != a) m |= 4;
+        mask[p] = m;
+        vbase[p] = nv;
+        if (verts && m) {
+            const float x = fmaf((float)i, fh, fox), y = fmaf((float)j, fh, foy),
+                        z = fmaf((float)k, fh, foz);
+            const idx_t step[3] = {1, nx, (idx_t)nx * ny};
+            idx_t o = nv;
+            for (int ax = 0; ax < 3; ax++) {
+                if (!((m >> ax) & 1)) continue;
+                if (o >= maxv) break;
+                const float t = (iso - v[p]) / (v[p + step[ax]] - v[p]);
+                const float d = t * fh;
+                verts[3 * o + 0] = ax == 0 ? x + d : x;
+                verts[3 * o + 1] = ax == 1 ? y + d : y;
+                verts[3 * o + 2] = ax == 2 ? z + d : z;
+                o++;
+            }
+        }
+        nv += (m & 1) + ((m >> 1) & 1) + ((m >> 2) & 1);
+    }
+    vbase[P] = nv;
+    idx_t nf = 0;
+    const int cx = nx - 1, cy = ny - 1, cz = nz - 1;
+    for (idx_t c = 0; c < (idx_t)cx * cy * cz; c++) {
+        const int i = (int)(c % cx), j = (int)((c / cx) % cy), k = (int)(c / ((idx_t)cx * cy));
+        const idx_t p = ((idx_t)k * ny + j) * nx + i;
+        int cs = 0;
+        for (int q = 0; q < 8; q++) {
+            const idx_t o = (q & 1) + ((q >> 1) & 1) * (idx_t)nx + (q >> 2) * (idx_t)nx * ny;
+            if (v[p + o] > iso) cs |= 1 << q;
+        }
+        for (int t = 0; t < ntri[cs]; t++, nf++) {
+            if (!faces || nf >= maxf) continue;
+            for (int s = 0; s < 3; s++) {
+                const int e = tri[cs * 36 + 3 * t + s];
+                const int ax = e >> 2, u = e & 1, w = (e >> 1) & 1;
+                int oi = i, oj = j, ok = k;
+                if (ax == 0) {
+                    oj += u;
+                    ok += w;
+                } else if (ax == 1) {
+                    oi += u;
+                    ok += w;
+                } else {
+                    oi += u;
+                    oj += w;
+                }
+                const idx_t q = ((idx_t)ok * ny + oj) * nx + oi;
+                int rank = 0;
+                for (int b = 0; b < ax; b++) rank += (mask[q] >> b) & 1;
+                faces[3 * nf + s] = (int)(vbase[q] + rank);
+            }
+        }
+    }
+    *nv_out = nv;
+    *nf_out = nf;
+    free(mask);
+    free(vbase);
+    return 0;
+}

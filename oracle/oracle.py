@@ -201,6 +201,30 @@ class Oracle:
             raise RuntimeError("oracle direct sum failed")
         return out
 
+    def marching_cubes(self, values: np.ndarray, origin, spacing: float, iso: float,
+                       tri: np.ndarray, ntri: np.ndarray):
+        """Regular-grid marching cubes with a given case table (the checker of
+        cagr_marching_cubes).  values: [nz, ny, nx] float32."""
+        v = np.ascontiguousarray(values, np.float32)
+        nz, ny, nx = v.shape
+        tri = np.ascontiguousarray(tri, np.int8).reshape(-1)
+        ntri = np.ascontiguousarray(ntri, np.uint8)
+        f = self.lib.oracle_marching_cubes
+        f.restype = ctypes.c_int
+        f.argtypes = [_p, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 4 + \
+            [ctypes.c_float, _p, _p, _p, _i64, _p, _i64, _p, _p]
+        nv, nf = ctypes.c_int64(), ctypes.c_int64()
+        args = [_ptr(v), nx, ny, nz, float(origin[0]), float(origin[1]), float(origin[2]),
+                float(spacing), float(iso), _ptr(tri), _ptr(ntri)]
+        if f(*args, None, 0, None, 0, ctypes.byref(nv), ctypes.byref(nf)) != 0:
+            raise MemoryError("oracle marching cubes")
+        verts = np.zeros((nv.value, 3), np.float32)
+        faces = np.zeros((nf.value, 3), np.int32)
+        if f(*args, _ptr(verts), nv.value, _ptr(faces), nf.value, ctypes.byref(nv),
+             ctypes.byref(nf)) != 0:
+            raise MemoryError("oracle marching cubes")
+        return verts, faces
+
     # -- the reference's per-call composition ----------------------------------
     def forward(self, op: str, tree: Tree, points: np.ndarray, values: np.ndarray,
                 widths: np.ndarray, queries: np.ndarray | None = None,
