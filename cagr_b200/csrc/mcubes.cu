@@ -20,11 +20,13 @@
 //     its edges' inside-to-outside directions (outward), then fan-triangulated.
 // A corner is inside when value > iso (NaN is outside).
 //
-// Device pipeline (three passes over grid points and cells, two scans):
-//   edges:  per grid point, its crossed +x/+y/+z edges (bit mask) and count
-//   verts:  one vertex per crossed edge, at the linear root along the edge
-//   cells:  per cell, its case and triangle count
-//   tris:   per cell, triangles as vertex indices (shared edges share vertices)
+// Device pipeline over units of 128 consecutive grid points of one x-row:
+//   count:  per unit, its points' crossed +x/+y/+z edges and its cells' triangles
+//   scan:   per-unit counts -> each unit's first vertex and first triangle
+//   emit:   per unit, one vertex per crossed edge (the linear root along it) and
+//           each cell's triangles as vertex indices (shared edges share vertices)
+// Output order is grid-point order for vertices (edges +x, +y, +z of a point)
+// and cell order for triangles, with no per-point scratch.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -41,7 +43,7 @@ namespace cagr {
 namespace {
 
 constexpr int kMaxTri = 12;  // the generator checks the bound
-constexpr int kBlock = 256;
+constexpr int kChunk = 128;  // grid points per unit (one block)
 
 struct McTable {
     int8_t tri[256][3 * kMaxTri];
@@ -215,7 +217,7 @@ int upload_table() {
 }
 
 struct Grid {
-    int nx, ny, nz;
+    int nx, ny, nz, nchunks;
     float ox, oy, oz, h, iso;
 };
 
@@ -225,48 +227,16 @@ __device__ __forceinline__ int64_t gid(const Grid& g, int i, int j, int k) {
     return ((int64_t)k * g.ny + j) * g.nx + i;
 }
 
-// crossed edges owned by each grid point (+x, +y, +z) and their count
-__global__ void k_mc_edges(const float* __restrict__ v, Grid g, uint8_t* __restrict__ mask,
-                           int32_t* __restrict__ cnt) {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t total = (int64_t)g.nx * g.ny * g.nz;
-    if (p >= total) return;
-    const int i = (int)(p % g.nx), j = (int)((p / g.nx) % g.ny), k = (int)(p / ((int64_t)g.nx * g.ny));
+// crossed edges owned by grid point (i, j, k): bit a = the edge toward +axis a
+__device__ __forceinline__ uint32_t point_mask(const float* __restrict__ v, const Grid& g, int i,
+                                               int j, int k) {
+    const int64_t p = gid(g, i, j, k);
     const bool a = inside(v[p], g.iso);
-    uint8_t m = 0;
+    uint32_t m = 0;
     if (i + 1 < g.nx && inside(v[p + 1], g.iso) != a) m |= 1;
     if (j + 1 < g.ny && inside(v[p + g.nx], g.iso) != a) m |= 2;
     if (k + 1 < g.nz && inside(v[p + (int64_t)g.nx * g.ny], g.iso) != a) m |= 4;
-    mask[p] = m;
-    cnt[p] = __popc(m);
-}
-
-// root position on a crossed edge: t = (iso - v0) / (v1 - v0), reference rounding
-__device__ __forceinline__ float root_t(float v0, float v1, float iso) {
-    return __fdiv_rn(__fsub_rn(iso, v0), __fsub_rn(v1, v0));
-}
-
-__global__ void k_mc_verts(const float* __restrict__ v, Grid g, const uint8_t* __restrict__ mask,
-                           const int64_t* __restrict__ vbase, float* __restrict__ verts) {
-    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t total = (int64_t)g.nx * g.ny * g.nz;
-    if (p >= total) return;
-    const uint8_t m = mask[p];
-    if (!m) return;
-    const int i = (int)(p % g.nx), j = (int)((p / g.nx) % g.ny), k = (int)(p / ((int64_t)g.nx * g.ny));
-    const float x = __fmaf_rn(float(i), g.h, g.ox), y = __fmaf_rn(float(j), g.h, g.oy),
-                z = __fmaf_rn(float(k), g.h, g.oz);
-    int64_t o = vbase[p];
-    const int64_t step[3] = {1, g.nx, (int64_t)g.nx * g.ny};
-    for (int a = 0; a < 3; a++) {
-        if (!((m >> a) & 1)) continue;
-        const float t = root_t(v[p], v[p + step[a]], g.iso);
-        const float d = __fmul_rn(t, g.h);
-        verts[3 * o + 0] = a == 0 ? __fadd_rn(x, d) : x;
-        verts[3 * o + 1] = a == 1 ? __fadd_rn(y, d) : y;
-        verts[3 * o + 2] = a == 2 ? __fadd_rn(z, d) : z;
-        o++;
-    }
+    return m;
 }
 
 __device__ __forceinline__ int cell_case(const float* __restrict__ v, const Grid& g, int64_t p) {
@@ -280,44 +250,132 @@ __device__ __forceinline__ int cell_case(const float* __restrict__ v, const Grid
     return c;
 }
 
-__global__ void k_mc_cells(const float* __restrict__ v, Grid g, int32_t* __restrict__ tcnt) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int cx = g.nx - 1, cy = g.ny - 1, cz = g.nz - 1;
-    if (c >= (int64_t)cx * cy * cz) return;
-    const int i = (int)(c % cx), j = (int)((c / cx) % cy), k = (int)(c / ((int64_t)cx * cy));
-    tcnt[c] = c_ntri[cell_case(v, g, gid(g, i, j, k))];
+// root position on a crossed edge: t = (iso - v0) / (v1 - v0), reference rounding
+__device__ __forceinline__ float root_t(float v0, float v1, float iso) {
+    return __fdiv_rn(__fsub_rn(iso, v0), __fsub_rn(v1, v0));
 }
 
-__global__ void k_mc_tris(const float* __restrict__ v, Grid g, const uint8_t* __restrict__ mask,
-                          const int64_t* __restrict__ vbase, const int64_t* __restrict__ tbase,
-                          int32_t* __restrict__ faces) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int cx = g.nx - 1, cy = g.ny - 1, cz = g.nz - 1;
-    if (c >= (int64_t)cx * cy * cz) return;
-    const int i = (int)(c % cx), j = (int)((c / cx) % cy), k = (int)(c / ((int64_t)cx * cy));
-    const int64_t p = gid(g, i, j, k);
-    const int cs = cell_case(v, g, p);
-    const int nt = c_ntri[cs];
+// A unit is kChunk consecutive grid points of one x-row (and the cells whose
+// lowest corner they are).  Units in (row, chunk) order are in grid-point order,
+// so per-unit counts scanned give each unit's first vertex and triangle.
+struct Unit {
+    int i0, j, k, chunk;
+};
+
+__device__ __forceinline__ Unit unit_of(const Grid& g, int64_t u) {
+    Unit r;
+    r.chunk = (int)(u % g.nchunks);
+    const int64_t row = u / g.nchunks;
+    r.j = (int)(row % g.ny);
+    r.k = (int)(row / g.ny);
+    r.i0 = r.chunk * kChunk;
+    return r;
+}
+
+// per unit: vertices (crossed edges owned by its points), triangles (its cells)
+__global__ void __launch_bounds__(kChunk) k_mc_count(const float* __restrict__ v, Grid g,
+                                                      int32_t* __restrict__ vcnt,
+                                                      int32_t* __restrict__ tcnt) {
+    using Reduce = cub::BlockReduce<int32_t, kChunk>;
+    __shared__ typename Reduce::TempStorage tmp;
+    const Unit U = unit_of(g, blockIdx.x);
+    const int i = U.i0 + (int)threadIdx.x;
+    int32_t packed = 0;  // vertices + 2^16 * triangles (<= 3 * kChunk and kMaxTri * kChunk)
+    if (i < g.nx) {
+        packed = __popc(point_mask(v, g, i, U.j, U.k));
+        if (i + 1 < g.nx && U.j + 1 < g.ny && U.k + 1 < g.nz)
+            packed += (int32_t)c_ntri[cell_case(v, g, gid(g, i, U.j, U.k))] << 16;
+    }
+    const int32_t sum = Reduce(tmp).Sum(packed);
+    if (threadIdx.x == 0) {
+        vcnt[blockIdx.x] = sum & 0xffff;
+        tcnt[blockIdx.x] = sum >> 16;
+    }
+}
+
+// per unit: its vertices, and its cells' triangles as vertex indices.  A cell's
+// edges are owned by points in 4 point rows (dy, dz in {0, 1}) at x = i or i + 1;
+// each row's in-unit vertex prefix comes from one block scan of 4 packed 16-bit
+// counts, and x = i0 + kChunk (the next unit's first point) from that unit's base.
+__global__ void __launch_bounds__(kChunk) k_mc_emit(const float* __restrict__ v, Grid g,
+                                                     const int64_t* __restrict__ vbase,
+                                                     const int64_t* __restrict__ tbase,
+                                                     float* __restrict__ verts,
+                                                     int32_t* __restrict__ faces) {
+    using ScanV = cub::BlockScan<unsigned long long, kChunk>;
+    using ScanT = cub::BlockScan<int32_t, kChunk>;
+    __shared__ typename ScanV::TempStorage tmp_v;
+    __shared__ typename ScanT::TempStorage tmp_t;
+    __shared__ uint8_t s_mask[4][kChunk + 1];
+    __shared__ unsigned long long s_pre[kChunk];
+    __shared__ int64_t s_base[4], s_next[4];
+    const Unit U = unit_of(g, blockIdx.x);
+    const int t = (int)threadIdx.x;
+    const int i = U.i0 + t;
+    const bool cell_row = U.j + 1 < g.ny && U.k + 1 < g.nz;
+    const int rows = cell_row ? 4 : 1;
+    unsigned long long c = 0;
+    uint32_t own = 0;
+    for (int r = 0; r < rows; r++) {
+        const uint32_t m = i < g.nx ? point_mask(v, g, i, U.j + (r & 1), U.k + (r >> 1)) : 0u;
+        if (r == 0) own = m;
+        s_mask[r][t] = (uint8_t)m;
+        c |= (unsigned long long)__popc(m) << (16 * r);
+    }
+    int cs = 0, nt = 0;
+    if (cell_row && i + 1 < g.nx) {
+        cs = cell_case(v, g, gid(g, i, U.j, U.k));
+        nt = c_ntri[cs];
+    }
+    unsigned long long cpre;
+    int32_t tpre;
+    ScanV(tmp_v).ExclusiveSum(c, cpre);
+    ScanT(tmp_t).ExclusiveSum(nt, tpre);
+    s_pre[t] = cpre;
+    if (t < rows) {
+        const int64_t row = (int64_t)(U.k + (t >> 1)) * g.ny + (U.j + (t & 1));
+        s_base[t] = vbase[row * g.nchunks + U.chunk];
+        if (U.chunk + 1 < g.nchunks) {
+            s_next[t] = vbase[row * g.nchunks + U.chunk + 1];
+            s_mask[t][kChunk] = (uint8_t)point_mask(v, g, U.i0 + kChunk, U.j + (t & 1), U.k + (t >> 1));
+        }
+    }
+    __syncthreads();
+    if (own) {
+        const float x = __fmaf_rn(float(i), g.h, g.ox), y = __fmaf_rn(float(U.j), g.h, g.oy),
+                    z = __fmaf_rn(float(U.k), g.h, g.oz);
+        const int64_t p = gid(g, i, U.j, U.k);
+        const int64_t step[3] = {1, g.nx, (int64_t)g.nx * g.ny};
+        int64_t o = s_base[0] + (int64_t)(cpre & 0xffffu);
+        for (int a = 0; a < 3; a++) {
+            if (!((own >> a) & 1)) continue;
+            const float tt = root_t(v[p], v[p + step[a]], g.iso);
+            const float d = __fmul_rn(tt, g.h);
+            verts[3 * o + 0] = a == 0 ? __fadd_rn(x, d) : x;
+            verts[3 * o + 1] = a == 1 ? __fadd_rn(y, d) : y;
+            verts[3 * o + 2] = a == 2 ? __fadd_rn(z, d) : z;
+            o++;
+        }
+    }
     if (!nt) return;
-    int64_t o = tbase[c];
-    for (int t = 0; t < nt; t++) {
+    const int64_t o = tbase[blockIdx.x] + tpre;
+    for (int q = 0; q < nt; q++) {
         for (int s = 0; s < 3; s++) {
-            const int e = c_tri[cs][3 * t + s];
+            const int e = c_tri[cs][3 * q + s];
             const int a = e >> 2, u = e & 1, w = (e >> 1) & 1;
-            int oi = i, oj = j, ok = k;  // the grid point owning edge e of this cell
-            if (a == 0) {
-                oj += u;
-                ok += w;
-            } else if (a == 1) {
-                oi += u;
-                ok += w;
-            } else {
-                oi += u;
-                oj += w;
-            }
-            const int64_t q = gid(g, oi, oj, ok);
-            const int rank = __popc(mask[q] & ((1u << a) - 1u));
-            faces[3 * (o + t) + s] = (int32_t)(vbase[q] + rank);
+            // the point owning edge e of this cell, as (dx, row r = dy + 2 dz)
+            const int dx = a == 0 ? 0 : u;
+            const int dy = a == 0 ? u : (a == 1 ? 0 : w);
+            const int dz = a == 2 ? 0 : w;
+            const int r = dy + 2 * dz, li = t + dx;
+            const uint32_t below = (1u << a) - 1u;
+            int64_t id;
+            if (li < kChunk)
+                id = s_base[r] + (int64_t)((s_pre[li] >> (16 * r)) & 0xffffu) +
+                     __popc(s_mask[r][li] & below);
+            else
+                id = s_next[r] + __popc(s_mask[r][kChunk] & below);
+            faces[3 * (o + q) + s] = (int32_t)id;
         }
     }
 }
@@ -353,44 +411,42 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
     if ((int64_t)nx * ny * nz >= (int64_t(1) << 31))
         return set_error(kErrOverflow, "grid too large for 32-bit vertex indices");
     if (int rc = upload_table()) return rc;
-    Grid g{nx, ny, nz, (float)origin[0], (float)origin[1], (float)origin[2], (float)spacing,
-           (float)iso};
-    const int64_t P = (int64_t)nx * ny * nz, C = (int64_t)(nx - 1) * (ny - 1) * (nz - 1);
-    uint8_t* mask = nullptr;
-    int32_t *cnt = nullptr, *tcnt = nullptr;
+    const int nchunks = (nx + kChunk - 1) / kChunk;
+    Grid g{nx, ny, nz, nchunks, (float)origin[0], (float)origin[1], (float)origin[2],
+           (float)spacing, (float)iso};
+    const int64_t U = (int64_t)nchunks * ny * nz;
+    int32_t *vcnt = nullptr, *tcnt = nullptr;
     int64_t *vbase = nullptr, *tbase = nullptr;
     auto cleanup = [&] {
-        cudaFreeAsync(mask, s);
-        cudaFreeAsync(cnt, s);
+        cudaFreeAsync(vcnt, s);
         cudaFreeAsync(tcnt, s);
         cudaFreeAsync(vbase, s);
         cudaFreeAsync(tbase, s);
     };
-    if (cudaMallocAsync((void**)&mask, P, s) != cudaSuccess ||
-        cudaMallocAsync((void**)&cnt, 4 * (P + 1), s) != cudaSuccess ||
-        cudaMallocAsync((void**)&tcnt, 4 * (C + 1), s) != cudaSuccess ||
-        cudaMallocAsync((void**)&vbase, 8 * (P + 1), s) != cudaSuccess ||
-        cudaMallocAsync((void**)&tbase, 8 * (C + 1), s) != cudaSuccess) {
+    if (cudaMallocAsync((void**)&vcnt, 4 * (U + 1), s) != cudaSuccess ||
+        cudaMallocAsync((void**)&tcnt, 4 * (U + 1), s) != cudaSuccess ||
+        cudaMallocAsync((void**)&vbase, 8 * (U + 1), s) != cudaSuccess ||
+        cudaMallocAsync((void**)&tbase, 8 * (U + 1), s) != cudaSuccess) {
         cleanup();
         return set_error(kErrAlloc, "marching cubes scratch");
     }
-    cudaMemsetAsync(cnt + P, 0, 4, s);
-    cudaMemsetAsync(tcnt + C, 0, 4, s);
-    k_mc_edges<<<(unsigned)((P + kBlock - 1) / kBlock), kBlock, 0, s>>>(values, g, mask, cnt);
-    k_mc_cells<<<(unsigned)((C + kBlock - 1) / kBlock), kBlock, 0, s>>>(values, g, tcnt);
+    cudaMemsetAsync(vcnt + U, 0, 4, s);
+    cudaMemsetAsync(tcnt + U, 0, 4, s);
+    k_mc_count<<<(unsigned)U, kChunk, 0, s>>>(values, g, vcnt, tcnt);
     int rc = cub_scan([&](void* t, size_t& b) {
-        return cub::DeviceScan::ExclusiveSum(t, b, cnt, vbase, P + 1, s);
+        return cub::DeviceScan::ExclusiveSum(t, b, vcnt, vbase, U + 1, s);
     }, s);
     if (!rc)
         rc = cub_scan([&](void* t, size_t& b) {
-            return cub::DeviceScan::ExclusiveSum(t, b, tcnt, tbase, C + 1, s);
+            return cub::DeviceScan::ExclusiveSum(t, b, tcnt, tbase, U + 1, s);
         }, s);
     int64_t nv = 0, nf = 0;
     if (!rc) {
-        cudaMemcpyAsync(&nv, vbase + P, 8, cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(&nf, tbase + C, 8, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&nv, vbase + U, 8, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&nf, tbase + U, 8, cudaMemcpyDeviceToHost, s);
         if (cudaStreamSynchronize(s) != cudaSuccess) rc = set_error(kErrCuda, "marching cubes counts");
     }
+    if (!rc && nv > INT32_MAX) rc = set_error(kErrOverflow, "more than 2^31 - 1 vertices");
     if (!rc) {
         *nverts = nv;
         *nfaces = nf;
@@ -398,10 +454,7 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
             if (nv > max_verts || nf > max_faces) {
                 rc = set_error(kErrOverflow, "output buffers too small for the mesh");
             } else {
-                k_mc_verts<<<(unsigned)((P + kBlock - 1) / kBlock), kBlock, 0, s>>>(values, g, mask,
-                                                                                   vbase, verts);
-                k_mc_tris<<<(unsigned)((C + kBlock - 1) / kBlock), kBlock, 0, s>>>(
-                    values, g, mask, vbase, tbase, faces);
+                k_mc_emit<<<(unsigned)U, kChunk, 0, s>>>(values, g, vbase, tbase, verts, faces);
                 if (cudaGetLastError() != cudaSuccess) rc = set_error(kErrCuda, "marching cubes launch");
             }
         }

@@ -9,9 +9,9 @@ samples (:427-466), iso-value = the median of the field at the samples
 ask for regular G^3 grids, so here the grid is regular and everything up to
 the mesh stays on the GPU:
 
-    field  = cagr_field_grid(A3, continuous)      (grid nodes, Morton order)
-    iso    = median of A3 at the samples
-    mesh   = cagr_marching_cubes(field, iso)
+    field  = -cagr_field_grid(A3, continuous)     (grid nodes, Morton order)
+    iso    = -(median of A3 at the samples)
+    mesh   = cagr_marching_cubes(field, iso)       (inside = field > iso)
 """
 from __future__ import annotations
 
@@ -145,9 +145,13 @@ def reconstruct(points: torch.Tensor, mu: torch.Tensor, grid: int = 128,
     wn.scatter(attrs, weights=weights)
     samples = wn.multiply("A3", float(width), continuous=True)[:, 0]
     n = samples.shape[0]
-    iso = float(torch.kthvalue(samples.float().cpu(), n // 2 + 1).values)  # nth_element(n/2)
+    # grid value = -field and iso = -(median field at the samples), as the driver sets
+    # them (main_GaussRecon_cuda.cu:478,485-486): with outward normals the field is
+    # lower inside, so inside = value > iso
+    iso = -float(torch.kthvalue(samples.float(), n // 2 + 1).values)  # nth_element(n/2)
     spacing = (hi - lo) / (grid - 1)
     field = field_grid(wn, (grid, grid, grid), (lo, lo, lo), spacing, float(width))
+    field.neg_()
     torch.cuda.synchronize(dev)
     sec["field"] = time.perf_counter() - t0
     t0 = time.perf_counter()

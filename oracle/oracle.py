@@ -46,12 +46,15 @@ _i64 = ctypes.c_int64
 
 def build_oracle(force: bool = False) -> None:
     """Compile the C restatement (and, when the reference checkout exists,
-    the reference host build)."""
+    the reference host build and its CUDA kernels for sm_100a)."""
     if force or not os.path.exists(LIB_PATH) or (
             os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, "cagr_oracle.c"))):
         subprocess.check_call(["make", "-s", "-C", HERE, "all"])
     if os.path.isdir(REF_ROOT) and (force or not os.path.exists(REF_LIB_PATH)):
         subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF_ROOT={REF_ROOT}"])
+    gpu_lib = os.path.join(HERE, "_ref", "libwnref_gpu.so")
+    if os.path.isdir(REF_ROOT) and (force or not os.path.exists(gpu_lib)):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref-gpu", f"REF_ROOT={REF_ROOT}"])
 
 
 def _ptr(a: np.ndarray | None):

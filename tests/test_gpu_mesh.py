@@ -63,6 +63,30 @@ def test_marching_cubes_bit_exact_against_oracle(cuda_lib, oracle):
     assert np.array_equal(v_gpu.cpu().numpy(), v_ref)
 
 
+@pytest.mark.parametrize("shape", [(20, 24, 300), (9, 130, 257), (3, 2, 129)])
+def test_marching_cubes_non_cubic_multi_unit_rows(cuda_lib, oracle, shape):
+    """x-rows longer than one 128-point unit (cells whose +x corner is the next
+    unit's first point), non-cubic grids, thin slabs."""
+    import torch
+    from cagr_b200.mesh import marching_cubes, mc_table
+    nz, ny, nx = shape
+    rng = np.random.default_rng(54 + nx)
+    h = 0.01
+    z, y, x = np.meshgrid(np.arange(nz) * h, np.arange(ny) * h, np.arange(nx) * h, indexing="ij")
+    f = np.zeros(x.shape)
+    for _ in range(20):
+        c = rng.uniform(0, 1, 3) * np.array([nx, ny, nz]) * h
+        s = rng.uniform(0.02, 0.3)
+        f += np.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) / (2 * s * s))
+    vals = f.astype(np.float32)
+    iso = float(np.median(vals))
+    v_gpu, f_gpu = marching_cubes(torch.from_numpy(vals).cuda(), (0.0, 0.0, 0.0), h, iso)
+    v_ref, f_ref = oracle.marching_cubes(vals, (0.0, 0.0, 0.0), h, iso, *mc_table())
+    assert len(f_ref) > 0
+    assert np.array_equal(f_gpu.cpu().numpy(), f_ref)
+    assert np.array_equal(v_gpu.cpu().numpy(), v_ref)
+
+
 def test_reconstruct_sphere(cuda_lib):
     import torch
     from cagr_b200.mesh import reconstruct
