@@ -58,6 +58,8 @@ _SIGNATURES = {
                                    _pi64, _p]),
     "cagr_mc_table": (_i32, [_p, _p]),
     "cagr_scatter_noalloc": (_i32, [_p] * 6 + [_i64, _i32, _p, _p, _p, _i32, _p, _p, _p, _p]),
+    "cagr_pool_trim": (_i32, [_i64]),
+    "cagr_pool_reserved": (_i32, [_pi64, _pi64]),
 }
 
 _lib = None

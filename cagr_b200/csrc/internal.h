@@ -23,6 +23,11 @@ int set_error(int code, const std::string& msg);
         }                                                                                \
     } while (0)
 
+// Stream-ordered device memory from the library's per-device pool (memory.cu):
+// freed blocks stay reserved for later calls.
+int pool_alloc(void** p, size_t bytes, cudaStream_t s);
+void pool_free(void* p, cudaStream_t s);
+
 // Device arrays owned by one tree.  All pointers are device pointers.
 struct Tree {
     int dtype = 0;  // 0 = float32, 1 = float64

@@ -385,9 +385,9 @@ int cub_scan(F&& f, cudaStream_t s) {
     size_t bytes = 0;
     CAGR_CUDA(f(nullptr, bytes));
     void* tmp = nullptr;
-    CAGR_CUDA(cudaMallocAsync(&tmp, bytes ? bytes : 16, s));
+    if (int rc = pool_alloc(&tmp, bytes, s)) return rc;
     cudaError_t e = f(tmp, bytes);
-    cudaFreeAsync(tmp, s);
+    pool_free(tmp, s);
     if (e != cudaSuccess) return set_error(kErrCuda, cudaGetErrorString(e));
     return kOk;
 }
@@ -418,22 +418,23 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
     int32_t *vcnt = nullptr, *tcnt = nullptr;
     int64_t *vbase = nullptr, *tbase = nullptr;
     auto cleanup = [&] {
-        cudaFreeAsync(vcnt, s);
-        cudaFreeAsync(tcnt, s);
-        cudaFreeAsync(vbase, s);
-        cudaFreeAsync(tbase, s);
+        pool_free(vcnt, s);
+        pool_free(tcnt, s);
+        pool_free(vbase, s);
+        pool_free(tbase, s);
     };
-    if (cudaMallocAsync((void**)&vcnt, 4 * (U + 1), s) != cudaSuccess ||
-        cudaMallocAsync((void**)&tcnt, 4 * (U + 1), s) != cudaSuccess ||
-        cudaMallocAsync((void**)&vbase, 8 * (U + 1), s) != cudaSuccess ||
-        cudaMallocAsync((void**)&tbase, 8 * (U + 1), s) != cudaSuccess) {
+    int rc = pool_alloc((void**)&vcnt, 4 * (U + 1), s);
+    if (!rc) rc = pool_alloc((void**)&tcnt, 4 * (U + 1), s);
+    if (!rc) rc = pool_alloc((void**)&vbase, 8 * (U + 1), s);
+    if (!rc) rc = pool_alloc((void**)&tbase, 8 * (U + 1), s);
+    if (rc) {
         cleanup();
-        return set_error(kErrAlloc, "marching cubes scratch");
+        return rc;
     }
     cudaMemsetAsync(vcnt + U, 0, 4, s);
     cudaMemsetAsync(tcnt + U, 0, 4, s);
     k_mc_count<<<(unsigned)U, kChunk, 0, s>>>(values, g, vcnt, tcnt);
-    int rc = cub_scan([&](void* t, size_t& b) {
+    rc = cub_scan([&](void* t, size_t& b) {
         return cub::DeviceScan::ExclusiveSum(t, b, vcnt, vbase, U + 1, s);
     }, s);
     if (!rc)

@@ -235,14 +235,9 @@ __global__ void k_export_moments(const T* __restrict__ rec, int64_t M, T* __rest
     if (weights) weights[n] = r[10];
 }
 
-int ensure_slot(Tree* t, int slot, size_t elem) {
+int ensure_slot(Tree* t, int slot, size_t elem, cudaStream_t s) {
     if (t->rec[slot]) return kOk;
-    cudaError_t e = cudaMalloc(&t->rec[slot], elem * (size_t)(t->m + t->n) * CAGR_REC_STRIDE);
-    if (e != cudaSuccess) {
-        t->rec[slot] = nullptr;
-        return set_error(kErrAlloc, std::string("record allocation: ") + cudaGetErrorString(e));
-    }
-    return kOk;
+    return pool_alloc(&t->rec[slot], elem * (size_t)(t->m + t->n) * CAGR_REC_STRIDE, s);
 }
 
 template <typename T, int DIM, int NS>
@@ -269,7 +264,7 @@ int run(Tree* t, MomParams<T, DIM, NS> p, cudaStream_t s) {
 template <typename T>
 int launch_moments(Tree* t, int slot, const void* attrs, int dim, const void* weights,
                    cudaStream_t s) {
-    if (int rc = ensure_slot(t, slot, sizeof(T))) return rc;
+    if (int rc = ensure_slot(t, slot, sizeof(T), s)) return rc;
     int rc;
     if (dim == 3) {
         MomParams<T, 3, 1> p;
@@ -294,13 +289,11 @@ int launch_moments(Tree* t, int slot, const void* attrs, int dim, const void* we
 template <typename T>
 int launch_moments3(Tree* t, const void* values3, cudaStream_t s) {
     for (int k = 0; k < 3; k++)
-        if (int rc = ensure_slot(t, k, sizeof(T))) return rc;
-    if (!t->adj_nodes) {
-        cudaError_t e = cudaMalloc(&t->adj_nodes, sizeof(T) * 12 * (size_t)t->m);
-        if (e == cudaSuccess) e = cudaMalloc(&t->adj_points, sizeof(T) * 8 * (size_t)t->n);
-        if (e != cudaSuccess)
-            return set_error(kErrAlloc, std::string("adjoint records: ") + cudaGetErrorString(e));
-    }
+        if (int rc = ensure_slot(t, k, sizeof(T), s)) return rc;
+    if (!t->adj_nodes)
+        if (int rc = pool_alloc(&t->adj_nodes, sizeof(T) * 12 * (size_t)t->m, s)) return rc;
+    if (!t->adj_points)
+        if (int rc = pool_alloc(&t->adj_points, sizeof(T) * 8 * (size_t)t->n, s)) return rc;
     MomParams<T, 1, 3> p;
     p.attrs = (const T*)values3;
     p.astride = 3;

@@ -40,37 +40,20 @@ inline unsigned grid_for(int64_t n, int block = kBlock) {
     return (unsigned)((n + block - 1) / block);
 }
 
-// Stream-ordered temporary buffer.
+// Stream-ordered temporary buffer from the library's pool.
 struct Tmp {
     void* p = nullptr;
     cudaStream_t s = nullptr;
-    ~Tmp() {
-        if (p) cudaFreeAsync(p, s);
-    }
+    ~Tmp() { pool_free(p, s); }
 };
 
 int tmp_alloc(Tmp& t, size_t bytes, cudaStream_t s) {
     t.s = s;
-    if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMallocAsync(&t.p, bytes, s);
-    if (e != cudaSuccess) {
-        t.p = nullptr;
-        return set_error(kErrAlloc, std::string("cudaMallocAsync(") + std::to_string(bytes) +
-                                        "): " + cudaGetErrorString(e));
-    }
-    return kOk;
+    return pool_alloc(&t.p, bytes, s);
 }
 
-int dev_alloc(void** p, size_t bytes) {
-    if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc(p, bytes);
-    if (e != cudaSuccess) {
-        *p = nullptr;
-        return set_error(kErrAlloc, std::string("cudaMalloc(") + std::to_string(bytes) +
-                                        "): " + cudaGetErrorString(e));
-    }
-    return kOk;
-}
+// A tree array: from the pool, ordered on the build stream, freed by tree_free.
+int dev_alloc(void** p, size_t bytes, cudaStream_t s) { return pool_alloc(p, bytes, s); }
 
 // ---- step 1: Morton codes -------------------------------------------------
 
@@ -339,7 +322,7 @@ int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) 
     if (int rc = tmp_alloc(keys, sizeof(uint64_t) * n, st)) return rc;
     if (int rc = tmp_alloc(sorted_keys, sizeof(uint64_t) * n, st)) return rc;
     if (int rc = tmp_alloc(idx, sizeof(int32_t) * n, st)) return rc;
-    if (int rc = dev_alloc((void**)&t->perm, sizeof(int32_t) * n)) return rc;
+    if (int rc = dev_alloc((void**)&t->perm, sizeof(int32_t) * n, st)) return rc;
     k_morton<T><<<gN, kBlock, 0, st>>>(pts, n, D, (uint64_t*)keys.p, (int32_t*)idx.p);
     CAGR_CUDA(cudaGetLastError());
     const int end_bit = 3 * D;
@@ -410,13 +393,13 @@ int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) 
     t->num_leaves = NL;
 
     // 4: nodes
-    if (int rc = dev_alloc((void**)&t->meta, sizeof(int4) * M)) return rc;
-    if (int rc = dev_alloc((void**)&t->nchild, M)) return rc;
-    if (int rc = dev_alloc((void**)&t->parent, sizeof(int32_t) * M)) return rc;
-    if (int rc = dev_alloc((void**)&t->children, sizeof(int32_t) * M * 8)) return rc;
-    if (int rc = dev_alloc((void**)&t->leaf_ids, sizeof(int32_t) * NL)) return rc;
-    if (int rc = dev_alloc((void**)&t->n2p_start, sizeof(int64_t) * (M + 1))) return rc;
-    if (int rc = dev_alloc((void**)&t->counters, sizeof(uint32_t) * M)) return rc;
+    if (int rc = dev_alloc((void**)&t->meta, sizeof(int4) * M, st)) return rc;
+    if (int rc = dev_alloc((void**)&t->nchild, M, st)) return rc;
+    if (int rc = dev_alloc((void**)&t->parent, sizeof(int32_t) * M, st)) return rc;
+    if (int rc = dev_alloc((void**)&t->children, sizeof(int32_t) * M * 8, st)) return rc;
+    if (int rc = dev_alloc((void**)&t->leaf_ids, sizeof(int32_t) * NL, st)) return rc;
+    if (int rc = dev_alloc((void**)&t->n2p_start, sizeof(int64_t) * (M + 1), st)) return rc;
+    if (int rc = dev_alloc((void**)&t->counters, sizeof(uint32_t) * M, st)) return rc;
     CAGR_CUDA(cudaMemsetAsync(t->counters, 0, sizeof(uint32_t) * M, st));
     Tmp nchild, npts64;
     if (int rc = tmp_alloc(nchild, sizeof(int32_t) * M, st)) return rc;
@@ -444,7 +427,7 @@ int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) 
         return rc;
     int64_t L = 0;
     CAGR_CUDA(cudaMemcpyAsync(&L, t->n2p_start + M, 8, cudaMemcpyDeviceToHost, st));
-    if (int rc = dev_alloc((void**)&t->invperm, sizeof(int32_t) * n)) return rc;
+    if (int rc = dev_alloc((void**)&t->invperm, sizeof(int32_t) * n, st)) return rc;
     k_inv<<<gN, kBlock, 0, st>>>(t->perm, n, t->invperm);
     Tmp cnt, off;
     if (int rc = tmp_alloc(cnt, sizeof(int32_t) * n, st)) return rc;
@@ -466,7 +449,7 @@ int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) 
     if (int rc = tmp_alloc(pn, sizeof(int32_t) * L, st)) return rc;
     if (int rc = tmp_alloc(pp, sizeof(int32_t) * L, st)) return rc;
     if (int rc = tmp_alloc(pn2, sizeof(int32_t) * L, st)) return rc;
-    if (int rc = dev_alloc((void**)&t->n2p, sizeof(int32_t) * L)) return rc;
+    if (int rc = dev_alloc((void**)&t->n2p, sizeof(int32_t) * L, st)) return rc;
     k_walk<true><<<gN, kBlock, 0, st>>>(t->invperm, sk, t->meta, t->children, D, n, nullptr,
                                         (const int64_t*)off.p, (int32_t*)pn.p, (int32_t*)pp.p);
     CAGR_CUDA(cudaGetLastError());
@@ -481,7 +464,7 @@ int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) 
         return rc;
 
     // sorted positions
-    if (int rc = dev_alloc(&t->spos, sizeof(T) * 3 * n)) return rc;
+    if (int rc = dev_alloc(&t->spos, sizeof(T) * 3 * n, st)) return rc;
     k_spos<T><<<gN, kBlock, 0, st>>>(pts, t->perm, n, (T*)t->spos);
     CAGR_CUDA(cudaGetLastError());
 
@@ -511,20 +494,18 @@ int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) 
 
 void tree_free(Tree* t) {
     if (!t) return;
-    cudaFree(t->perm);
-    cudaFree(t->invperm);
-    cudaFree(t->meta);
-    cudaFree(t->nchild);
-    cudaFree(t->parent);
-    cudaFree(t->children);
-    cudaFree(t->leaf_ids);
-    cudaFree(t->n2p_start);
-    cudaFree(t->n2p);
-    cudaFree(t->spos);
-    cudaFree(t->counters);
-    for (int k = 0; k < 3; k++) cudaFree(t->rec[k]);
-    cudaFree(t->adj_nodes);
-    cudaFree(t->adj_points);
+    // the arrays may be in use on any stream: finish the device's work, then
+    // return them to the pool
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(t->device);
+    cudaDeviceSynchronize();
+    void* arrays[] = {t->perm,     t->invperm,  t->meta,      t->nchild, t->parent,
+                      t->children, t->leaf_ids, t->n2p_start, t->n2p,    t->spos,
+                      t->counters, t->rec[0],   t->rec[1],    t->rec[2], t->adj_nodes,
+                      t->adj_points};
+    for (void* p : arrays) pool_free(p, nullptr);
+    if (prev >= 0) cudaSetDevice(prev);
     delete t;
 }
 

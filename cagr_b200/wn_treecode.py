@@ -31,6 +31,22 @@ def _stream(device: torch.device) -> ctypes.c_void_p:
     return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
 
 
+def pool_reserved(device=None) -> tuple[int, int]:
+    """(bytes the library's memory pool on `device` holds, bytes in use)."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    r, u = ctypes.c_int64(), ctypes.c_int64()
+    with torch.cuda.device(dev):
+        check(_lib.lib().cagr_pool_reserved(ctypes.byref(r), ctypes.byref(u)), "cagr_pool_reserved")
+    return r.value, u.value
+
+
+def pool_trim(keep_bytes: int = 0, device=None) -> None:
+    """Releases reserved, unused library memory on `device` beyond keep_bytes."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    with torch.cuda.device(dev):
+        check(_lib.lib().cagr_pool_trim(int(keep_bytes)), "cagr_pool_trim")
+
+
 def _ptr(t: torch.Tensor | None) -> ctypes.c_void_p | None:
     return None if t is None else ctypes.c_void_p(t.data_ptr())
 

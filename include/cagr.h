@@ -225,6 +225,16 @@ int cagr_scatter_noalloc(const int64_t* parent_dev, const int64_t* children_dev,
  * FP32-bound traversal kernels.  Synchronises `stream`. */
 int cagr_probe_fp32_peak(int64_t iters, double* gflops, void* stream);
 
+/* Device memory (no counterpart in the reference, whose allocations are
+ * torch's): every array the library allocates -- trees, node records, build
+ * and marching-cubes scratch -- comes from one stream-ordered pool per device
+ * that keeps freed memory reserved for later calls.  cagr_pool_trim
+ * synchronises the current device and releases reserved, unused memory beyond
+ * keep_bytes; cagr_pool_reserved reports the bytes the current device's pool
+ * holds from the driver and the bytes in use. */
+int cagr_pool_trim(int64_t keep_bytes);
+int cagr_pool_reserved(int64_t* reserved_bytes, int64_t* used_bytes);
+
 #ifdef __cplusplus
 }
 #endif

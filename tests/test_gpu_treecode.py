@@ -222,3 +222,27 @@ def test_errors_are_raised(cuda_lib):
         wn.multiply("A21", 0.01)  # no moments computed yet
     with pytest.raises(AssertionError):
         wn.forward_A21(torch.zeros(99, 3, device="cuda"), 0.01)
+
+
+def test_memory_pool_reuses_freed_trees(cuda_lib):
+    """Trees and records come from the library's pool: a destroyed tree's memory
+    stays reserved and serves the next tree of the same size, with nothing in
+    use afterwards; trimming returns it to the driver."""
+    torch = _torch()
+    from cagr_b200 import WindingNumberTreecode
+    from cagr_b200.wn_treecode import pool_reserved, pool_trim
+    cloud = sphere_cloud(20000, seed=60)
+    pts = torch.from_numpy(cloud).cuda()
+    mu = torch.from_numpy(smooth_normals(cloud, seed=61)).cuda()
+    for _ in range(2):
+        wn = WindingNumberTreecode(pts)
+        wn.forward_A2(mu, 0.01)
+        wn.close()
+    reserved, used = pool_reserved()
+    assert used == 0 and reserved > 0
+    wn = WindingNumberTreecode(pts)
+    wn.forward_A2(mu, 0.01)
+    wn.close()
+    assert pool_reserved() == (reserved, 0)
+    pool_trim(0)
+    assert pool_reserved()[0] < reserved
