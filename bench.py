@@ -346,19 +346,23 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if not args.no_solve:
         from cagr_b200.mesh import reconstruct
         from cagr_b200.solver import PRESET_WIDTHS, cagr_solve
-        # untimed warm-up of the same code path on a 20k subsample (first-use
-        # module loading of every kernel and torch op the solve touches)
-        sub = P[:: max(1, P.shape[0] // 20000)].contiguous()
-        reconstruct(sub, cagr_solve(sub, *PRESET_WIDTHS["l0"]).normals, grid=64)
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        res = cagr_solve(P, *PRESET_WIDTHS["l0"])
-        torch.cuda.synchronize(dev)
-        t_solve = time.perf_counter() - t0
-        t1 = time.perf_counter()
-        rec = reconstruct(P, res.normals, grid=args.grid)
-        torch.cuda.synchronize(dev)
-        t_rec = time.perf_counter() - t1
+
+        def pipeline():
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            res = cagr_solve(P, *PRESET_WIDTHS["l0"])
+            torch.cuda.synchronize(dev)
+            t1 = time.perf_counter()
+            rec = reconstruct(P, res.normals, grid=args.grid)
+            torch.cuda.synchronize(dev)
+            return res, rec, t1 - t0, time.perf_counter() - t1
+
+        # the first run pays one-off costs (module loading of the kernels and torch
+        # ops it touches, growth of the memory pools to this size): reported apart,
+        # the second run is the number
+        _, rec, c_solve, c_rec = pipeline()
+        del rec
+        res, rec, t_solve, t_rec = pipeline()
         solve = {"total_s": round(t_solve + t_rec, 4), "solve_s": round(t_solve, 4),
                  "tree_build_s": round(res.time_tree_s, 4),
                  "iterations_s": round(res.time_main_s, 4),
@@ -366,7 +370,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                  "reconstruct_s": round(t_rec, 4), "grid": args.grid,
                  "field_s": round(rec.seconds["field"], 4),
                  "marching_cubes_s": round(rec.seconds["marching_cubes"], 4),
-                 "vertices": int(rec.vertices.shape[0]), "faces": int(rec.faces.shape[0])}
+                 "vertices": int(rec.vertices.shape[0]), "faces": int(rec.faces.shape[0]),
+                 "first_call_total_s": round(c_solve + c_rec, 4)}
         del rec
 
     # measured FP32 FMA peak (roofline denominator)

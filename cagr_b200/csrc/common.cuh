@@ -42,7 +42,10 @@ enum Status : int {
 
 __host__ __device__ inline bool node_leaf(const int4& m) { return m.z < 0; }
 __host__ __device__ inline int node_npts(const int4& m) { return m.z < 0 ? -m.z : m.z; }
-__host__ __device__ inline int node_depth(const int4& m) { return m.w; }
+__host__ __device__ inline int node_depth(const int4& m) { return m.w & 0xff; }
+// internal node whose children are all one-point leaves: children n+1 .. n+npts,
+// child c holding sorted point pstart + c
+__host__ __device__ inline bool node_twig(const int4& m) { return (m.w >> 8) & 1; }
 
 // 4-vector of T and aligned loads of one record component.
 template <typename T>

@@ -210,10 +210,16 @@ __global__ void k_emit(const uint64_t* __restrict__ sk, const int8_t* __restrict
     }
 }
 
-__global__ void k_pack(uint8_t* __restrict__ out, const int32_t* __restrict__ nchild, int64_t M) {
+// child counts as bytes; marks twigs (internal nodes with as many children as
+// points: every child is a one-point leaf) in bit 8 of meta.w
+__global__ void k_pack(uint8_t* __restrict__ out, const int32_t* __restrict__ nchild,
+                       int4* __restrict__ meta, int64_t M) {
     int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= M) return;
-    out[id] = (uint8_t)nchild[id];
+    const int c = nchild[id];
+    out[id] = (uint8_t)c;
+    const int z = meta[id].z;
+    if (z > 0 && z == c) meta[id].w |= 1 << 8;
 }
 
 __global__ void k_leaf_ids(const int32_t* __restrict__ nn, const int32_t* __restrict__ base,
@@ -410,7 +416,7 @@ int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) 
                                   (const int32_t*)base.p, (const int8_t*)d0a.p,
                                   (const int8_t*)dla.p, t->meta, t->parent, t->children,
                                   (int32_t*)nchild.p, (int64_t*)npts64.p);
-    k_pack<<<grid_for(M), kBlock, 0, st>>>(t->nchild, (const int32_t*)nchild.p, M);
+    k_pack<<<grid_for(M), kBlock, 0, st>>>(t->nchild, (const int32_t*)nchild.p, t->meta, M);
     k_leaf_ids<<<gN, kBlock, 0, st>>>((const int32_t*)nn.p, (const int32_t*)base.p,
                                       (const int8_t*)d0a.p, (const int8_t*)dla.p,
                                       (const int32_t*)leafrank.p, n, t->leaf_ids);
