@@ -58,7 +58,10 @@ struct Tree {
     //   point [N*8] : (y.x, y.y, y.z, e_0 s_0), (e_1 s_1, e_2 s_2, 0, 0),  e_k = exp(-y_k/2)
     void* adj_nodes = nullptr;
     void* adj_points = nullptr;
+    //   sums  [M*8] : (W_0, W_1, W_2, 0), (A_0, A_1, A_2, 0)  (the climb's running sums)
+    void* adj_sums = nullptr;
     bool adj_valid = false;
+    bool slot_adj[3] = {false, false, false};  // slot k's latest moments are the adjoint's
 };
 
 int tree_build(const void* points, int64_t n, int dtype, int max_depth, int leaf_size,

@@ -74,6 +74,7 @@ struct MomParams {
     T* rec[NS];
     T* adjn = nullptr;  // NS == 3: packed adjoint node records [M*12]
     T* adjp = nullptr;  // NS == 3: packed adjoint point records [N*8]
+    T* adjs = nullptr;  // NS == 3: node sums (W_k), (A_k) [M*8]
 };
 
 // Running sums of one node, per slot.
@@ -109,7 +110,8 @@ __device__ __forceinline__ void leaf_pass(const MomParams<T, DIM, NS>& p, int no
 #pragma unroll
             for (int c = 0; c < DIM; c++) a[c] = p.attrs[(int64_t)pt * p.astride + k * DIM + c];
             const T w = (NS == 1 && p.weights) ? p.weights[pt] : weight_of(a, DIM);
-            write_record<T, DIM>(p.rec[k] + (M + s) * CAGR_REC_STRIDE, pos, e, a, w, T(0));
+            if constexpr (NS == 1)
+                write_record<T, DIM>(p.rec[k] + (M + s) * CAGR_REC_STRIDE, pos, e, a, w, T(0));
             es[k] = e[k] * a[0];
         }
         if constexpr (NS == 3) {
@@ -151,6 +153,29 @@ __device__ __forceinline__ void children_pass(const MomParams<T, DIM, NS>& p, in
 #pragma unroll
     for (int q = 0; q < 8; q++) {
         if (ch[q] < 0) continue;
+        if constexpr (NS == 3) {
+            // the packed records: centroids (adjn) and sums (adjs) of the three slots
+            const T* a = p.adjn + (int64_t)ch[q] * 12;
+            const T* sm = p.adjs + (int64_t)ch[q] * 8;
+            const Vec4<T> cq[3] = {CG ? ld4_cg(a) : ld4(a), CG ? ld4_cg(a + 4) : ld4(a + 4),
+                                   CG ? ld4_cg(a + 8) : ld4(a + 8)};
+            const Vec4<T> sw = CG ? ld4_cg(sm) : ld4(sm);
+            const Vec4<T> sa = CG ? ld4_cg(sm + 4) : ld4(sm + 4);
+            const T wcs[3] = {sw.x, sw.y, sw.z};
+            const T acs[3] = {sa.x, sa.y, sa.z};
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const T wc = wcs[k];
+                const T rc[3] = {cq[k].x, cq[k].y, cq[k].z};
+                S.W[k] = add_rn(S.W[k], wc);
+                S.A[k][0] = add_rn(S.A[k][0], acs[k]);
+                for (int d = 0; d < 3; d++) {
+                    S.R[k][d] = add_rn(S.R[k][d], mul_rn(rc[d], wc));
+                    S.P[k][d] = add_rn(S.P[k][d], rc[d]);
+                }
+            }
+            continue;
+        }
 #pragma unroll
         for (int k = 0; k < NS; k++) {
             const T* r = p.rec[k] + (int64_t)ch[q] * CAGR_REC_STRIDE;
@@ -186,11 +211,19 @@ __device__ __forceinline__ void finish_node(const MomParams<T, DIM, NS>& p, int 
             const T inv = div_rn(T(1), T(count));
             for (int d = 0; d < 3; d++) c[d] = mul_rn(S.P[k][d], inv);
         }
-        exps(c, e);
-        write_record<T, DIM>(p.rec[k] + (int64_t)node * CAGR_REC_STRIDE, c, e, S.A[k], S.W[k],
-                             mac_radius2<T>(depth));
-        if constexpr (NS == 3)
-            st4<T>(p.adjn + (int64_t)node * 12 + 4 * k, make4(c[0], c[1], c[2], e[k] * S.A[k][0]));
+        if constexpr (NS == 1) {
+            exps(c, e);
+            write_record<T, DIM>(p.rec[k] + (int64_t)node * CAGR_REC_STRIDE, c, e, S.A[k], S.W[k],
+                                 mac_radius2<T>(depth));
+        } else {
+            // slot k of the adjoint needs exp(-c_k[k]/2) only
+            const T ek = exp_t(c[k] * T(-0.5));
+            st4<T>(p.adjn + (int64_t)node * 12 + 4 * k, make4(c[0], c[1], c[2], ek * S.A[k][0]));
+        }
+    }
+    if constexpr (NS == 3) {
+        st4<T>(p.adjs + (int64_t)node * 8, make4(S.W[0], S.W[1], S.W[2], T(0)));
+        st4<T>(p.adjs + (int64_t)node * 8 + 4, make4(S.A[0][0], S.A[1][0], S.A[2][0], T(0)));
     }
 }
 
@@ -219,6 +252,19 @@ __global__ void __launch_bounds__(kBlock) k_moments_climb(const MomParams<T, DIM
         depth = node_depth(pm);
         children_pass<true>(p, node, S);
     }
+}
+
+// Slot k of the packed adjoint records in the reference layout.
+template <typename T>
+__global__ void k_export_adj(const T* __restrict__ adjn, const T* __restrict__ adjs, int64_t M,
+                             int k, T* __restrict__ node_attrs, T* __restrict__ reppoints,
+                             T* __restrict__ weights) {
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= M) return;
+    if (node_attrs) node_attrs[n] = adjs[n * 8 + 4 + k];
+    if (reppoints)
+        for (int d = 0; d < 3; d++) reppoints[n * 3 + d] = adjn[n * 12 + 4 * k + d];
+    if (weights) weights[n] = adjs[n * 8 + k];
 }
 
 template <typename T, int DIM>
@@ -286,22 +332,30 @@ int launch_moments(Tree* t, int slot, const void* attrs, int dim, const void* we
     return kOk;
 }
 
+// Three scalar attributes into the packed adjoint records only (the record
+// slots are not written: the three-slot traversal reads the packed layout,
+// and export reads centroids and sums from it).  Slots 0..2 are marked empty
+// for single-slot operators until the next cagr_scatter into them.
 template <typename T>
 int launch_moments3(Tree* t, const void* values3, cudaStream_t s) {
-    for (int k = 0; k < 3; k++)
-        if (int rc = ensure_slot(t, k, sizeof(T), s)) return rc;
     if (!t->adj_nodes)
         if (int rc = pool_alloc(&t->adj_nodes, sizeof(T) * 12 * (size_t)t->m, s)) return rc;
     if (!t->adj_points)
         if (int rc = pool_alloc(&t->adj_points, sizeof(T) * 8 * (size_t)t->n, s)) return rc;
+    if (!t->adj_sums)
+        if (int rc = pool_alloc(&t->adj_sums, sizeof(T) * 8 * (size_t)t->m, s)) return rc;
     MomParams<T, 1, 3> p;
     p.attrs = (const T*)values3;
     p.astride = 3;
-    for (int k = 0; k < 3; k++) p.rec[k] = (T*)t->rec[k];
+    for (int k = 0; k < 3; k++) p.rec[k] = nullptr;
     p.adjn = (T*)t->adj_nodes;
     p.adjp = (T*)t->adj_points;
+    p.adjs = (T*)t->adj_sums;
     if (int rc = run(t, p, s)) return rc;
-    for (int k = 0; k < 3; k++) t->rec_dim[k] = 1;
+    for (int k = 0; k < 3; k++) {
+        t->rec_dim[k] = 0;
+        t->slot_adj[k] = true;
+    }
     t->adj_valid = true;
     return kOk;
 }
@@ -313,7 +367,7 @@ int moments(Tree* t, int slot, const void* attrs, int dim, const void* weights,
     if (slot < 0 || slot > 2) return set_error(kErrInvalid, "moment slot must be 0, 1 or 2");
     if (dim != 1 && dim != 3) return set_error(kErrInvalid, "attribute dim must be 1 or 3");
     if (!attrs) return set_error(kErrInvalid, "attrs is null");
-    t->adj_valid = false;  // a single-slot pass overwrites one of the adjoint's slots
+    t->slot_adj[slot] = false;  // export of this slot reads the record slot again
     return t->dtype == 0 ? launch_moments<float>(t, slot, attrs, dim, weights, stream)
                          : launch_moments<double>(t, slot, attrs, dim, weights, stream);
 }
@@ -326,9 +380,22 @@ int moments3(Tree* t, const void* values3, cudaStream_t stream) {
 
 int moments_export(const Tree* t, int slot, void* node_attrs, void* reppoints, void* weights,
                    cudaStream_t stream) {
-    if (slot < 0 || slot > 2 || !t->rec[slot] || t->rec_dim[slot] == 0)
-        return set_error(kErrState, "no moments computed in this slot");
+    if (slot < 0 || slot > 2) return set_error(kErrInvalid, "moment slot must be 0, 1 or 2");
     const unsigned grid = (unsigned)((t->m + kBlock - 1) / kBlock);
+    if (t->slot_adj[slot] && t->adj_valid) {
+        if (t->dtype == 0)
+            k_export_adj<float><<<grid, kBlock, 0, stream>>>(
+                (const float*)t->adj_nodes, (const float*)t->adj_sums, t->m, slot,
+                (float*)node_attrs, (float*)reppoints, (float*)weights);
+        else
+            k_export_adj<double><<<grid, kBlock, 0, stream>>>(
+                (const double*)t->adj_nodes, (const double*)t->adj_sums, t->m, slot,
+                (double*)node_attrs, (double*)reppoints, (double*)weights);
+        CAGR_CUDA(cudaGetLastError());
+        return kOk;
+    }
+    if (!t->rec[slot] || t->rec_dim[slot] == 0)
+        return set_error(kErrState, "no moments computed in this slot");
     const int dim = t->rec_dim[slot];
     if (t->dtype == 0) {
         if (dim == 3)

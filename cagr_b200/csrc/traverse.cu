@@ -637,16 +637,17 @@ int dispatch(const Tree* t, const TraverseArgs& a, cudaStream_t s) {
     p.accumulate = a.accumulate;
     const bool scalar_in = a.op == kOpAT || a.op == kOpA2T1 || a.op == kOpA2T2 ||
                            a.op == kOpA2T3 || a.op == kOpA2TFused;
-    const int need_dim = a.op == kOpCount ? t->rec_dim[0] : (scalar_in ? 1 : 3);
-    if (!t->rec[0] || t->rec_dim[0] == 0 || t->rec_dim[0] != need_dim)
-        return set_error(kErrState, "node moments of the right attribute dim are not computed");
-    for (int k = 0; k < 3; k++) p.rec[k] = (const T*)t->rec[0];
     const int slots = (a.op == kOpA2TFused && a.slots == 3) ? 3 : 1;
     if (slots == 3) {
         if (!t->adj_valid || !t->adj_nodes)
             return set_error(kErrState, "A2T sum needs the three-slot moments (cagr_scatter3)");
         p.adjn = (const T*)t->adj_nodes;
         p.adjp = (const T*)t->adj_points;
+    } else {
+        const int need_dim = a.op == kOpCount ? t->rec_dim[0] : (scalar_in ? 1 : 3);
+        if (!t->rec[0] || t->rec_dim[0] == 0 || t->rec_dim[0] != need_dim)
+            return set_error(kErrState, "node moments of the right attribute dim are not computed");
+        for (int k = 0; k < 3; k++) p.rec[k] = (const T*)t->rec[0];
     }
     const int out_dim = (a.op == kOpA || a.op == kOpA3 || a.op == kOpA21 || a.op == kOpA22 ||
                          a.op == kOpA23 || a.op == kOpCount)

@@ -509,7 +509,7 @@ void tree_free(Tree* t) {
     void* arrays[] = {t->perm,     t->invperm,  t->meta,      t->nchild, t->parent,
                       t->children, t->leaf_ids, t->n2p_start, t->n2p,    t->spos,
                       t->counters, t->rec[0],   t->rec[1],    t->rec[2], t->adj_nodes,
-                      t->adj_points};
+                      t->adj_points, t->adj_sums};
     for (void* p : arrays) pool_free(p, nullptr);
     if (prev >= 0) cudaSetDevice(prev);
     delete t;

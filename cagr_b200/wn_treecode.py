@@ -283,7 +283,10 @@ class WindingNumberTreecode:
         return self._forward("A3", normals, widths, continuous, queries)
 
     def scatter3(self, values3: torch.Tensor):
-        """Node moments of the three columns of values3 ([N, 3]) into slots 0..2."""
+        """Node moments of the three columns of values3 ([N, 3]), each with its own
+        |v_k| weights, into the packed records that A2T_SUM reads.  scatter_export(k, 1)
+        returns column k's moments until the next scatter into slot k; single-slot
+        operators need a scatter() first."""
         values3 = self._check_values(values3, "values")
         assert len(values3.shape) == 2 and values3.shape[1] == 3
         with torch.cuda.device(self.device):

@@ -132,9 +132,13 @@ int cagr_scatter(cagr_tree* tree, int slot, const void* attrs_dev, int attr_dim,
                  const void* weights_dev, void* stream);
 
 /* Node moments of three scalar attributes at once: column k of values3_dev
- * ([n,3], original point order) goes to slot k with weights |v_k| -- the three
+ * ([n,3], original point order) is scattered with weights |v_k| -- the three
  * scatter_point_attrs_to_nodes calls the reference makes before its A2T1,
- * A2T2 and A2T3 kernels (wn_treecode_func.py:271-351), in one launch. */
+ * A2T2 and A2T3 kernels (wn_treecode_func.py:271-351), in one launch.  The
+ * result is held in the packed records CAGR_OP_A2T_SUM reads, not in the
+ * record slots: cagr_scatter_export(tree, k, ...) returns column k's moments
+ * (attr dim 1) until the next cagr_scatter into slot k, and single-slot
+ * operators need a cagr_scatter first (they report CAGR_ERR_STATE). */
 int cagr_scatter3(cagr_tree* tree, const void* values3_dev, void* stream);
 
 /* Copies slot `slot` out in the reference layout: node_attrs [M, attr_dim],

@@ -246,3 +246,32 @@ def test_memory_pool_reuses_freed_trees(cuda_lib):
     assert pool_reserved() == (reserved, 0)
     pool_trim(0)
     assert pool_reserved()[0] < reserved
+
+
+def test_three_slot_scatter_and_slots_are_independent(cuda_lib, oracle):
+    """scatter3 fills the packed adjoint records only: single-slot operators
+    then need a scatter, a later single-slot scatter leaves the adjoint
+    records (and the export of the other columns) intact."""
+    torch = _torch()
+    from cagr_b200._lib import CagrError
+    from oracle.oracle import point_weights
+    pts = sphere_cloud(3000, seed=62)
+    s = random_values(len(pts), 3, seed=63)
+    b = random_values(len(pts), 1, seed=64)
+    wn = _tree(pts)
+    tr = oracle.build_tree(pts)
+    S = torch.from_numpy(s).cuda()
+    wn.scatter(torch.from_numpy(b).cuda())           # slot 0 holds b
+    wn.scatter3(S)                                   # slots now report the adjoint's columns
+    with pytest.raises(CagrError):
+        wn.multiply("A2T1", 0.01)                    # record slot 0 no longer current
+    first = wn.multiply("A2T_SUM", 0.01).clone()
+    wn.scatter(torch.from_numpy(b).cuda())           # slot 0 = b again
+    assert torch.equal(wn.multiply("A2T_SUM", 0.01), first)
+    a0, _, _ = (t.cpu().numpy() for t in wn.scatter_export(0, 1))
+    assert np.array_equal(a0, oracle.moments(tr, pts, point_weights(b), b).attrs)
+    col = np.ascontiguousarray(s[:, 1:2])
+    a1, r1, w1 = (t.cpu().numpy() for t in wn.scatter_export(1, 1))
+    mom = oracle.moments(tr, pts, point_weights(col), col)
+    assert np.array_equal(a1, mom.attrs) and np.array_equal(r1, mom.rep)
+    assert np.array_equal(w1, mom.weights)
