@@ -297,13 +297,28 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     d_mu = torch.empty_like(MU)
     d_w = torch.empty_like(WV)
 
+    # the copies the computation does not wait for run on a side stream: w
+    # uploads while A.mu runs, A.mu's result downloads while A^T.w runs (all of
+    # them inside the timed region: the step ends when the side stream is done)
+    side = torch.cuda.Stream(device=dev)
+    w_up, a_done = torch.cuda.Event(), torch.cuda.Event()
+
     def e2e_step():
+        side.wait_stream(stream)                 # the previous step is done with d_w
         d_mu.copy_(h_mu, non_blocking=True)
-        d_w.copy_(h_w, non_blocking=True)
+        with torch.cuda.stream(side):
+            d_w.copy_(h_w, non_blocking=True)
+            w_up.record(side)
         oa = wn.forward_A2(d_mu, W)
+        a_done.record(stream)
+        with torch.cuda.stream(side):
+            side.wait_event(a_done)
+            oa.record_stream(side)
+            h_oa.copy_(oa, non_blocking=True)
+        stream.wait_event(w_up)                  # only the upload of w
         ot = wn.forward_A2T_sum(d_w, W)
-        h_oa.copy_(oa, non_blocking=True)
         h_ot.copy_(ot, non_blocking=True)
+        stream.wait_stream(side)                 # the step ends with A.mu's download too
 
     for _ in range(2):
         e2e_step()

@@ -43,6 +43,13 @@ enum Status : int {
 __host__ __device__ inline bool node_leaf(const int4& m) { return m.z < 0; }
 __host__ __device__ inline int node_npts(const int4& m) { return m.z < 0 ? -m.z : m.z; }
 __host__ __device__ inline int node_depth(const int4& m) { return m.w & 0xff; }
+// A node record's r0.w is its acceptance radius (4 half_w)^2, negated for a
+// one-point leaf whose centroid equals its point bit for bit (then the node
+// record and the point record give identical pair terms).
+template <typename T>
+__device__ __forceinline__ T rec_radius2(T r0w) { return fabs(r0w); }
+template <typename T>
+__device__ __forceinline__ bool rec_same_leaf(T r0w) { return r0w < T(0); }
 // internal node whose children are all one-point leaves: children n+1 .. n+npts,
 // child c holding sorted point pstart + c
 __host__ __device__ inline bool node_twig(const int4& m) { return (m.w >> 8) & 1; }

@@ -5,9 +5,10 @@
 // 2*tree_depth kernels over ALL M nodes (find-next + nonleaf,
 // wn_treecode_cuda_kernels.cu:419-553).  Here one launch does the whole
 // reduction: one thread per leaf computes the leaf moments, then climbs; at
-// every parent the last-arriving child (atomic arrival counter, reset by the
-// thread that completes the node) computes the parent from its children in
-// octant order.  No thread ever waits for another.  (A level-synchronous
+// every parent the last-arriving child (arrival counter incremented by an
+// acquire-release atomic, so the last arrival sees its siblings' records; reset
+// by the thread that completes the node) computes the parent from its children
+// in octant order.  No thread ever waits for another.  (A level-synchronous
 // variant -- one launch per depth -- measured slower at 1M points: its ~15
 // dependent launches cost more than the arrival counters.)  The
 // floating-point operation order is the reference's, so node sums, weights and
@@ -213,8 +214,14 @@ __device__ __forceinline__ void finish_node(const MomParams<T, DIM, NS>& p, int 
         }
         if constexpr (NS == 1) {
             exps(c, e);
+            T r0w = mac_radius2<T>(depth);
+            // a one-point leaf whose centroid is its point exactly: the node
+            // record equals the point record for every pair term (marked by the
+            // sign of the acceptance radius)
+            if (count == 1 && c[0] == S.P[k][0] && c[1] == S.P[k][1] && c[2] == S.P[k][2])
+                r0w = -r0w;
             write_record<T, DIM>(p.rec[k] + (int64_t)node * CAGR_REC_STRIDE, c, e, S.A[k], S.W[k],
-                                 mac_radius2<T>(depth));
+                                 r0w);
         } else {
             // slot k of the adjoint needs exp(-c_k[k]/2) only
             const T ek = exp_t(c[k] * T(-0.5));
@@ -225,6 +232,14 @@ __device__ __forceinline__ void finish_node(const MomParams<T, DIM, NS>& p, int 
         st4<T>(p.adjs + (int64_t)node * 8, make4(S.W[0], S.W[1], S.W[2], T(0)));
         st4<T>(p.adjs + (int64_t)node * 8 + 4, make4(S.A[0][0], S.A[1][0], S.A[2][0], T(0)));
     }
+}
+
+// Arrival at a parent: add 1 with release (this thread's records are visible to
+// whoever arrives later) and acquire (the last arrival sees every sibling's).
+__device__ __forceinline__ uint32_t arrive_acq_rel(uint32_t* counter) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(counter) : "memory");
+    return old;
 }
 
 // Each leaf thread climbs while it is the last child to arrive at the parent.
@@ -240,12 +255,10 @@ __global__ void __launch_bounds__(kBlock) k_moments_climb(const MomParams<T, DIM
     while (true) {
         finish_node(p, node, depth, count, S);
         if (node == 0) return;
-        __threadfence();
         const int par = p.parent[node];
-        const uint32_t arrived = atomicAdd(&p.counters[par], 1u);
+        const uint32_t arrived = arrive_acq_rel(&p.counters[par]);
         if (arrived + 1u != (uint32_t)p.nchild[par]) return;
         p.counters[par] = 0u;
-        __threadfence();
         const int4 pm = p.meta[par];
         node = par;
         count = node_npts(pm);

@@ -249,14 +249,14 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p)
         T dz = sub_rn(L.q2, r0.z);
         T d2 = dist2_exact(dx, dy, dz);
         const bool active = d <= kd;
-        const bool far = d2 > r0.w;
+        const bool far = d2 > rec_radius2(r0.w);
         const bool open = active && !far;
         if (active) kd = (open && !leaf) ? d + 1 : d;
         const bool any_open = __any_sync(kFull, open);
         if (mt.z == -1) {
             // single-point leaf: far lanes take the node term, near lanes the point
             const T* src = r;
-            if (open) {
+            if (open && !rec_same_leaf(r0.w)) {
                 src = rec + ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
                 const Vec4<T> s0 = ld4(src);
                 dx = sub_rn(L.q0, s0.x);
@@ -380,12 +380,12 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t_shared(const TravP
         T dz = sub_rn(L.q2, r0.z);
         T d2 = dist2_exact(dx, dy, dz);
         const bool active = d <= kd;
-        const bool far = d2 > r0.w;
+        const bool far = d2 > rec_radius2(r0.w);
         const bool open = active && !far;
         if (active) kd = (open && !leaf) ? d + 1 : d;
         const bool any_open = __any_sync(kFull, open);
         const T* src = r;
-        if (leaf && open) {
+        if (leaf && open) {  // (the same-point flag measured slower here)
             src = rec + ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
             const Vec4<T> s0 = ld4(src);
             dx = sub_rn(L.q0, s0.x);
