@@ -181,6 +181,18 @@ def cpu_reference_step_ms(p, widths, mu, wvals, sample: int, threads: int):
     return ms, kind, desc
 
 
+def max_over_ranks(values, world: int, device):
+    """Each rank runs one replica: the job's step time is the slowest rank's.
+    A collective over the process group (NCCL on GPUs, gloo in the CPU tests)."""
+    if world <= 1:
+        return list(values)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(list(values), device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
 def run_reference_arm(args, rank: int):
     if rank != 0:
         return
@@ -396,12 +408,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                "cagr_probe_fp32_peak")
     peak_tflops = gf.value / 1e3
 
-    T = float(np.mean(step_ms))
-    E = float(np.mean(e2e_ms))
-    if world > 1:
-        t = torch.tensor([T, E], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        T, E = float(t[0]), float(t[1])
+    T, E = max_over_ranks([float(np.mean(step_ms)), float(np.mean(e2e_ms))], world, dev)
     if rank != 0:
         return
 
