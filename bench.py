@@ -41,6 +41,10 @@ UNIT = "ms"
 FLOPS_A2_FUSED = 29      # three directions
 FLOPS_A2T = 22           # d (3) + |d|^2 (5) + r^-3 (2) + e s r^-3 (2) + 3 FMA (6) + e s r^-1/2 (3) + add (1)
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the two
+# traversals on this workload, from one ncu capture of this build's kernels
+# (profiles/step_kernels_union8_1M.md); ncu is not run inside the bench
+TRAFFIC_BYTES = {"A2T_SUM": 158_257_664 + 6_055_168, "A2_FUSED": 137_173_760 + 5_257_472}
 
 
 def parse():
@@ -416,11 +420,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     a2_avg = float(np.mean(a2_ms))
     a2t_avg = float(np.mean(a2t_ms))
     if a2t_avg >= a2_avg:
-        dom, dur = "k_traverse_a2t<3 slots> (A2T_SUM)", a2t_avg
+        dom, dur, key = "k_traverse_a2t3 (A2T_SUM)", a2t_avg, "A2T_SUM"
         terms_dom, fpt = float(sum(terms_t)), FLOPS_A2T
     else:
-        dom, dur = "k_traverse<A2_FUSED>", a2_avg
+        dom, dur, key = "k_traverse<A2_FUSED>", a2_avg, "A2_FUSED"
         terms_dom, fpt = terms_a2, FLOPS_A2_FUSED
+    traffic = TRAFFIC_BYTES[key] if args.n == 1_000_000 and args.workload == "union8" else None
     achieved = terms_dom * fpt / (dur * 1e-3) / 1e12
     cpu = None
     if not args.no_cpu_baseline:
@@ -445,7 +450,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "fp32", "kernel": dom, "achieved": round(achieved, 3),
                      "peak": round(peak_tflops, 3), "unit": "TFLOP/s",
-                     "frac": round(achieved / peak_tflops, 4), "traffic": None,
+                     "frac": round(achieved / peak_tflops, 4), "traffic": traffic,
+                     "traffic_unit": "bytes per launch (ncu capture)",
                      "peak_source": "measured FP32 FMA probe (cagr_probe_fp32_peak)",
                      "pair_terms_per_launch": round(terms_dom), "flops_per_term": fpt},
         "kernels_ms": {"moments_per_step": round(float(np.mean(mom_ms)), 4),
