@@ -194,8 +194,10 @@ const McTable* host_table(std::string& err) {
     return &table;
 }
 
-__constant__ int8_t c_tri[256][3 * kMaxTri];
-__constant__ uint8_t c_ntri[256];
+// The case table in global memory, read through the read-only cache: lanes of
+// a warp index it with different cases, which constant memory would serialise.
+__device__ int8_t g_tri[256][3 * kMaxTri];
+__device__ uint8_t g_ntri[256];
 
 std::mutex g_upload_mutex;
 bool g_uploaded[64] = {};
@@ -209,8 +211,8 @@ int upload_table() {
     if (dev < 0 || dev >= 64) return set_error(kErrInvalid, "device index too large");
     std::lock_guard<std::mutex> lock(g_upload_mutex);
     if (!g_uploaded[dev]) {
-        CAGR_CUDA(cudaMemcpyToSymbol(c_tri, T->tri, sizeof(T->tri)));
-        CAGR_CUDA(cudaMemcpyToSymbol(c_ntri, T->ntri, sizeof(T->ntri)));
+        CAGR_CUDA(cudaMemcpyToSymbol(g_tri, T->tri, sizeof(T->tri)));
+        CAGR_CUDA(cudaMemcpyToSymbol(g_ntri, T->ntri, sizeof(T->ntri)));
         g_uploaded[dev] = true;
     }
     return kOk;
@@ -218,6 +220,7 @@ int upload_table() {
 
 struct Grid {
     int nx, ny, nz, nchunks;
+    int64_t units;
     float ox, oy, oz, h, iso;
 };
 
@@ -272,24 +275,57 @@ __device__ __forceinline__ Unit unit_of(const Grid& g, int64_t u) {
     return r;
 }
 
-// per unit: vertices (crossed edges owned by its points), triangles (its cells)
+// per unit: vertices (crossed edges owned by its points), triangles (its cells).
+// Each thread reads its x in the 4 point rows r = dy + 2 dz around the unit's
+// row once; warp ballots turn them into inside-bit rows in shared memory (bit x
+// of row r, x = 0 .. kChunk, the last one being the next unit's first point),
+// from which edge crossings and cell cases (corner dx + 2 r) are bit lookups.
 __global__ void __launch_bounds__(kChunk) k_mc_count(const float* __restrict__ v, Grid g,
                                                       int32_t* __restrict__ vcnt,
                                                       int32_t* __restrict__ tcnt) {
     using Reduce = cub::BlockReduce<int32_t, kChunk>;
+    constexpr int kWords = kChunk / 32;
     __shared__ typename Reduce::TempStorage tmp;
-    const Unit U = unit_of(g, blockIdx.x);
-    const int i = U.i0 + (int)threadIdx.x;
-    int32_t packed = 0;  // vertices + 2^16 * triangles (<= 3 * kChunk and kMaxTri * kChunk)
-    if (i < g.nx) {
-        packed = __popc(point_mask(v, g, i, U.j, U.k));
-        if (i + 1 < g.nx && U.j + 1 < g.ny && U.k + 1 < g.nz)
-            packed += (int32_t)c_ntri[cell_case(v, g, gid(g, i, U.j, U.k))] << 16;
-    }
-    const int32_t sum = Reduce(tmp).Sum(packed);
-    if (threadIdx.x == 0) {
-        vcnt[blockIdx.x] = sum & 0xffff;
-        tcnt[blockIdx.x] = sum >> 16;
+    __shared__ uint32_t s_bits[4][kWords + 1];
+    for (int64_t u = blockIdx.x; u < g.units; u += gridDim.x) {
+        const Unit U = unit_of(g, u);
+        const int t = (int)threadIdx.x, lane = t & 31;
+        const int i = U.i0 + t;
+        const bool has_y = U.j + 1 < g.ny, has_z = U.k + 1 < g.nz;
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const bool ok = i < g.nx && (!(r & 1) || has_y) && (!(r & 2) || has_z);
+            const bool in = ok && inside(v[gid(g, i, U.j + (r & 1), U.k + (r >> 1))], g.iso);
+            const uint32_t b = __ballot_sync(0xffffffffu, in);
+            if (lane == 0) s_bits[r][t >> 5] = b;
+        }
+        if (t < 4) {
+            const int x = U.i0 + kChunk;
+            const bool ok = x < g.nx && (!(t & 1) || has_y) && (!(t & 2) || has_z);
+            s_bits[t][kWords] =
+                (ok && inside(v[gid(g, x, U.j + (t & 1), U.k + (t >> 1))], g.iso)) ? 1u : 0u;
+        }
+        __syncthreads();
+        auto bit = [&](int r, int x) { return (int)((s_bits[r][x >> 5] >> (x & 31)) & 1u); };
+        int32_t packed = 0;  // vertices + 2^16 * triangles (<= 3 * kChunk and kMaxTri * kChunk)
+        if (i < g.nx) {
+            const int a = bit(0, t);
+            const bool has_x = i + 1 < g.nx;
+            packed = (has_x && bit(0, t + 1) != a) + (has_y && bit(1, t) != a) +
+                     (has_z && bit(2, t) != a);
+            if (has_x && has_y && has_z) {
+                int cs = 0;
+#pragma unroll
+                for (int r = 0; r < 4; r++) cs |= (bit(r, t) | (bit(r, t + 1) << 1)) << (2 * r);
+                packed += (int32_t)__ldg(&g_ntri[cs]) << 16;
+            }
+        }
+        const int32_t sum = Reduce(tmp).Sum(packed);
+        if (t == 0) {
+            vcnt[u] = sum & 0xffff;
+            tcnt[u] = sum >> 16;
+        }
+        __syncthreads();  // shared memory is reused by the next unit
     }
 }
 
@@ -309,74 +345,79 @@ __global__ void __launch_bounds__(kChunk) k_mc_emit(const float* __restrict__ v,
     __shared__ uint8_t s_mask[4][kChunk + 1];
     __shared__ unsigned long long s_pre[kChunk];
     __shared__ int64_t s_base[4], s_next[4];
-    const Unit U = unit_of(g, blockIdx.x);
-    const int t = (int)threadIdx.x;
-    const int i = U.i0 + t;
-    const bool cell_row = U.j + 1 < g.ny && U.k + 1 < g.nz;
-    const int rows = cell_row ? 4 : 1;
-    unsigned long long c = 0;
-    uint32_t own = 0;
-    for (int r = 0; r < rows; r++) {
-        const uint32_t m = i < g.nx ? point_mask(v, g, i, U.j + (r & 1), U.k + (r >> 1)) : 0u;
-        if (r == 0) own = m;
-        s_mask[r][t] = (uint8_t)m;
-        c |= (unsigned long long)__popc(m) << (16 * r);
-    }
-    int cs = 0, nt = 0;
-    if (cell_row && i + 1 < g.nx) {
-        cs = cell_case(v, g, gid(g, i, U.j, U.k));
-        nt = c_ntri[cs];
-    }
-    unsigned long long cpre;
-    int32_t tpre;
-    ScanV(tmp_v).ExclusiveSum(c, cpre);
-    ScanT(tmp_t).ExclusiveSum(nt, tpre);
-    s_pre[t] = cpre;
-    if (t < rows) {
-        const int64_t row = (int64_t)(U.k + (t >> 1)) * g.ny + (U.j + (t & 1));
-        s_base[t] = vbase[row * g.nchunks + U.chunk];
-        if (U.chunk + 1 < g.nchunks) {
-            s_next[t] = vbase[row * g.nchunks + U.chunk + 1];
-            s_mask[t][kChunk] = (uint8_t)point_mask(v, g, U.i0 + kChunk, U.j + (t & 1), U.k + (t >> 1));
+    for (int64_t u = blockIdx.x; u < g.units; u += gridDim.x) {
+        // a unit with neither vertices nor triangles (most of the grid) has nothing
+        // to emit; the test is the same for the whole block
+        if (vbase[u + 1] == vbase[u] && tbase[u + 1] == tbase[u]) continue;
+        const Unit U = unit_of(g, u);
+        const int t = (int)threadIdx.x;
+        const int i = U.i0 + t;
+        const bool cell_row = U.j + 1 < g.ny && U.k + 1 < g.nz;
+        const int rows = cell_row ? 4 : 1;
+        unsigned long long c = 0;
+        uint32_t own = 0;
+        for (int r = 0; r < rows; r++) {
+            const uint32_t m = i < g.nx ? point_mask(v, g, i, U.j + (r & 1), U.k + (r >> 1)) : 0u;
+            if (r == 0) own = m;
+            s_mask[r][t] = (uint8_t)m;
+            c |= (unsigned long long)__popc(m) << (16 * r);
         }
-    }
-    __syncthreads();
-    if (own) {
-        const float x = __fmaf_rn(float(i), g.h, g.ox), y = __fmaf_rn(float(U.j), g.h, g.oy),
-                    z = __fmaf_rn(float(U.k), g.h, g.oz);
-        const int64_t p = gid(g, i, U.j, U.k);
-        const int64_t step[3] = {1, g.nx, (int64_t)g.nx * g.ny};
-        int64_t o = s_base[0] + (int64_t)(cpre & 0xffffu);
-        for (int a = 0; a < 3; a++) {
-            if (!((own >> a) & 1)) continue;
-            const float tt = root_t(v[p], v[p + step[a]], g.iso);
-            const float d = __fmul_rn(tt, g.h);
-            verts[3 * o + 0] = a == 0 ? __fadd_rn(x, d) : x;
-            verts[3 * o + 1] = a == 1 ? __fadd_rn(y, d) : y;
-            verts[3 * o + 2] = a == 2 ? __fadd_rn(z, d) : z;
-            o++;
+        int cs = 0, nt = 0;
+        if (cell_row && i + 1 < g.nx) {
+            cs = cell_case(v, g, gid(g, i, U.j, U.k));
+            nt = __ldg(&g_ntri[cs]);
         }
-    }
-    if (!nt) return;
-    const int64_t o = tbase[blockIdx.x] + tpre;
-    for (int q = 0; q < nt; q++) {
-        for (int s = 0; s < 3; s++) {
-            const int e = c_tri[cs][3 * q + s];
-            const int a = e >> 2, u = e & 1, w = (e >> 1) & 1;
-            // the point owning edge e of this cell, as (dx, row r = dy + 2 dz)
-            const int dx = a == 0 ? 0 : u;
-            const int dy = a == 0 ? u : (a == 1 ? 0 : w);
-            const int dz = a == 2 ? 0 : w;
-            const int r = dy + 2 * dz, li = t + dx;
-            const uint32_t below = (1u << a) - 1u;
-            int64_t id;
-            if (li < kChunk)
-                id = s_base[r] + (int64_t)((s_pre[li] >> (16 * r)) & 0xffffu) +
-                     __popc(s_mask[r][li] & below);
-            else
-                id = s_next[r] + __popc(s_mask[r][kChunk] & below);
-            faces[3 * (o + q) + s] = (int32_t)id;
+        unsigned long long cpre;
+        int32_t tpre;
+        ScanV(tmp_v).ExclusiveSum(c, cpre);
+        ScanT(tmp_t).ExclusiveSum(nt, tpre);
+        s_pre[t] = cpre;
+        if (t < rows) {
+            const int64_t row = (int64_t)(U.k + (t >> 1)) * g.ny + (U.j + (t & 1));
+            s_base[t] = vbase[row * g.nchunks + U.chunk];
+            if (U.chunk + 1 < g.nchunks) {
+                s_next[t] = vbase[row * g.nchunks + U.chunk + 1];
+                s_mask[t][kChunk] = (uint8_t)point_mask(v, g, U.i0 + kChunk, U.j + (t & 1), U.k + (t >> 1));
+            }
         }
+        __syncthreads();
+        if (own) {
+            const float x = __fmaf_rn(float(i), g.h, g.ox), y = __fmaf_rn(float(U.j), g.h, g.oy),
+                        z = __fmaf_rn(float(U.k), g.h, g.oz);
+            const int64_t p = gid(g, i, U.j, U.k);
+            const int64_t step[3] = {1, g.nx, (int64_t)g.nx * g.ny};
+            int64_t o = s_base[0] + (int64_t)(cpre & 0xffffu);
+            for (int a = 0; a < 3; a++) {
+                if (!((own >> a) & 1)) continue;
+                const float tt = root_t(v[p], v[p + step[a]], g.iso);
+                const float d = __fmul_rn(tt, g.h);
+                verts[3 * o + 0] = a == 0 ? __fadd_rn(x, d) : x;
+                verts[3 * o + 1] = a == 1 ? __fadd_rn(y, d) : y;
+                verts[3 * o + 2] = a == 2 ? __fadd_rn(z, d) : z;
+                o++;
+            }
+        }
+        const int64_t o = tbase[u] + tpre;
+        for (int q = 0; q < nt; q++) {
+            for (int s = 0; s < 3; s++) {
+                const int e = __ldg(&g_tri[cs][3 * q + s]);
+                const int a = e >> 2, u = e & 1, w = (e >> 1) & 1;
+                // the point owning edge e of this cell, as (dx, row r = dy + 2 dz)
+                const int dx = a == 0 ? 0 : u;
+                const int dy = a == 0 ? u : (a == 1 ? 0 : w);
+                const int dz = a == 2 ? 0 : w;
+                const int r = dy + 2 * dz, li = t + dx;
+                const uint32_t below = (1u << a) - 1u;
+                int64_t id;
+                if (li < kChunk)
+                    id = s_base[r] + (int64_t)((s_pre[li] >> (16 * r)) & 0xffffu) +
+                         __popc(s_mask[r][li] & below);
+                else
+                    id = s_next[r] + __popc(s_mask[r][kChunk] & below);
+                faces[3 * (o + q) + s] = (int32_t)id;
+            }
+        }
+        __syncthreads();  // shared memory is reused by the next unit
     }
 }
 
@@ -412,9 +453,12 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
         return set_error(kErrOverflow, "grid too large for 32-bit vertex indices");
     if (int rc = upload_table()) return rc;
     const int nchunks = (nx + kChunk - 1) / kChunk;
-    Grid g{nx, ny, nz, nchunks, (float)origin[0], (float)origin[1], (float)origin[2],
-           (float)spacing, (float)iso};
     const int64_t U = (int64_t)nchunks * ny * nz;
+    Grid g{nx, ny, nz, nchunks, U, (float)origin[0], (float)origin[1], (float)origin[2],
+           (float)spacing, (float)iso};
+    // one block per unit (measured faster than resident blocks looping over the
+    // units); the kernels loop over units with a grid stride all the same
+    const unsigned grid_c = (unsigned)U, grid_e = (unsigned)U;
     int32_t *vcnt = nullptr, *tcnt = nullptr;
     int64_t *vbase = nullptr, *tbase = nullptr;
     auto cleanup = [&] {
@@ -433,7 +477,7 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
     }
     cudaMemsetAsync(vcnt + U, 0, 4, s);
     cudaMemsetAsync(tcnt + U, 0, 4, s);
-    k_mc_count<<<(unsigned)U, kChunk, 0, s>>>(values, g, vcnt, tcnt);
+    k_mc_count<<<grid_c, kChunk, 0, s>>>(values, g, vcnt, tcnt);
     rc = cub_scan([&](void* t, size_t& b) {
         return cub::DeviceScan::ExclusiveSum(t, b, vcnt, vbase, U + 1, s);
     }, s);
@@ -455,7 +499,7 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
             if (nv > max_verts || nf > max_faces) {
                 rc = set_error(kErrOverflow, "output buffers too small for the mesh");
             } else {
-                k_mc_emit<<<(unsigned)U, kChunk, 0, s>>>(values, g, vbase, tbase, verts, faces);
+                k_mc_emit<<<grid_e, kChunk, 0, s>>>(values, g, vbase, tbase, verts, faces);
                 if (cudaGetLastError() != cudaSuccess) rc = set_error(kErrCuda, "marching cubes launch");
             }
         }
