@@ -21,14 +21,16 @@ CAGR_OK = 0
 CAGR_F32, CAGR_F64 = 0, 1
 # operators
 OPS = {"A": 0, "AT": 1, "A3": 2, "A21": 3, "A22": 4, "A23": 5, "A2T1": 6, "A2T2": 7,
-       "A2T3": 8, "G": 9, "A2_FUSED": 10, "A2T_SUM": 11, "COUNT": 12, "A2T_SUM_SHARED": 13}
+       "A2T3": 8, "G": 9, "A2_FUSED": 10, "A2T_SUM": 11, "COUNT": 12, "A2T_SUM_SHARED": 13,
+       "A2_INSIDE": 14}
 # multiply flags
 FLAG_CONTINUOUS = 1
 FLAG_ACCUMULATE = 2
 ATTR_DIM = {"A": 3, "AT": 1, "A3": 3, "A21": 3, "A22": 3, "A23": 3, "A2T1": 1, "A2T2": 1,
-            "A2T3": 1, "G": 3, "A2_FUSED": 3, "A2T_SUM": 3, "A2T_SUM_SHARED": 1}
+            "A2T3": 1, "G": 3, "A2_FUSED": 3, "A2T_SUM": 3, "A2T_SUM_SHARED": 1, "A2_INSIDE": 3}
 OUT_DIM = {"A": 1, "AT": 3, "A3": 1, "A21": 1, "A22": 1, "A23": 1, "A2T1": 3, "A2T2": 3,
-           "A2T3": 3, "G": 3, "A2_FUSED": 3, "A2T_SUM": 3, "A2T_SUM_SHARED": 3, "COUNT": 1}
+           "A2T3": 3, "G": 3, "A2_FUSED": 3, "A2T_SUM": 3, "A2T_SUM_SHARED": 3, "COUNT": 1,
+           "A2_INSIDE": 4}
 
 _p = ctypes.c_void_p
 _i64 = ctypes.c_int64
@@ -59,6 +61,7 @@ _SIGNATURES = {
     "cagr_mc_table": (_i32, [_p, _p]),
     "cagr_scatter_noalloc": (_i32, [_p] * 6 + [_i64, _i32, _p, _p, _p, _i32, _p, _p, _p, _p]),
     "cagr_pool_trim": (_i32, [_i64]),
+    "cagr_adjoint": (_i32, [_p, _i32, _p, ctypes.c_double, _i32, _p, _p, _p]),
     "cagr_pool_reserved": (_i32, [_pi64, _pi64]),
 }
 

@@ -48,6 +48,7 @@ int op_attr_dim(int op) {
         case CAGR_OP_A2T_SUM: return 3;         // three scalar columns, one per slot
         case CAGR_OP_A2T_SUM_SHARED: return 1;  // one scalar column shared by the three
         case CAGR_OP_COUNT: return -1;  // any: counts with whatever slot 0 holds
+        case CAGR_OP_A2_INSIDE: return 3;
         default: return 0;
     }
 }
@@ -162,6 +163,22 @@ int cagr_multiply(const cagr_tree* tree, int op, const void* queries_dev,
     a.out = out_dev;
     a.out_stride = (int)out_stride;
     return cagr::traverse(tree->t, a, as_stream(stream));
+}
+
+int cagr_adjoint(cagr_tree* tree, int op, const void* widths_dev, double width, int flags,
+                 const void* grad_out_dev, void* grad_attrs_dev, void* stream) {
+    if (int rc = check_tree(tree)) return rc;
+    if (op != CAGR_OP_A2_FUSED)
+        return set_error(CAGR_ERR_INVALID, "the adjoint is implemented for CAGR_OP_A2_FUSED");
+    if (flags & ~CAGR_FLAG_CONTINUOUS) return set_error(CAGR_ERR_INVALID, "unknown flag bits");
+    if (!grad_out_dev || !grad_attrs_dev)
+        return set_error(CAGR_ERR_INVALID, "grad_out and grad_attrs must be device buffers");
+    cagr::TraverseArgs a;
+    a.op = cagr::kOpA2Fused;
+    a.continuous = (flags & CAGR_FLAG_CONTINUOUS) ? 1 : 0;
+    a.widths = widths_dev;
+    a.width = width;
+    return cagr::adjoint(tree->t, a, grad_out_dev, grad_attrs_dev, as_stream(stream));
 }
 
 int cagr_field_grid(const cagr_tree* tree, int op, int nx, int ny, int nz,

@@ -98,6 +98,7 @@ enum Op : int {
     kOpA2Fused = 10,    // (A21, A22, A23) in one traversal -> [N', 3]
     kOpA2TFused = 11,   // sum_k A2Tk(s_k) with slot k holding s_k -> [N', 3]
     kOpCount = 12,      // pair terms per query with the slot-0 moments -> [N', 1]
+    kOpA2Inside = 14,   // sums over inside-width pair terms (d.m, m_0, m_1, m_2) -> [N', 4]
 };
 
 struct TraverseArgs {
@@ -121,6 +122,12 @@ struct TraverseArgs {
 };
 
 int traverse(const Tree* t, const TraverseArgs& a, cudaStream_t stream);
+
+// J^T grad for the fused A2 on the tree's points (a.op = kOpA2Fused; a.widths,
+// a.width, a.continuous as in the forward); grad and grad_attrs [n,3] in
+// original point order.
+int adjoint(const Tree* t, const TraverseArgs& a, const void* grad, void* grad_attrs,
+            cudaStream_t stream);
 
 // Marching cubes (mcubes.cu).  The case table: tri[256][36] edge ids (12
 // triangles at most) and ntri[256].

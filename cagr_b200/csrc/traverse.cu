@@ -70,6 +70,9 @@ struct TravParams {
     T* out = nullptr;
     int out_stride = 1;
     int accumulate = 0;  // add into `out` instead of overwriting it
+    const T* g = nullptr;  // adjoint: d loss / d out per query [nq, 3], original order
+    T* accn = nullptr;     // adjoint: per-node accumulators [M, 3]
+    T* accp = nullptr;     // adjoint: per-point accumulators [N, 3], Morton order
 };
 
 template <typename T>
@@ -83,7 +86,7 @@ struct OpInfo {
                                OP == kOpA2Fused;
     static constexpr bool a2t = OP == kOpA2T1 || OP == kOpA2T2 || OP == kOpA2T3;
     static constexpr bool uses_exp = a2 || a2t;
-    static constexpr bool dim3 = a2 || OP == kOpA || OP == kOpG;
+    static constexpr bool dim3 = a2 || OP == kOpA || OP == kOpG || OP == kOpA2Inside;
     // which convection direction a single-direction operator uses
     static constexpr int k [[maybe_unused]] = (OP == kOpA21 || OP == kOpA2T1)   ? 0
                                               : (OP == kOpA22 || OP == kOpA2T2) ? 1
@@ -123,6 +126,14 @@ __device__ __forceinline__ void pair_term(Lane<T>& L, const T* __restrict__ src,
             if constexpr (OP == kOpA) {
                 L.acc0 += dm * rinv3;
                 if (CONT && !outside) L.in0 += dm * L.iw3;
+            } else if constexpr (OP == kOpA2Inside) {
+                // the continuous kernel's inside-width sums (the width derivative)
+                if (!outside) {
+                    L.acc0 += dm;
+                    L.in0 += m0;
+                    L.in1 += m1;
+                    L.in2 += m2;
+                }
             } else if constexpr (OP == kOpG) {
                 const T rinv5 = rinv3 * rinv * rinv;
                 const T c = T(3) * dm * rinv5;
@@ -318,6 +329,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p)
         put(o, 0, L.acc0 + L.in0, acc);
     } else if constexpr (OP == kOpCount) {
         put(o, 0, L.acc0, acc);
+    } else if constexpr (OP == kOpA2Inside) {
+        put(o, 0, L.acc0, acc);
+        put(o, 1, L.in0, acc);
+        put(o, 2, L.in1, acc);
+        put(o, 3, L.in2, acc);
     } else {
         put(o, 0, L.acc0, acc);
         put(o, 1, L.acc1, acc);
@@ -652,7 +668,7 @@ int dispatch(const Tree* t, const TraverseArgs& a, cudaStream_t s) {
     const int out_dim = (a.op == kOpA || a.op == kOpA3 || a.op == kOpA21 || a.op == kOpA22 ||
                          a.op == kOpA23 || a.op == kOpCount)
                             ? 1
-                            : 3;
+                            : (a.op == kOpA2Inside ? 4 : 3);
     p.out_stride = a.out_stride > 0 ? a.out_stride : out_dim;
     if (p.nq == 0) return kOk;
     switch (a.op) {
@@ -669,8 +685,216 @@ int dispatch(const Tree* t, const TraverseArgs& a, cudaStream_t s) {
         case kOpA2Fused: return launch_op<T, kOpA2Fused>(p, a.continuous, 1, s);
         case kOpA2TFused: return launch_op<T, kOpA2TFused>(p, 0, slots, s);
         case kOpCount: return launch_op<T, kOpCount>(p, 0, 1, s);
+        case kOpA2Inside: return launch_op<T, kOpA2Inside>(p, 0, 1, s);
         default: return set_error(kErrInvalid, "unknown operator " + std::to_string(a.op));
     }
+}
+
+// ---- adjoint of the fused A2 ------------------------------------------------
+//
+// With the forward's moments (same centroids, decisions and pair terms) the
+// fused A2 is linear in the attributes: out_k(x) = sum over terms of
+// ex_k(x) e_k(src) (d . m / r^3 + m_k / (2r)) outside the width, plus
+// e^w (d . m / w^3 + m_k / (2w)) inside it (continuous kernel), where m is the
+// source's attribute sum (a node: the sum over its points).  So
+//   d loss / d m_src = sum over the terms using src of
+//       sum_k g_k ex_k e_k (d / r^3 + u_k / (2r))     (outside)
+//       sum_k g_k e^w (d / w^3 + u_k / (2w))          (inside, continuous)
+// and d loss / d mu_j = the sum of that over j's point terms and over every
+// node containing j.  k_adjoint_a2 walks exactly as k_traverse<A2Fused> and
+// adds each term's vector into the node or point it used (all lanes taking a
+// term at a visit use the same node or point: one warp sum, one atomic add per
+// component); k_adj_push adds the leaf-to-root node sums to each point's own.
+
+// Adds (a, b, c) of the lanes with `take` into dst[0..2] (the same dst for all
+// of them); called by the whole warp.
+template <typename T>
+__device__ __forceinline__ void warp_red3(bool take, T a, T b, T c, T* dst) {
+    const unsigned m = __ballot_sync(kFull, take);
+    if (m == 0u) return;
+    if (!take) a = b = c = T(0);
+    if (__popc(m) > 1) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(kFull, a, o);
+            b += __shfl_xor_sync(kFull, b, o);
+            c += __shfl_xor_sync(kFull, c, o);
+        }
+    }
+    if ((int)(threadIdx.x & 31) == __ffs(m) - 1) {
+        atomicAdd(dst, a);
+        atomicAdd(dst + 1, b);
+        atomicAdd(dst + 2, c);
+    }
+}
+
+// d loss / d m of one term; G_k = g_k ex_k(x) (query side), gs_k = g_k, ew = e^w
+template <typename T, bool CONT>
+__device__ __forceinline__ void adj_term(const Lane<T>& L, const T* src, T dx, T dy, T dz, T d2,
+                                         const T* G, const T* gs, T ew, T* v) {
+    if (d2 >= L.tw) {
+        const T rinv = rsqrt_t(d2);
+        const Vec4<T> r1 = ld4(src + 4);  // (e1, e2, e3, a0)
+        const T G0 = G[0] * r1.x, G1 = G[1] * r1.y, G2 = G[2] * r1.z;
+        const T c = (G0 + G1 + G2) * (rinv * rinv * rinv);
+        const T h = T(0.5) * rinv;
+        v[0] = dx * c + h * G0;
+        v[1] = dy * c + h * G1;
+        v[2] = dz * c + h * G2;
+    } else if (CONT) {
+        const T c = (gs[0] + gs[1] + gs[2]) * ew * L.iw3;
+        const T h = T(0.5) * ew * L.iw;
+        v[0] = dx * c + h * gs[0];
+        v[1] = dy * c + h * gs[1];
+        v[2] = dz * c + h * gs[2];
+    } else {
+        v[0] = v[1] = v[2] = T(0);
+    }
+}
+
+template <typename T, bool CONT>
+__global__ void __launch_bounds__(kWarps * 32) k_adjoint_a2(const TravParams<T> p) {
+    const int lane = threadIdx.x & 31;
+    const int64_t qi = ((int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32 + lane;
+    if (__all_sync(kFull, qi >= p.nq)) return;
+    Lane<T> L;
+    int64_t oidx;
+    T w;
+    const bool valid = load_query(p, qi, L, oidx, w);
+    T gs[3] = {T(0), T(0), T(0)};
+    if (valid)
+        for (int k = 0; k < 3; k++) gs[k] = p.g[oidx * 3 + k];
+    const T G[3] = {gs[0] * exp_t(L.q0 * T(0.5)), gs[1] * exp_t(L.q1 * T(0.5)),
+                    gs[2] * exp_t(L.q2 * T(0.5))};
+    const T ew = CONT ? exp_t(w) : T(0);
+
+    const int M = (int)p.M;
+    const T* __restrict__ rec = p.rec[0];
+    int kd = valid ? 0 : -1;
+    int n = 0;
+    while (n < M) {
+        const int4 mt = __ldg(p.meta + n);
+        const int d = node_depth(mt);
+        const bool leaf = node_leaf(mt);
+        const T* r = rec + (int64_t)n * CAGR_REC_STRIDE;
+        const Vec4<T> r0 = ld4(r);
+        T dx = sub_rn(L.q0, r0.x);
+        T dy = sub_rn(L.q1, r0.y);
+        T dz = sub_rn(L.q2, r0.z);
+        T d2 = dist2_exact(dx, dy, dz);
+        const bool active = d <= kd;
+        const bool far = d2 > rec_radius2(r0.w);
+        const bool open = active && !far;
+        if (active) kd = (open && !leaf) ? d + 1 : d;
+        const bool any_open = __any_sync(kFull, open);
+        if (mt.z == -1) {
+            // one-point leaf: the node record for far lanes, the point for near ones
+            const bool use_pt = open && !rec_same_leaf(r0.w);
+            const T* src = r;
+            if (use_pt) {
+                src = rec + ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
+                const Vec4<T> s0 = ld4(src);
+                dx = sub_rn(L.q0, s0.x);
+                dy = sub_rn(L.q1, s0.y);
+                dz = sub_rn(L.q2, s0.z);
+                d2 = dist2_exact(dx, dy, dz);
+            }
+            T v[3];
+            adj_term<T, CONT>(L, src, dx, dy, dz, d2, G, gs, ew, v);
+            warp_red3(active && !use_pt, v[0], v[1], v[2], p.accn + (int64_t)n * 3);
+            warp_red3(active && use_pt, v[0], v[1], v[2], p.accp + (int64_t)mt.y * 3);
+            n = mt.x;
+            continue;
+        }
+        {
+            T v[3];
+            adj_term<T, CONT>(L, r, dx, dy, dz, d2, G, gs, ew, v);
+            warp_red3(active && far, v[0], v[1], v[2], p.accn + (int64_t)n * 3);
+        }
+        if (leaf) {
+            const int np = -mt.z;
+            if (any_open) {
+                const T* pr = rec + ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
+                for (int j = 0; j < np; j++, pr += CAGR_REC_STRIDE) {
+                    const Vec4<T> s0 = ld4(pr);
+                    const T ex = sub_rn(L.q0, s0.x);
+                    const T ey = sub_rn(L.q1, s0.y);
+                    const T ez = sub_rn(L.q2, s0.z);
+                    T v[3];
+                    adj_term<T, CONT>(L, pr, ex, ey, ez, dist2_exact(ex, ey, ez), G, gs, ew, v);
+                    warp_red3(open, v[0], v[1], v[2], p.accp + ((int64_t)mt.y + j) * 3);
+                }
+            }
+            n = mt.x;
+        } else {
+            n = any_open ? n + 1 : mt.x;
+        }
+    }
+}
+
+// per leaf: the sum of its and its ancestors' node vectors, added to each of
+// its points' own vector; written in original point order
+template <typename T>
+__global__ void k_adj_push(const int32_t* __restrict__ leaf_ids, int64_t num_leaves,
+                           const int4* __restrict__ meta, const int32_t* __restrict__ parent,
+                           const int32_t* __restrict__ perm, const T* __restrict__ accn,
+                           const T* __restrict__ accp, T* __restrict__ grad) {
+    const int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= num_leaves) return;
+    const int leafn = leaf_ids[li];
+    T s0 = T(0), s1 = T(0), s2 = T(0);
+    for (int n = leafn; n >= 0; n = parent[n]) {
+        s0 += accn[(int64_t)n * 3];
+        s1 += accn[(int64_t)n * 3 + 1];
+        s2 += accn[(int64_t)n * 3 + 2];
+    }
+    const int4 lm = meta[leafn];
+    const int np = node_npts(lm);
+    for (int j = 0; j < np; j++) {
+        const int64_t s = (int64_t)lm.y + j;
+        const int64_t pt = perm[s];
+        grad[pt * 3] = accp[s * 3] + s0;
+        grad[pt * 3 + 1] = accp[s * 3 + 1] + s1;
+        grad[pt * 3 + 2] = accp[s * 3 + 2] + s2;
+    }
+}
+
+template <typename T>
+int adjoint_impl(const Tree* t, const TraverseArgs& a, const void* grad, void* grad_attrs,
+                 cudaStream_t s) {
+    TravParams<T> p;
+    p.M = t->m;
+    p.N = t->n;
+    p.nq = t->n;
+    p.meta = t->meta;
+    p.spos = (const T*)t->spos;
+    p.perm = t->perm;
+    p.widths = (const T*)a.widths;
+    p.width = (T)a.width;
+    for (int k = 0; k < 3; k++) p.rec[k] = (const T*)t->rec[0];
+    p.g = (const T*)grad;
+    if (p.nq == 0) return kOk;
+    void *accn = nullptr, *accp = nullptr;
+    int rc = pool_alloc(&accn, sizeof(T) * 3 * (size_t)t->m, s);
+    if (!rc) rc = pool_alloc(&accp, sizeof(T) * 3 * (size_t)t->n, s);
+    if (!rc) {
+        p.accn = (T*)accn;
+        p.accp = (T*)accp;
+        cudaMemsetAsync(accn, 0, sizeof(T) * 3 * (size_t)t->m, s);
+        cudaMemsetAsync(accp, 0, sizeof(T) * 3 * (size_t)t->n, s);
+        const int64_t blocks = ((p.nq + 31) / 32 + kWarps - 1) / kWarps;
+        if (a.continuous)
+            k_adjoint_a2<T, true><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
+        else
+            k_adjoint_a2<T, false><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
+        k_adj_push<T><<<(unsigned)((t->num_leaves + 255) / 256), 256, 0, s>>>(
+            t->leaf_ids, t->num_leaves, t->meta, t->parent, t->perm, p.accn, p.accp,
+            (T*)grad_attrs);
+        if (cudaGetLastError() != cudaSuccess) rc = set_error(kErrCuda, "adjoint launch");
+    }
+    pool_free(accn, s);
+    pool_free(accp, s);
+    return rc;
 }
 
 }  // namespace
@@ -685,6 +909,16 @@ int traverse(const Tree* t, const TraverseArgs& a, cudaStream_t stream) {
     if (a.qorder && !a.queries)
         return set_error(kErrInvalid, "a query order needs explicit queries");
     return t->dtype == 0 ? dispatch<float>(t, a, stream) : dispatch<double>(t, a, stream);
+}
+
+int adjoint(const Tree* t, const TraverseArgs& a, const void* grad, void* grad_attrs,
+            cudaStream_t stream) {
+    if (a.op != kOpA2Fused) return set_error(kErrInvalid, "the adjoint covers the fused A2 only");
+    if (!t->rec[0] || t->rec_dim[0] != 3)
+        return set_error(kErrState, "the adjoint needs the forward's [n,3] moments in slot 0");
+    if (!a.widths && !(a.width == a.width)) return set_error(kErrInvalid, "width is NaN");
+    return t->dtype == 0 ? adjoint_impl<float>(t, a, grad, grad_attrs, stream)
+                         : adjoint_impl<double>(t, a, grad, grad_attrs, stream);
 }
 
 }  // namespace cagr

@@ -138,6 +138,86 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
     return SolveResult(normals, float(r_norm), float(rk_norm), t1 - t0, t2 - t1, calls)
 
 
+def cagr_solve_autograd(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40,
+                        n_sd: int = 30, wnnc_steps: int = 8, widths: torch.Tensor | None = None,
+                        max_tree_depth: int = 15,
+                        tree: WindingNumberTreecode | None = None) -> SolveResult:
+    """The CAGR solve driven through the differentiable operator
+    (cagr_b200.autograd.convection_gauss) and its true adjoint.
+
+    Objective per iteration, at main_CAGR.py's width of that iteration (:103):
+        L(mu) = 1/2 sum_k || -A2k(mu) - b ||^2,   b = 1/2   (main_CAGR.py:50,107-110)
+    -- the reference's three-block system, with J = -A2 (the fused A21/A22/A23),
+    whose gradient the reference forms with its A2T operators; here
+    grad L = J^T (J mu - b) comes from autograd, i.e. from the adjoint treecode
+    kernel.  Steps: steepest descent with exact
+    line search for i <= n_sd (:105-118), then CG on the normal equations
+    J^T J mu = J^T b (:126-144; symmetric with the true adjoint), then the
+    WNNC G steps (:167-174).  Dots and norms in FP64 as in cagr_solve."""
+    from .autograd import convection_gauss
+    assert wsmin <= wsmax
+    dev = points.device
+    n = points.shape[0]
+    t0 = time.perf_counter()
+    wn = tree if tree is not None else WindingNumberTreecode(points, max_tree_depth)
+    torch.cuda.synchronize(dev)
+    t1 = time.perf_counter()
+    base = torch.ones(n, device=dev, dtype=points.dtype) if widths is None else widths
+    b = torch.full((n, 1), 0.5, device=dev, dtype=points.dtype)
+    calls = 0
+
+    def J(x, w):                       # [N,3] -> [N,3]: the operator -A2 (no graph)
+        nonlocal calls
+        calls += 3
+        with torch.no_grad():
+            return -convection_gauss(wn, x, w)
+
+    def JT(x, w, v):                   # J^T v at the moments of x (the adjoint kernel)
+        nonlocal calls
+        calls += 3
+        xr = x.detach().requires_grad_(True)
+        out = -convection_gauss(wn, xr, w)
+        (g,) = torch.autograd.grad(out, xr, grad_outputs=v)
+        return g
+
+    def scale(i):
+        return wsmin + ((iters - 1 - i) / (iters - 1)) * (wsmax - wsmin)
+
+    normals = torch.zeros(n, 3, device=dev, dtype=points.dtype)
+    r = rk = pk = None
+    w = base * scale(0)
+    for i in range(iters):
+        w = base * scale(i)
+        if i <= n_sd:
+            res = b - J(normals, w)                       # b - J mu, [N,3]
+            r = JT(normals, w, res)                       # -grad L
+            Jr = J(r, w)
+            alpha = (_dot(r, r) / _dot(Jr, Jr)).to(normals.dtype)
+            normals = normals + alpha * r
+            if i == n_sd:
+                rk = JT(normals, w, b - J(normals, w))
+                pk = rk
+        else:
+            Jp = J(pk, w)
+            alpha = (_dot(rk, rk) / _dot(Jp, Jp)).to(normals.dtype)
+            normals = normals + alpha * pk
+            rk2 = rk - alpha * JT(pk, w, Jp)
+            beta = (_dot(rk2, rk2) / _dot(rk, rk)).to(normals.dtype)
+            pk = rk2 + beta * pk
+            rk = rk2
+    r_norm = torch.linalg.norm(r.double()) if r is not None else torch.zeros(())
+    rk_norm = torch.linalg.norm(rk.double()) if rk is not None else torch.zeros(())
+    for _ in range(wnnc_steps):
+        calls += 1
+        g = wn.forward_G(normals.contiguous(), w).double()
+        g = g / torch.clamp(torch.linalg.norm(g, dim=-1, keepdim=True), min=1e-12)
+        length = torch.linalg.norm(normals.double(), dim=-1, keepdim=True)
+        normals = (g * length).to(points.dtype).contiguous()
+    torch.cuda.synchronize(dev)
+    t2 = time.perf_counter()
+    return SolveResult(normals, float(r_norm), float(rk_norm), t1 - t0, t2 - t1, calls)
+
+
 def orient_file(path_in: str, width_config: str = "l0", wsmin: float | None = None,
                 wsmax: float | None = None, device: str = "cuda") -> tuple[np.ndarray, SolveResult]:
     """main_CAGR.py end to end for an .xyz/.npy file: returns [xyz, mu] rows as the

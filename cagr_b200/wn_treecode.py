@@ -206,6 +206,24 @@ class WindingNumberTreecode:
                 f"cagr_multiply({op})")
         return out
 
+    def adjoint_A2(self, grad_out: torch.Tensor, widths, continuous: bool = False,
+                   out: torch.Tensor | None = None) -> torch.Tensor:
+        """J^T grad_out of the fused A2 ([N,3] -> [N,3]) with the moments currently in
+        slot 0 (those of the forward call): the exact adjoint of the forward's
+        traversal (same centroids, decisions and pair terms), recomputed, not stored."""
+        n = self.points.shape[0]
+        g = self._check_values(grad_out, "grad_out")
+        assert g.shape == (n, 3)
+        wt, ws = self._widths(widths, n)
+        if out is None:
+            out = torch.empty(n, 3, dtype=self.dtype, device=self.device)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().cagr_adjoint(
+                self.handle, OPS["A2_FUSED"], _ptr(wt), ws,
+                _lib.FLAG_CONTINUOUS if continuous else 0, _ptr(g), _ptr(out),
+                _stream(self.device)), "cagr_adjoint")
+        return out
+
     def _forward(self, op: str, values: torch.Tensor, widths, continuous: bool = False,
                  queries: torch.Tensor | None = None) -> torch.Tensor:
         values = self._check_values(values, "values")

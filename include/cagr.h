@@ -79,7 +79,8 @@ enum {
     CAGR_OP_A2_FUSED = 10,
     CAGR_OP_A2T_SUM = 11,
     CAGR_OP_COUNT = 12,
-    CAGR_OP_A2T_SUM_SHARED = 13
+    CAGR_OP_A2T_SUM_SHARED = 13,
+    CAGR_OP_A2_INSIDE = 14
 };
 
 /* cagr_multiply / cagr_forward flags. */
@@ -222,6 +223,25 @@ int cagr_scatter_noalloc(const int64_t* parent_dev, const int64_t* children_dev,
                          int dtype, const void* points_dev, const void* weights_dev,
                          const void* attrs_dev, int attr_dim, void* node_attrs_dev,
                          void* reppoints_dev, void* node_weights_dev, void* stream);
+
+/* Exact adjoint of CAGR_OP_A2_FUSED on the tree's own points (no counterpart
+ * in the reference, whose A2T1..A2T3 are a different operator:
+ * wn_treecode_cuda_kernels.cu:263-379 against :113-224).  With the slot-0
+ * moments of the forward call (the same centroids, hence the same acceptance
+ * decisions and pair terms), the forward is linear in the point attributes mu;
+ * this returns grad_attrs = J^T grad_out for grad_out [n,3] (d loss / d out,
+ * original point order): grad_attrs [n,3] (original order), the sum over the
+ * pair terms of the forward of grad_out . d(term)/d(mu).  op must be
+ * CAGR_OP_A2_FUSED; widths / width / flags (CAGR_FLAG_CONTINUOUS only) as in
+ * the forward call.  The traversal is recomputed, not stored.  Allocates
+ * 3 (M + n) scalars of scratch from the library's pool.
+ *
+ * CAGR_OP_A2_INSIDE (for cagr_multiply, no reference counterpart) returns per
+ * query [N',4] the sums over the pair terms inside the width (r < w) of
+ * (d . m, m_0, m_1, m_2): with them the derivative of the continuous
+ * kernel's output with respect to the query's width is closed-form. */
+int cagr_adjoint(cagr_tree* tree, int op, const void* widths_dev, double width, int flags,
+                 const void* grad_out_dev, void* grad_attrs_dev, void* stream);
 
 /* Diagnostic with no counterpart in the reference: measures this GPU's FP32
  * FMA throughput (a long chain of independent fused multiply-adds on every
