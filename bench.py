@@ -305,6 +305,22 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     torch.cuda.synchronize(dev)
     clk = clocks.stop()
 
+    # the autograd backward of A.mu (cagr_b200.autograd): moments of mu + the
+    # adjoint traversal (exact transpose of the forward's) + push to the points
+    G = torch.randn(args.n, 3, device=dev, generator=torch.Generator(dev).manual_seed(3))
+    grad_mu = torch.empty_like(MU)
+    adj_ms = []
+    for it in range(args.warmup + 5):
+        flush.fill_(1.0)
+        a, b = ev(), ev()
+        a.record(stream)
+        wn.scatter(MU)
+        wn.adjoint_A2(G, W, out=grad_mu)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        if it >= args.warmup:
+            adj_ms.append(a.elapsed_time(b))
+
     # end to end through the public API with host buffers
     h_mu = torch.from_numpy(mu).pin_memory()
     h_w = WV.cpu().pin_memory()
@@ -455,7 +471,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                      "peak_source": "measured FP32 FMA probe (cagr_probe_fp32_peak)",
                      "pair_terms_per_launch": round(terms_dom), "flops_per_term": fpt},
         "kernels_ms": {"moments_per_step": round(float(np.mean(mom_ms)), 4),
-                       "A2_FUSED": round(a2_avg, 4), "A2T_SUM": round(a2t_avg, 4)},
+                       "A2_FUSED": round(a2_avg, 4), "A2T_SUM": round(a2t_avg, 4),
+                       "A2_FUSED_backward": round(float(np.mean(adj_ms)), 4)},
         "pair_terms": {"A2_FUSED": round(terms_a2), "A2T1": round(terms_t[0]),
                        "A2T2": round(terms_t[1]), "A2T3": round(terms_t[2])},
         "fp64_ms_per_step": None if fp64_ms is None else round(fp64_ms, 3),
