@@ -182,11 +182,17 @@ def blobs(n: int = 4_000_000, seed: int = 4, noise: float = 5e-4, k: int = 32) -
     C = rng.uniform(-1, 1, size=(k, 3))
     S = rng.uniform(0.15, 0.35, size=k)
 
+    inv2 = 1.0 / (S * S)
+    cc = (C * C).sum(1)
+
     def f_grad(p):
-        d = p[:, None, :] - C[None]
-        g = np.exp(-(d * d).sum(-1) / (2 * S * S))
+        # |p - c|^2 = |p|^2 - 2 p.c + |c|^2 and grad f = -sum_i g_i (p - c_i) / s_i^2,
+        # as matrix products over the k blobs
+        r2 = np.maximum((p * p).sum(1)[:, None] - 2.0 * (p @ C.T) + cc[None], 0.0)
+        g = np.exp(-0.5 * r2 * inv2[None])
         f = g.sum(1)
-        grad = -(g[:, :, None] * d / (S * S)[None, :, None]).sum(1)
+        gw = g * inv2[None]
+        grad = gw @ C - p * gw.sum(1)[:, None]
         return f, grad
 
     out, have = [], 0
@@ -195,12 +201,18 @@ def blobs(n: int = 4_000_000, seed: int = 4, noise: float = 5e-4, k: int = 32) -
         # start near blob surfaces: centre + radius ~ s * 1.2 in a random direction
         idx = rng.integers(0, k, size=m)
         p = C[idx] + _unit(rng, m) * (S[idx] * rng.uniform(0.8, 2.0, size=m))[:, None]
-        for _ in range(12):
-            f, g = f_grad(p)
+        # Newton steps on the points not yet on the level set (|f - 1/2| < 1e-6)
+        act = np.arange(m)
+        ok = np.zeros(m, bool)
+        for _ in range(13):
+            f, g = f_grad(p[act])
+            done = np.abs(f - 0.5) < 1e-6
+            ok[act[done]] = True
+            act, f, g = act[~done], f[~done], g[~done]
+            if act.size == 0:
+                break
             gg = (g * g).sum(1) + 1e-12
-            p = p - ((f - 0.5) / gg)[:, None] * g
-        f, g = f_grad(p)
-        ok = np.abs(f - 0.5) < 1e-6
+            p[act] = p[act] - ((f - 0.5) / gg)[:, None] * g
         p = p[ok]
         # density ratio 10x across x in [-1.5, 1.5]
         dens = 0.1 + 0.9 * np.clip((p[:, 0] + 1.5) / 3.0, 0, 1)

@@ -24,10 +24,10 @@ def normalize(points: np.ndarray) -> np.ndarray:
 
 
 class _Ops:
-    def __init__(self, impl, points):
+    def __init__(self, impl, points, max_depth: int = 15, leaf_size: int = 1):
         self.impl = impl
         self.p = points
-        self.tree = impl.build_tree(points)
+        self.tree = impl.build_tree(points, max_depth, leaf_size)
         self.calls = 0
 
     def fwd(self, op, values, w):
@@ -38,13 +38,16 @@ class _Ops:
 
 
 def solve(points: np.ndarray, wsmin: float, wsmax: float, impl=None, iters: int = 40,
-          n_sd: int = 30, lambda0: float = 0.0, wnnc_steps: int = 8) -> np.ndarray:
-    """points: normalised float32 [N, 3].  Returns mu [N, 3] float32."""
+          n_sd: int = 30, lambda0: float = 0.0, wnnc_steps: int = 8,
+          base_widths: np.ndarray | None = None, max_depth: int = 15,
+          leaf_size: int = 1) -> np.ndarray:
+    """points: normalised float32 [N, 3].  Returns mu [N, 3] float32.
+    base_widths: per-point widths the schedule scales (main_CAGR.py:61 uses ones)."""
     impl = impl or Oracle()
     f32 = np.float32
-    o = _Ops(impl, points)
+    o = _Ops(impl, points, max_depth, leaf_size)
     n = points.shape[0]
-    ones = np.ones(n, f32)
+    ones = np.ones(n, f32) if base_widths is None else np.ascontiguousarray(base_widths, f32)
     normals = np.zeros((n, 3), f32)
     b = np.full((n, 1), 0.5, f32)
 
