@@ -13,8 +13,8 @@ width 1.5 x the mean distance to the 10 nearest neighbours.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Prints one JSON line (rank 0).  For N > 1 (torchrun) every rank runs an
-independent replica (the operator does not shard on one GPU's worth of work;
-see DESIGN.md) and times are the max over ranks.
+independent replica (one GPU's worth of work does not need sharding) and
+times are the max over ranks.
 """
 from __future__ import annotations
 
@@ -42,7 +42,7 @@ FLOPS_A2_FUSED = 29      # three directions
 FLOPS_A2T = 22           # d (3) + |d|^2 (5) + r^-3 (2) + e s r^-3 (2) + 3 FMA (6) + e s r^-1/2 (3) + add (1)
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the two
-# traversals on this workload, from one ncu capture of this build's kernels
+# traversals on this workload, from one ncu capture of these kernels
 # (profiles/step_kernels_union8_1M.md); ncu is not run inside the bench
 TRAFFIC_BYTES = {"A2T_SUM": 158_257_664 + 6_055_168, "A2_FUSED": 137_173_760 + 5_257_472}
 

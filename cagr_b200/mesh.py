@@ -145,9 +145,9 @@ def reconstruct(points: torch.Tensor, mu: torch.Tensor, grid: int = 128,
     wn.scatter(attrs, weights=weights)
     samples = wn.multiply("A3", float(width), continuous=True)[:, 0]
     n = samples.shape[0]
-    # grid value = -field and iso = -(median field at the samples), as the driver sets
-    # them (main_GaussRecon_cuda.cu:478,485-486): with outward normals the field is
-    # lower inside, so inside = value > iso
+    # grid value = -field and iso = -(median field at the samples), as the GaussRecon
+    # program sets them (main_GaussRecon_cuda.cu:478,485-486): with outward normals
+    # the field is lower inside, so inside = value > iso
     iso = -float(torch.kthvalue(samples.float(), n // 2 + 1).values)  # nth_element(n/2)
     spacing = (hi - lo) / (grid - 1)
     field = field_grid(wn, (grid, grid, grid), (lo, lo, lo), spacing, float(width))

@@ -255,7 +255,7 @@ int cagr_probe_fp32_peak(int64_t iters, double* gflops, void* stream);
  * that keeps freed memory reserved for later calls.  cagr_pool_trim
  * synchronises the current device and releases reserved, unused memory beyond
  * keep_bytes; cagr_pool_reserved reports the bytes the current device's pool
- * holds from the driver and the bytes in use. */
+ * holds from the CUDA driver and the bytes in use. */
 int cagr_pool_trim(int64_t keep_bytes);
 int cagr_pool_reserved(int64_t* reserved_bytes, int64_t* used_bytes);
 

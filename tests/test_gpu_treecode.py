@@ -227,7 +227,7 @@ def test_errors_are_raised(cuda_lib):
 def test_memory_pool_reuses_freed_trees(cuda_lib):
     """Trees and records come from the library's pool: a destroyed tree's memory
     stays reserved and serves the next tree of the same size, with nothing in
-    use afterwards; trimming returns it to the driver."""
+    use afterwards; trimming returns it to the CUDA driver."""
     torch = _torch()
     from cagr_b200 import WindingNumberTreecode
     from cagr_b200.wn_treecode import pool_reserved, pool_trim
