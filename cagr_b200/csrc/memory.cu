@@ -5,7 +5,7 @@
 // created on the first use on a device with an unbounded release threshold:
 // freed blocks stay mapped and serve the next call without new page mappings or
 // an implicit device synchronisation.  cagr_pool_trim returns memory to the
-// driver; cagr_pool_reserved reports what the pool holds.  The pools are
+// CUDA driver; cagr_pool_reserved reports what the pool holds.  The pools are
 // separate from the device's default pool and from the framework allocator of
 // the caller, so neither trims the other's memory.
 #include <mutex>
