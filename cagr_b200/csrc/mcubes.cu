@@ -265,12 +265,12 @@ struct Unit {
     int i0, j, k, chunk;
 };
 
-__device__ __forceinline__ Unit unit_of(const Grid& g, int64_t u) {
+// the block's unit: blocks are laid out (chunk, j, k), so no index division
+__device__ __forceinline__ Unit block_unit() {
     Unit r;
-    r.chunk = (int)(u % g.nchunks);
-    const int64_t row = u / g.nchunks;
-    r.j = (int)(row % g.ny);
-    r.k = (int)(row / g.ny);
+    r.chunk = (int)blockIdx.x;
+    r.j = (int)blockIdx.y;
+    r.k = (int)blockIdx.z;
     r.i0 = r.chunk * kChunk;
     return r;
 }
@@ -287,8 +287,9 @@ __global__ void __launch_bounds__(kChunk) k_mc_count(const float* __restrict__ v
     constexpr int kWords = kChunk / 32;
     __shared__ typename Reduce::TempStorage tmp;
     __shared__ uint32_t s_bits[4][kWords + 1];
-    for (int64_t u = blockIdx.x; u < g.units; u += gridDim.x) {
-        const Unit U = unit_of(g, u);
+    {
+        const Unit U = block_unit();
+        const int64_t u = ((int64_t)U.k * g.ny + U.j) * g.nchunks + U.chunk;
         const int t = (int)threadIdx.x, lane = t & 31;
         const int i = U.i0 + t;
         const bool has_y = U.j + 1 < g.ny, has_z = U.k + 1 < g.nz;
@@ -325,7 +326,6 @@ __global__ void __launch_bounds__(kChunk) k_mc_count(const float* __restrict__ v
             vcnt[u] = sum & 0xffff;
             tcnt[u] = sum >> 16;
         }
-        __syncthreads();  // shared memory is reused by the next unit
     }
 }
 
@@ -345,11 +345,12 @@ __global__ void __launch_bounds__(kChunk) k_mc_emit(const float* __restrict__ v,
     __shared__ uint8_t s_mask[4][kChunk + 1];
     __shared__ unsigned long long s_pre[kChunk];
     __shared__ int64_t s_base[4], s_next[4];
-    for (int64_t u = blockIdx.x; u < g.units; u += gridDim.x) {
+    {
+        const Unit U = block_unit();
+        const int64_t u = ((int64_t)U.k * g.ny + U.j) * g.nchunks + U.chunk;
         // a unit with neither vertices nor triangles (most of the grid) has nothing
         // to emit; the test is the same for the whole block
-        if (vbase[u + 1] == vbase[u] && tbase[u + 1] == tbase[u]) continue;
-        const Unit U = unit_of(g, u);
+        if (vbase[u + 1] == vbase[u] && tbase[u + 1] == tbase[u]) return;
         const int t = (int)threadIdx.x;
         const int i = U.i0 + t;
         const bool cell_row = U.j + 1 < g.ny && U.k + 1 < g.nz;
@@ -417,7 +418,6 @@ __global__ void __launch_bounds__(kChunk) k_mc_emit(const float* __restrict__ v,
                 faces[3 * (o + q) + s] = (int32_t)id;
             }
         }
-        __syncthreads();  // shared memory is reused by the next unit
     }
 }
 
@@ -456,9 +456,10 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
     const int64_t U = (int64_t)nchunks * ny * nz;
     Grid g{nx, ny, nz, nchunks, U, (float)origin[0], (float)origin[1], (float)origin[2],
            (float)spacing, (float)iso};
-    // one block per unit (measured faster than resident blocks looping over the
-    // units); the kernels loop over units with a grid stride all the same
-    const unsigned grid_c = (unsigned)U, grid_e = (unsigned)U;
+    // one block per unit, blocks laid out (chunk, j, k)
+    if (ny > 65535 || nz > 65535)
+        return set_error(kErrInvalid, "marching cubes needs ny, nz <= 65535");
+    const dim3 grid_c((unsigned)nchunks, (unsigned)ny, (unsigned)nz), grid_e = grid_c;
     int32_t *vcnt = nullptr, *tcnt = nullptr;
     int64_t *vbase = nullptr, *tbase = nullptr;
     auto cleanup = [&] {
