@@ -22,15 +22,16 @@ CAGR_F32, CAGR_F64 = 0, 1
 # operators
 OPS = {"A": 0, "AT": 1, "A3": 2, "A21": 3, "A22": 4, "A23": 5, "A2T1": 6, "A2T2": 7,
        "A2T3": 8, "G": 9, "A2_FUSED": 10, "A2T_SUM": 11, "COUNT": 12, "A2T_SUM_SHARED": 13,
-       "A2_INSIDE": 14}
+       "A2_INSIDE": 14, "A2T_RHS": 15}
 # multiply flags
 FLAG_CONTINUOUS = 1
 FLAG_ACCUMULATE = 2
 ATTR_DIM = {"A": 3, "AT": 1, "A3": 3, "A21": 3, "A22": 3, "A23": 3, "A2T1": 1, "A2T2": 1,
-            "A2T3": 1, "G": 3, "A2_FUSED": 3, "A2T_SUM": 3, "A2T_SUM_SHARED": 1, "A2_INSIDE": 3}
+            "A2T3": 1, "G": 3, "A2_FUSED": 3, "A2T_SUM": 3, "A2T_SUM_SHARED": 1, "A2_INSIDE": 3,
+            "A2T_RHS": 3}
 OUT_DIM = {"A": 1, "AT": 3, "A3": 1, "A21": 1, "A22": 1, "A23": 1, "A2T1": 3, "A2T2": 3,
            "A2T3": 3, "G": 3, "A2_FUSED": 3, "A2T_SUM": 3, "A2T_SUM_SHARED": 3, "COUNT": 1,
-           "A2_INSIDE": 4}
+           "A2_INSIDE": 4, "A2T_RHS": 3}
 
 _p = ctypes.c_void_p
 _i64 = ctypes.c_int64

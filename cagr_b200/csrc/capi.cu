@@ -49,6 +49,7 @@ int op_attr_dim(int op) {
         case CAGR_OP_A2T_SUM_SHARED: return 1;  // one scalar column shared by the three
         case CAGR_OP_COUNT: return -1;  // any: counts with whatever slot 0 holds
         case CAGR_OP_A2_INSIDE: return 3;
+        case CAGR_OP_A2T_RHS: return 3;
         default: return 0;
     }
 }
@@ -149,9 +150,9 @@ int cagr_multiply(const cagr_tree* tree, int op, const void* queries_dev,
         return set_error(CAGR_ERR_INVALID, "out_stride out of range");
     cagr::TraverseArgs a;
     a.op = op;
-    if (op == CAGR_OP_A2T_SUM || op == CAGR_OP_A2T_SUM_SHARED) {
+    if (op == CAGR_OP_A2T_SUM || op == CAGR_OP_A2T_SUM_SHARED || op == CAGR_OP_A2T_RHS) {
         a.op = cagr::kOpA2TFused;
-        a.slots = op == CAGR_OP_A2T_SUM ? 3 : 1;
+        a.slots = op == CAGR_OP_A2T_SUM ? 3 : (op == CAGR_OP_A2T_RHS ? 4 : 1);
     }
     a.continuous = (flags & CAGR_FLAG_CONTINUOUS) ? 1 : 0;
     a.accumulate = (flags & CAGR_FLAG_ACCUMULATE) ? 1 : 0;
@@ -185,7 +186,8 @@ int cagr_field_grid(const cagr_tree* tree, int op, int nx, int ny, int nz,
                     const double* origin, double spacing, const void* widths_dev, double width,
                     int flags, void* out_dev, void* stream) {
     if (int rc = check_tree(tree)) return rc;
-    if (op_attr_dim(op) <= 0 || op == CAGR_OP_A2T_SUM || op == CAGR_OP_A2T_SUM_SHARED)
+    if (op_attr_dim(op) <= 0 || op == CAGR_OP_A2T_SUM || op == CAGR_OP_A2T_SUM_SHARED ||
+        op == CAGR_OP_A2T_RHS)
         return set_error(CAGR_ERR_INVALID, "unsupported operator for grid queries");
     if (!origin) return set_error(CAGR_ERR_INVALID, "origin is null");
     if (flags & ~(CAGR_FLAG_CONTINUOUS | CAGR_FLAG_ACCUMULATE))

@@ -347,8 +347,8 @@ int launch_moments(Tree* t, int slot, const void* attrs, int dim, const void* we
 
 // Three scalar attributes into the packed adjoint records only (the record
 // slots are not written: the three-slot traversal reads the packed layout,
-// and export reads centroids and sums from it).  Slots 0..2 are marked empty
-// for single-slot operators until the next cagr_scatter into them.
+// and export reads centroids and sums from it).  The record slots keep what
+// the last cagr_scatter into each put there.
 template <typename T>
 int launch_moments3(Tree* t, const void* values3, cudaStream_t s) {
     if (!t->adj_nodes)
@@ -366,7 +366,6 @@ int launch_moments3(Tree* t, const void* values3, cudaStream_t s) {
     p.adjs = (T*)t->adj_sums;
     if (int rc = run(t, p, s)) return rc;
     for (int k = 0; k < 3; k++) {
-        t->rec_dim[k] = 0;
         t->slot_adj[k] = true;
     }
     t->adj_valid = true;

@@ -458,6 +458,18 @@ __device__ __forceinline__ void a2t_term1(Lane<T>& L, bool take, T g, T dx, T dy
     if constexpr (K == 2) L.acc2 += h;
 }
 
+// The shared-slot (b) term of a near point: record (y, 0), (e(y), s).
+template <typename T>
+__device__ __forceinline__ void rhs_b_point(Lane<T>& L, const T* pr, const T* ex) {
+    const Vec4<T> s0 = ld4(pr);
+    const Vec4<T> r1 = ld4(pr + 4);
+    const T px = sub_rn(L.q0, s0.x);
+    const T py = sub_rn(L.q1, s0.y);
+    const T pz = sub_rn(L.q2, s0.z);
+    const T e[3] = {r1.x, r1.y, r1.z};
+    a2t_term(L, ex, e, r1.w, px, py, pz, dist2_exact(px, py, pz), 0, 3);
+}
+
 // Slot K of the three-slot adjoint walk: acceptance test against the slot's
 // own centroid and the lane's own active depth kd.
 template <typename T>
@@ -529,7 +541,14 @@ __device__ __forceinline__ ChildTest<T> child_test(const Lane<T>& L, const Vec4<
 // its own acceptance decisions, tracked by its own kd -- the three reference
 // calls A2T1(s1), A2T2(s2), A2T3(s3) with their own scatters.  A near point's
 // geometry is shared by the three directions.
-template <typename T>
+//
+// RHS: sum_k A2Tk(b) - sum_k A2Tk(s_k) in the same walk -- the right-hand side
+// minus the normal-equation product of one CAGR iteration (main_CAGR.py:108,
+// 114-115), at the same width.  b is a fourth slot with its own moments
+// (record slot 1, the shared three-direction form of k_traverse_a2t_shared),
+// its own centroids and its own kd; its terms are added, the s_k slots' terms
+// subtracted.
+template <typename T, bool RHS>
 __global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t3(const TravParams<T> p) {
     const int lane = threadIdx.x & 31;
     const int64_t qi = ((int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32 + lane;
@@ -539,10 +558,15 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t3(const TravParams<
     T w;
     const bool valid = load_query(p, qi, L, oidx, w);
     const T ex0 = exp_t(L.q0 * T(0.5)), ex1 = exp_t(L.q1 * T(0.5)), ex2 = exp_t(L.q2 * T(0.5));
+    // the s_k slots' sign: subtracted in the RHS form
+    const T sg = RHS ? T(-1) : T(1);
+    const T gx0 = sg * ex0, gx1 = sg * ex1, gx2 = sg * ex2;
+    const T exb[3] = {ex0, ex1, ex2};
     const int M = (int)p.M;
     const T* __restrict__ an = p.adjn;
     const T* __restrict__ ap = p.adjp;
-    int kd0 = valid ? 0 : -1, kd1 = kd0, kd2 = kd0;
+    const T* __restrict__ rb = p.rec[1];  // RHS: b's records
+    int kd0 = valid ? 0 : -1, kd1 = kd0, kd2 = kd0, kdb = kd0;
     int n = 0;
     while (n < M) {
         const int4 mt = __ldg(p.meta + n);
@@ -554,18 +578,38 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t3(const TravParams<
         const SlotTest<T> s0 = slot_test(L, c0, R2, d, leaf, kd0);
         const SlotTest<T> s1 = slot_test(L, c1, R2, d, leaf, kd1);
         const SlotTest<T> s2 = slot_test(L, c2, R2, d, leaf, kd2);
-        const bool open_any = s0.open || s1.open || s2.open;
+        bool open_any = s0.open || s1.open || s2.open;
+        SlotTest<T> sb;
+        Vec4<T> b1;
+        if constexpr (RHS) {
+            const T* r = rb + (int64_t)n * CAGR_REC_STRIDE;
+            const Vec4<T> b0 = ld4(r);  // (c_b, (4h)^2)
+            b1 = ld4(r + 4);            // (e(c_b), s_b)
+            sb = slot_test(L, b0, rec_radius2(b0.w), d, leaf, kdb);
+            open_any = open_any || sb.open;
+        }
         const bool any_open = __any_sync(kFull, open_any);
         // node terms, each slot against its own centroid
-        if (s0.active && s0.far) a2t_term1<T, 0>(L, true, ex0 * c0.w, s0.dx, s0.dy, s0.dz, s0.d2);
-        if (s1.active && s1.far) a2t_term1<T, 1>(L, true, ex1 * c1.w, s1.dx, s1.dy, s1.dz, s1.d2);
-        if (s2.active && s2.far) a2t_term1<T, 2>(L, true, ex2 * c2.w, s2.dx, s2.dy, s2.dz, s2.d2);
+        if (s0.active && s0.far) a2t_term1<T, 0>(L, true, gx0 * c0.w, s0.dx, s0.dy, s0.dz, s0.d2);
+        if (s1.active && s1.far) a2t_term1<T, 1>(L, true, gx1 * c1.w, s1.dx, s1.dy, s1.dz, s1.d2);
+        if (s2.active && s2.far) a2t_term1<T, 2>(L, true, gx2 * c2.w, s2.dx, s2.dy, s2.dz, s2.d2);
+        if constexpr (RHS) {
+            if (sb.active && sb.far) {
+                const T e[3] = {b1.x, b1.y, b1.z};
+                a2t_term(L, exb, e, b1.w, sb.dx, sb.dy, sb.dz, sb.d2, 0, 3);
+            }
+        }
         if (leaf) {
             if (any_open) {
                 const int np = -mt.z;
                 const T* pp = ap + (int64_t)mt.y * 8;
-                for (int j = 0; j < np; j++, pp += 8)
-                    if (open_any) a2t3_point(L, pp, s0.open, s1.open, s2.open, ex0, ex1, ex2);
+                for (int j = 0; j < np; j++, pp += 8) {
+                    if (s0.open || s1.open || s2.open)
+                        a2t3_point(L, pp, s0.open, s1.open, s2.open, gx0, gx1, gx2);
+                    if constexpr (RHS) {
+                        if (sb.open) rhs_b_point(L, rb + ((int64_t)M + mt.y + j) * CAGR_REC_STRIDE, exb);
+                    }
+                }
             }
             n = mt.x;
         } else if (node_twig(mt)) {
@@ -578,16 +622,31 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t3(const TravParams<
                 const T* cq = q + 12;
                 const T* pp = ap + (int64_t)mt.y * 8;
                 for (int c = 0; c < nc; c++, cq += 12, pp += 8) {
-                    if (open_any) {
+                    if (s0.open || s1.open || s2.open) {
                         const Vec4<T> C0 = ld4(cq), C1 = ld4(cq + 4), C2 = ld4(cq + 8);
                         const ChildTest<T> t0 = child_test(L, C0, R2c, s0.open);
                         const ChildTest<T> t1 = child_test(L, C1, R2c, s1.open);
                         const ChildTest<T> t2 = child_test(L, C2, R2c, s2.open);
-                        if (t0.far) a2t_term1<T, 0>(L, true, ex0 * C0.w, t0.dx, t0.dy, t0.dz, t0.d2);
-                        if (t1.far) a2t_term1<T, 1>(L, true, ex1 * C1.w, t1.dx, t1.dy, t1.dz, t1.d2);
-                        if (t2.far) a2t_term1<T, 2>(L, true, ex2 * C2.w, t2.dx, t2.dy, t2.dz, t2.d2);
+                        if (t0.far) a2t_term1<T, 0>(L, true, gx0 * C0.w, t0.dx, t0.dy, t0.dz, t0.d2);
+                        if (t1.far) a2t_term1<T, 1>(L, true, gx1 * C1.w, t1.dx, t1.dy, t1.dz, t1.d2);
+                        if (t2.far) a2t_term1<T, 2>(L, true, gx2 * C2.w, t2.dx, t2.dy, t2.dz, t2.d2);
                         if (t0.near || t1.near || t2.near)
-                            a2t3_point(L, pp, t0.near, t1.near, t2.near, ex0, ex1, ex2);
+                            a2t3_point(L, pp, t0.near, t1.near, t2.near, gx0, gx1, gx2);
+                    }
+                    if constexpr (RHS) {
+                        if (sb.open) {
+                            // b's one-point-leaf child: its node record if far, else its point
+                            const T* cr = rb + ((int64_t)n + 1 + c) * CAGR_REC_STRIDE;
+                            const Vec4<T> B0 = ld4(cr);
+                            const ChildTest<T> tb = child_test(L, B0, rec_radius2(B0.w), true);
+                            if (tb.far) {
+                                const Vec4<T> B1 = ld4(cr + 4);
+                                const T e[3] = {B1.x, B1.y, B1.z};
+                                a2t_term(L, exb, e, B1.w, tb.dx, tb.dy, tb.dz, tb.d2, 0, 3);
+                            } else {
+                                rhs_b_point(L, rb + ((int64_t)M + mt.y + c) * CAGR_REC_STRIDE, exb);
+                            }
+                        }
                     }
                 }
             }
@@ -610,7 +669,9 @@ int launch_op(const TravParams<T>& p, int cont, int slots, cudaStream_t s) {
     if (blocks > 0x7fffffffLL) return set_error(kErrInvalid, "too many queries");
     if constexpr (OP == kOpA2TFused) {
         if (slots == 3)
-            k_traverse_a2t3<T><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
+            k_traverse_a2t3<T, false><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
+        else if (slots == 4)
+            k_traverse_a2t3<T, true><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
         else
             k_traverse_a2t_shared<T><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
     } else if (cont) {
@@ -653,12 +714,17 @@ int dispatch(const Tree* t, const TraverseArgs& a, cudaStream_t s) {
     p.accumulate = a.accumulate;
     const bool scalar_in = a.op == kOpAT || a.op == kOpA2T1 || a.op == kOpA2T2 ||
                            a.op == kOpA2T3 || a.op == kOpA2TFused;
-    const int slots = (a.op == kOpA2TFused && a.slots == 3) ? 3 : 1;
-    if (slots == 3) {
+    const int slots = a.op == kOpA2TFused ? a.slots : 1;
+    if (slots >= 3) {
         if (!t->adj_valid || !t->adj_nodes)
             return set_error(kErrState, "A2T sum needs the three-slot moments (cagr_scatter3)");
         p.adjn = (const T*)t->adj_nodes;
         p.adjp = (const T*)t->adj_points;
+        if (slots == 4) {
+            if (!t->rec[1] || t->rec_dim[1] != 1)
+                return set_error(kErrState, "the A2T right-hand side needs b's moments in slot 1");
+            p.rec[1] = (const T*)t->rec[1];
+        }
     } else {
         const int need_dim = a.op == kOpCount ? t->rec_dim[0] : (scalar_in ? 1 : 3);
         if (!t->rec[0] || t->rec_dim[0] == 0 || t->rec_dim[0] != need_dim)

@@ -6,7 +6,9 @@ width schedule that shrinks linearly from wsmax to wsmin (:103) -- 31
 steepest-descent-type steps (:105-118), a residual restart at i == 30
 (:119-125), 9 CG-type steps (:126-144) -- and 8 WNNC G steps (:167-174).
 Every operator application goes through the C ABI (A2k fused into one
-traversal; A2Tk as the reference composes them).  The iteration stays on the
+traversal; the three A2Tk of a step fused into one, and in the
+steepest-descent steps fused with the three of the right-hand side b, whose
+moments are computed once).  The iteration stays on the
 GPU: step lengths are device tensors, nothing is copied to the host until the
 caller asks for the result.
 
@@ -96,23 +98,27 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
     def scale(i):
         return wsmin + ((iters - 1 - i) / (iters - 1)) * (wsmax - wsmin)
 
+    def RHS(a_mu, w):  # A2Tb(w) - A2T(a_mu) in one traversal (b's moments in slot 1)
+        nonlocal calls
+        calls += 6
+        return wn.forward_A2T_rhs(a_mu, w)
+
     w = base * (wsmin + 0.5 * (wsmax - wsmin))
     rk1 = A2Tb(w)   # main_CAGR.py:98 (overwritten at i == n_sd)
+    wn.scatter(b, slot=1)   # b is constant: its moments serve every iteration
     pk = rk1
     r = rk1
     for i in range(iters):
         w = base * scale(i)
         if i <= n_sd:
             A_mu = -A2(normals, w)
-            AT_A_mu = A2T(A_mu.contiguous(), w)
-            r = A2Tb(w) - AT_A_mu - lambda0 * normals
+            r = RHS(A_mu.contiguous(), w) - lambda0 * normals   # A2Tb(w) - A2T(A_mu)
             A_r = -A2(r.contiguous(), w).sum(1, keepdim=True)
             alpha = (_dot(r, r) / _dot(A_r, A_r)).float()
             normals = normals + alpha * r
             if i == n_sd:
                 A_mu = -A2(normals, w)
-                AT_A_mu = A2T(A_mu.contiguous(), w)
-                rk1 = A2Tb(w) - AT_A_mu - lambda0 * normals
+                rk1 = RHS(A_mu.contiguous(), w) - lambda0 * normals
                 pk = rk1
         else:
             A_pk = -A2(pk.contiguous(), w)

@@ -303,8 +303,8 @@ class WindingNumberTreecode:
     def scatter3(self, values3: torch.Tensor):
         """Node moments of the three columns of values3 ([N, 3]), each with its own
         |v_k| weights, into the packed records that A2T_SUM reads.  scatter_export(k, 1)
-        returns column k's moments until the next scatter into slot k; single-slot
-        operators need a scatter() first."""
+        returns column k's moments until the next scatter into slot k; the record
+        slots (single-slot operators) keep what the last scatter() put there."""
         values3 = self._check_values(values3, "values")
         assert len(values3.shape) == 2 and values3.shape[1] == 3
         with torch.cuda.device(self.device):
@@ -321,6 +321,16 @@ class WindingNumberTreecode:
         assert values3.shape[0] == self.points.shape[0]
         self.scatter3(values3)
         return self.multiply("A2T_SUM", widths, out=out, accumulate=accumulate)
+
+    def forward_A2T_rhs(self, values3, widths, out: torch.Tensor | None = None):
+        """sum_k A2Tk(b) - sum_k A2Tk(values3[:, k]) -> [N, 3] in one traversal: b's
+        moments must be in slot 1 (scatter(b, slot=1)); values3's are computed here
+        (scatter3).  The residual of a CAGR steepest-descent step (main_CAGR.py:108),
+        with every input keeping its own moments and acceptance decisions."""
+        assert len(values3.shape) == 2 and values3.shape[1] == 3
+        assert values3.shape[0] == self.points.shape[0]
+        self.scatter3(values3)
+        return self.multiply("A2T_RHS", widths, out=out)
 
     def forward_A2T_shared(self, values, widths, out: torch.Tensor | None = None,
                            accumulate: bool = False):

@@ -80,7 +80,8 @@ enum {
     CAGR_OP_A2T_SUM = 11,
     CAGR_OP_COUNT = 12,
     CAGR_OP_A2T_SUM_SHARED = 13,
-    CAGR_OP_A2_INSIDE = 14
+    CAGR_OP_A2_INSIDE = 14,
+    CAGR_OP_A2T_RHS = 15
 };
 
 /* cagr_multiply / cagr_forward flags. */
@@ -137,9 +138,10 @@ int cagr_scatter(cagr_tree* tree, int slot, const void* attrs_dev, int attr_dim,
  * scatter_point_attrs_to_nodes calls the reference makes before its A2T1,
  * A2T2 and A2T3 kernels (wn_treecode_func.py:271-351), in one launch.  The
  * result is held in the packed records CAGR_OP_A2T_SUM reads, not in the
- * record slots: cagr_scatter_export(tree, k, ...) returns column k's moments
- * (attr dim 1) until the next cagr_scatter into slot k, and single-slot
- * operators need a cagr_scatter first (they report CAGR_ERR_STATE). */
+ * record slots, which keep what the last cagr_scatter put there (single-slot
+ * operators, and CAGR_OP_A2T_RHS's b in slot 1, read those);
+ * cagr_scatter_export(tree, k, ...) returns column k's moments (attr dim 1)
+ * until the next cagr_scatter into slot k. */
 int cagr_scatter3(cagr_tree* tree, const void* values3_dev, void* stream);
 
 /* Copies slot `slot` out in the reference layout: node_attrs [M, attr_dim],
@@ -223,6 +225,13 @@ int cagr_scatter_noalloc(const int64_t* parent_dev, const int64_t* children_dev,
                          int dtype, const void* points_dev, const void* weights_dev,
                          const void* attrs_dev, int attr_dim, void* node_attrs_dev,
                          void* reppoints_dev, void* node_weights_dev, void* stream);
+
+/* CAGR_OP_A2T_RHS (cagr_multiply; no reference counterpart as one call):
+ * sum_k A2Tk(b) - sum_k A2Tk(s_k) in one traversal, the residual the CAGR
+ * steepest-descent step forms from the reference's calls at one width
+ * (main_CAGR.py:108-115): b's moments in record slot 1 (cagr_scatter(tree, 1,
+ * b, 1, ...)), the s_k's from cagr_scatter3.  Every input keeps its own
+ * moments and acceptance decisions, as in the separate calls; out [N',3]. */
 
 /* Exact adjoint of CAGR_OP_A2_FUSED on the tree's own points (no counterpart
  * in the reference, whose A2T1..A2T3 are a different operator:
