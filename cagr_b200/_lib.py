@@ -64,6 +64,7 @@ _SIGNATURES = {
     "cagr_pool_trim": (_i32, [_i64]),
     "cagr_adjoint": (_i32, [_p, _i32, _p, ctypes.c_double, _i32, _p, _p, _p]),
     "cagr_pool_reserved": (_i32, [_pi64, _pi64]),
+    "cagr_debug_fail_allocations_after": (_i32, [_i64]),
 }
 
 _lib = None

@@ -8,6 +8,7 @@
 // CUDA driver; cagr_pool_reserved reports what the pool holds.  The pools are
 // separate from the device's default pool and from the framework allocator of
 // the caller, so neither trims the other's memory.
+#include <atomic>
 #include <mutex>
 #include <string>
 
@@ -20,6 +21,9 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_pool_mutex;
 cudaMemPool_t g_pools[kMaxDevices] = {};
+// fault injection (cagr_debug_fail_allocations_after): allocations still
+// allowed before every further one fails; negative = never fail
+std::atomic<long long> g_allow{-1};
 
 int current_pool(cudaMemPool_t* out) {
     int dev = 0;
@@ -50,6 +54,12 @@ int current_pool(cudaMemPool_t* out) {
 
 int pool_alloc(void** p, size_t bytes, cudaStream_t s) {
     *p = nullptr;
+    long long left = g_allow.load();
+    while (left > 0 && !g_allow.compare_exchange_weak(left, left - 1)) {
+    }
+    if (left == 0)
+        return set_error(kErrAlloc, "device allocation of " + std::to_string(bytes) +
+                                        " bytes refused (fault injection)");
     cudaMemPool_t pool;
     if (int rc = current_pool(&pool)) return rc;
     if (bytes == 0) bytes = 16;
@@ -96,6 +106,11 @@ int cagr_pool_trim(int64_t keep_bytes) {
 
 int cagr_pool_reserved(int64_t* reserved_bytes, int64_t* used_bytes) {
     return cagr::pool_reserved(reserved_bytes, used_bytes);
+}
+
+int cagr_debug_fail_allocations_after(int64_t n) {
+    cagr::g_allow.store(n < 0 ? -1 : (long long)n);
+    return CAGR_OK;
 }
 
 }  // extern "C"

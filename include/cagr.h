@@ -268,6 +268,12 @@ int cagr_probe_fp32_peak(int64_t iters, double* gflops, void* stream);
 int cagr_pool_trim(int64_t keep_bytes);
 int cagr_pool_reserved(int64_t* reserved_bytes, int64_t* used_bytes);
 
+/* Fault injection for tests (no counterpart in the reference, which checks no
+ * allocation at all): after n more library allocations succeed, every further
+ * one fails with CAGR_ERR_ALLOC, as a full device would make it; n < 0 turns
+ * this off (the default).  Process-wide. */
+int cagr_debug_fail_allocations_after(int64_t n);
+
 #ifdef __cplusplus
 }
 #endif
