@@ -263,7 +263,6 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p)
         const bool far = d2 > rec_radius2(r0.w);
         const bool open = active && !far;
         if (active) kd = (open && !leaf) ? d + 1 : d;
-        const bool any_open = __any_sync(kFull, open);
         if (mt.z == -1) {
             // single-point leaf: far lanes take the node term, near lanes the point
             const T* src = r;
@@ -279,6 +278,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p)
             n = mt.x;
             continue;
         }
+        // (the vote after the one-point-leaf path, which does not need it: mt
+        // is warp-uniform, so every lane of the warp gets here or none)
+        const bool any_open = __any_sync(kFull, open);
         if (active && far) pair_term<T, OP, CONT>(L, r, dx, dy, dz, d2);
         if (leaf) {
             const int np = -mt.z;
