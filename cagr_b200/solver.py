@@ -68,7 +68,6 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
 
     widths: per-point base widths (main_CAGR.py:61 uses ones); each iteration
     uses widths * width_scale."""
-    assert wsmin <= wsmax
     dev = points.device
     n = points.shape[0]
     t0 = time.perf_counter()
@@ -161,7 +160,6 @@ def cagr_solve_autograd(points: torch.Tensor, wsmin: float, wsmax: float, iters:
     J^T J mu = J^T b (:126-144; symmetric with the true adjoint), then the
     WNNC G steps (:167-174).  Dots and norms in FP64 as in cagr_solve."""
     from .autograd import convection_gauss
-    assert wsmin <= wsmax
     dev = points.device
     n = points.shape[0]
     t0 = time.perf_counter()
@@ -225,7 +223,8 @@ def cagr_solve_autograd(points: torch.Tensor, wsmin: float, wsmax: float, iters:
 
 
 def orient_file(path_in: str, width_config: str = "l0", wsmin: float | None = None,
-                wsmax: float | None = None, device: str = "cuda") -> tuple[np.ndarray, SolveResult]:
+                wsmax: float | None = None, device: str = "cuda",
+                iters: int = 40) -> tuple[np.ndarray, SolveResult]:
     """main_CAGR.py end to end for an .xyz/.npy file: returns [xyz, mu] rows as the
     reference writes them (:185-186)."""
     if path_in.endswith(".npy"):
@@ -237,6 +236,6 @@ def orient_file(path_in: str, width_config: str = "l0", wsmin: float | None = No
     else:
         lo, hi = PRESET_WIDTHS[width_config]
     pts = torch.from_numpy(normalize_points(raw)).to(device)
-    res = cagr_solve(pts, lo, hi)
+    res = cagr_solve(pts, lo, hi, iters=iters)
     out = np.concatenate([raw, res.normals.cpu().numpy().astype(np.float64)], 1)
     return out, res
