@@ -50,6 +50,8 @@ struct Tree {
     int64_t* n2p_start = nullptr;  // [M]
     int32_t* n2p = nullptr;        // [n2p_len] original indices
     void* spos = nullptr;          // [N*3] T, positions in sorted order
+    int32_t* qgroup = nullptr;     // [N] self-query qi is the point at sorted position qgroup[qi]
+                                   // (3-D Hilbert order: the traversals' warp grouping)
     uint32_t* counters = nullptr;  // [M], zero between moment passes
     void* rec[3] = {nullptr, nullptr, nullptr};  // [(M+N)*CAGR_REC_STRIDE] T per slot
     int rec_dim[3] = {0, 0, 0};    // attribute dim the slot was filled with (0 = empty)

