@@ -32,6 +32,11 @@ namespace cagr {
 namespace {
 
 constexpr int kBlock = 256;
+// The climb's blocks are small: a block stays resident until its last thread
+// has climbed, so a 256-thread block held 8 warps for one climbing lane
+// (measured at 1M points: 64 threads 0.208 -> 0.190 ms, with the parent
+// prefetch below 0.162 ms; 32 threads 0.166 ms).
+constexpr int kClimbBlock = 64;
 
 template <typename T>
 __device__ __forceinline__ T weight_of(const T* a, int dim) {
@@ -145,11 +150,9 @@ __device__ __forceinline__ void leaf_pass(const MomParams<T, DIM, NS>& p, int no
 // Sums over the children of `node` in octant order.  CG: read through L2
 // (children written by other threads of the same launch).
 template <bool CG, typename T, int DIM, int NS>
-__device__ __forceinline__ void children_pass(const MomParams<T, DIM, NS>& p, int node,
-                                              Sums<T, NS>& S) {
+__device__ __forceinline__ void children_pass(const MomParams<T, DIM, NS>& p, const int4 c0,
+                                              const int4 c1, Sums<T, NS>& S) {
     S.clear();
-    const int4 c0 = reinterpret_cast<const int4*>(p.children)[2 * (int64_t)node];
-    const int4 c1 = reinterpret_cast<const int4*>(p.children)[2 * (int64_t)node + 1];
     const int ch[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
 #pragma unroll
     for (int q = 0; q < 8; q++) {
@@ -244,7 +247,7 @@ __device__ __forceinline__ uint32_t arrive_acq_rel(uint32_t* counter) {
 
 // Each leaf thread climbs while it is the last child to arrive at the parent.
 template <typename T, int DIM, int NS>
-__global__ void __launch_bounds__(kBlock) k_moments_climb(const MomParams<T, DIM, NS> p) {
+__global__ void __launch_bounds__(kClimbBlock) k_moments_climb(const MomParams<T, DIM, NS> p) {
     const int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (li >= p.num_leaves) return;
     int node = p.leaf_ids[li];
@@ -252,18 +255,25 @@ __global__ void __launch_bounds__(kBlock) k_moments_climb(const MomParams<T, DIM
     Sums<T, NS> S;
     leaf_pass(p, node, lm, S);
     int count = node_npts(lm), depth = node_depth(lm);
+    // the parent's structure (read-only) is loaded while the arrival is in
+    // flight; only the children's records wait for it (measured at 1M points:
+    // 0.190 -> 0.162 ms for [n,3] moments)
+    int par = node == 0 ? 0 : p.parent[node];
     while (true) {
         finish_node(p, node, depth, count, S);
         if (node == 0) return;
-        const int par = p.parent[node];
-        const uint32_t arrived = arrive_acq_rel(&p.counters[par]);
-        if (arrived + 1u != (uint32_t)p.nchild[par]) return;
-        p.counters[par] = 0u;
         const int4 pm = p.meta[par];
+        const uint32_t need = p.nchild[par];
+        const int4 c0 = reinterpret_cast<const int4*>(p.children)[2 * (int64_t)par];
+        const int4 c1 = reinterpret_cast<const int4*>(p.children)[2 * (int64_t)par + 1];
+        const uint32_t arrived = arrive_acq_rel(&p.counters[par]);
+        if (arrived + 1u != need) return;
+        p.counters[par] = 0u;
         node = par;
+        par = par == 0 ? 0 : p.parent[par];  // the next level's, in flight meanwhile
         count = node_npts(pm);
         depth = node_depth(pm);
-        children_pass<true>(p, node, S);
+        children_pass<true>(p, c0, c1, S);
     }
 }
 
@@ -314,8 +324,8 @@ int run(Tree* t, MomParams<T, DIM, NS> p, cudaStream_t s) {
     p.n2p_start = t->n2p_start;
     p.spos = (const T*)t->spos;
     p.counters = t->counters;
-    const unsigned grid = (unsigned)((t->num_leaves + kBlock - 1) / kBlock);
-    k_moments_climb<T, DIM, NS><<<grid, kBlock, 0, s>>>(p);
+    const unsigned grid = (unsigned)((t->num_leaves + kClimbBlock - 1) / kClimbBlock);
+    k_moments_climb<T, DIM, NS><<<grid, kClimbBlock, 0, s>>>(p);
     CAGR_CUDA(cudaGetLastError());
     return kOk;
 }
