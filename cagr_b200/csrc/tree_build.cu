@@ -100,11 +100,14 @@ __global__ void k_morton(const T* __restrict__ pts, int64_t n, int D, uint64_t* 
 // 3.2 % fewer warp visits on the 1M-point union-of-primitives cloud.
 // Hilbert index: J. Skilling, "Programming the Hilbert curve", AIP Conf. Proc.
 // 707 (2004) -- axes to transposed index by inverse undo of the excess work,
-// Gray decode, then the three axes' bits interleaved from the top.
-constexpr int kHilbertBits = 21;
+// Gray decode, then the three axes' bits interleaved from the top.  10 bits
+// per axis group as well as 21 (a host simulation of the warp walk counts the
+// same visits) and keep the key in 32 bits: half the radix-sort passes.
+// Points in one cell keep their Morton order (stable sort).
+constexpr int kHilbertBits = 10;
 
 template <typename T>
-__global__ void k_hilbert(const T* __restrict__ spos, int64_t n, uint64_t* __restrict__ keys,
+__global__ void k_hilbert(const T* __restrict__ spos, int64_t n, uint32_t* __restrict__ keys,
                           int32_t* __restrict__ idx) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -133,7 +136,7 @@ __global__ void k_hilbert(const T* __restrict__ spos, int64_t n, uint64_t* __res
     X[0] ^= t;
     X[1] ^= t;
     X[2] ^= t;
-    keys[i] = (spread3(X[2]) | (spread3(X[1]) << 1) | (spread3(X[0]) << 2));
+    keys[i] = (uint32_t)(spread3(X[2]) | (spread3(X[1]) << 1) | (spread3(X[0]) << 2));
     idx[i] = (int32_t)i;
 }
 
@@ -524,12 +527,12 @@ int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) 
 
     // warp grouping of the self-queries (the Morton key buffers are free again)
     if (int rc = dev_alloc((void**)&t->qgroup, sizeof(int32_t) * n, st)) return rc;
-    k_hilbert<T><<<gN, kBlock, 0, st>>>((const T*)t->spos, n, (uint64_t*)keys.p, (int32_t*)idx.p);
+    k_hilbert<T><<<gN, kBlock, 0, st>>>((const T*)t->spos, n, (uint32_t*)keys.p, (int32_t*)idx.p);
     CAGR_CUDA(cudaGetLastError());
     if (int rc = cub_call(
             [&](void* tp, size_t& b) {
-                return cub::DeviceRadixSort::SortPairs(tp, b, (const uint64_t*)keys.p,
-                                                       (uint64_t*)sorted_keys.p,
+                return cub::DeviceRadixSort::SortPairs(tp, b, (const uint32_t*)keys.p,
+                                                       (uint32_t*)sorted_keys.p,
                                                        (const int32_t*)idx.p, t->qgroup, n, 0,
                                                        3 * kHilbertBits, st);
             },
