@@ -65,6 +65,7 @@ _SIGNATURES = {
     "cagr_adjoint": (_i32, [_p, _i32, _p, ctypes.c_double, _i32, _p, _p, _p]),
     "cagr_pool_reserved": (_i32, [_pi64, _pi64]),
     "cagr_debug_fail_allocations_after": (_i32, [_i64]),
+    "cagr_multiply_rhs_window": (_i32, [_p, _p, ctypes.c_double, _p, _i32, _p, _p]),
 }
 
 _lib = None

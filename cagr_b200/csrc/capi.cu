@@ -166,6 +166,22 @@ int cagr_multiply(const cagr_tree* tree, int op, const void* queries_dev,
     return cagr::traverse(tree->t, a, as_stream(stream));
 }
 
+int cagr_multiply_rhs_window(const cagr_tree* tree, const void* widths_dev, double width,
+                             const void* widths_hi_dev, int flags, void* out_dev, void* stream) {
+    if (int rc = check_tree(tree)) return rc;
+    if (flags & ~CAGR_FLAG_ACCUMULATE) return set_error(CAGR_ERR_INVALID, "unknown flag bits");
+    if (!widths_hi_dev) return set_error(CAGR_ERR_INVALID, "widths_hi must be a device buffer");
+    cagr::TraverseArgs a;
+    a.op = cagr::kOpA2TFused;
+    a.slots = 4;
+    a.accumulate = (flags & CAGR_FLAG_ACCUMULATE) ? 1 : 0;
+    a.widths = widths_dev;
+    a.width = width;
+    a.widths_hi = widths_hi_dev;
+    a.out = out_dev;
+    return cagr::traverse(tree->t, a, as_stream(stream));
+}
+
 int cagr_adjoint(cagr_tree* tree, int op, const void* widths_dev, double width, int flags,
                  const void* grad_out_dev, void* grad_attrs_dev, void* stream) {
     if (int rc = check_tree(tree)) return rc;

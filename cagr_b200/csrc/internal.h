@@ -113,6 +113,8 @@ struct TraverseArgs {
     int64_t nq = 0;
     const void* widths = nullptr;      // [nq] T or null (then `width`)
     double width = 0.0;
+    const void* widths_hi = nullptr;   // [nq] T or null: A2T right-hand side, b's terms
+                                       // only for t(widths) <= r^2 < t(widths_hi)
     void* out = nullptr;               // [nq, out_dim] T
     int out_stride = 0;                // scalars between consecutive queries (0 = out_dim)
     // regular-grid queries (instead of `queries`): node (i, j, k) at

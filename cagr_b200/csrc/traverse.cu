@@ -66,6 +66,7 @@ struct TravParams {
     const int32_t* qorder = nullptr;
     const T* widths = nullptr;
     T width = T(0);
+    const T* widths_hi = nullptr;  // A2T right-hand side: b's terms only below these widths
     int grid = 0;              // queries are the nodes of a regular grid
     int gx = 0, gy = 0, gz = 0;
     T gox = T(0), goy = T(0), goz = T(0), gh = T(0);
@@ -104,6 +105,7 @@ template <typename T>
 struct Lane {
     T q0, q1, q2;
     T tw;                 // width threshold on r^2 (r >= w  <=>  r^2 >= tw)
+    T twh;                // A2T right-hand side: b's terms need r^2 < twh as well
     T iw, iw3;            // 1/w, 1/w^3 (continuous kernel inside the width)
     T acc0, acc1, acc2;   // outside-width sums (without the per-query exp factor)
     T in0, in1, in2;      // inside-width sums (continuous kernel)
@@ -377,10 +379,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_traverse(const TravParams<T> p)
 //   acc += sum_k g_k (d / r^3 + e_k / (2r)),  g_k = exp(x_k/2) e_k(y) s,
 // where e(y) = exp(-y/2) comes from the record (folded per term so that the
 // three directions, which may use different sources, share one accumulator).
-template <typename T>
+template <typename T, bool WINDOW = false>
 __device__ __forceinline__ void a2t_term(Lane<T>& L, const T* ex, const T* e, T s, T dx, T dy,
                                          T dz, T d2, int klo, int khi) {
-    const bool outside = d2 >= L.tw;
+    // WINDOW: b's term in the right-hand side, kept only for tw <= r^2 < twh
+    const bool outside = d2 >= L.tw && (!WINDOW || d2 < L.twh);
     const T rinv = outside ? rsqrt_t(d2) : T(0);
     const T rinv3 = rinv * rinv * rinv;
     const T hr = T(0.5) * rinv;
@@ -502,7 +505,7 @@ __device__ __forceinline__ void rhs_b_point(Lane<T>& L, const T* pr, const T* ex
     const T py = sub_rn(L.q1, s0.y);
     const T pz = sub_rn(L.q2, s0.z);
     const T e[3] = {r1.x, r1.y, r1.z};
-    a2t_term(L, ex, e, r1.w, px, py, pz, dist2_exact(px, py, pz), 0, 3);
+    a2t_term<T, true>(L, ex, e, r1.w, px, py, pz, dist2_exact(px, py, pz), 0, 3);
 }
 
 // Slot K of the three-slot adjoint walk: acceptance test against the slot's
@@ -590,6 +593,8 @@ __device__ __forceinline__ void walk_a2t3(const TravParams<T>& p, const int64_t 
     int64_t oidx;
     T w;
     const bool valid = load_query(p, qi, L, oidx, w);
+    L.twh = T(INFINITY);
+    if (RHS && valid && p.widths_hi) L.twh = width_threshold(p.widths_hi[oidx]);
     const T ex0 = exp_t(L.q0 * T(0.5)), ex1 = exp_t(L.q1 * T(0.5)), ex2 = exp_t(L.q2 * T(0.5));
     // the s_k slots' sign: subtracted in the RHS form
     const T sg = RHS ? T(-1) : T(1);
@@ -627,9 +632,9 @@ __device__ __forceinline__ void walk_a2t3(const TravParams<T>& p, const int64_t 
         if (s1.active && s1.far) a2t_term1<T, 1>(L, true, gx1 * c1.w, s1.dx, s1.dy, s1.dz, s1.d2);
         if (s2.active && s2.far) a2t_term1<T, 2>(L, true, gx2 * c2.w, s2.dx, s2.dy, s2.dz, s2.d2);
         if constexpr (RHS) {
-            if (sb.active && sb.far) {
+            if (sb.active && sb.far && sb.d2 < L.twh) {
                 const T e[3] = {b1.x, b1.y, b1.z};
-                a2t_term(L, exb, e, b1.w, sb.dx, sb.dy, sb.dz, sb.d2, 0, 3);
+                a2t_term<T, true>(L, exb, e, b1.w, sb.dx, sb.dy, sb.dz, sb.d2, 0, 3);
             }
         }
         if (leaf) {
@@ -673,9 +678,12 @@ __device__ __forceinline__ void walk_a2t3(const TravParams<T>& p, const int64_t 
                             const Vec4<T> B0 = ld4(cr);
                             const ChildTest<T> tb = child_test(L, B0, rec_radius2(B0.w), true);
                             if (tb.far) {
-                                const Vec4<T> B1 = ld4(cr + 4);
-                                const T e[3] = {B1.x, B1.y, B1.z};
-                                a2t_term(L, exb, e, B1.w, tb.dx, tb.dy, tb.dz, tb.d2, 0, 3);
+                                if (tb.d2 < L.twh) {
+                                    const Vec4<T> B1 = ld4(cr + 4);
+                                    const T e[3] = {B1.x, B1.y, B1.z};
+                                    a2t_term<T, true>(L, exb, e, B1.w, tb.dx, tb.dy, tb.dz,
+                                                      tb.d2, 0, 3);
+                                }
                             } else {
                                 rhs_b_point(L, rb + ((int64_t)M + mt.y + c) * CAGR_REC_STRIDE, exb);
                             }
@@ -757,6 +765,7 @@ int dispatch(const Tree* t, const TraverseArgs& a, cudaStream_t s) {
     p.qorder = a.qorder;
     p.widths = (const T*)a.widths;
     p.width = (T)a.width;
+    p.widths_hi = (const T*)a.widths_hi;
     p.out = (T*)a.out;
     p.accumulate = a.accumulate;
     const bool scalar_in = a.op == kOpAT || a.op == kOpA2T1 || a.op == kOpA2T2 ||
@@ -1022,6 +1031,8 @@ int traverse(const Tree* t, const TraverseArgs& a, cudaStream_t stream) {
         return set_error(kErrInvalid, "grid queries need positive dims <= 2^20 and no query array");
     if (a.qorder && !a.queries)
         return set_error(kErrInvalid, "a query order needs explicit queries");
+    if (a.widths_hi && !(a.op == kOpA2TFused && a.slots == 4))
+        return set_error(kErrInvalid, "upper widths apply to the A2T right-hand side only");
     return t->dtype == 0 ? dispatch<float>(t, a, stream) : dispatch<double>(t, a, stream);
 }
 

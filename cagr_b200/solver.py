@@ -97,13 +97,20 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
     def scale(i):
         return wsmin + ((iters - 1 - i) / (iters - 1)) * (wsmax - wsmin)
 
+    # b is constant and the acceptance decisions do not depend on the width: b's
+    # terms at r >= the largest width of the steepest-descent phase are summed
+    # once (b_hi); each step's walk adds only b's terms below it
+    w_hi = base * max(scale(0), scale(min(n_sd, iters - 1)))
+    b_hi = None
+
     def RHS(a_mu, w):  # A2Tb(w) - A2T(a_mu) in one traversal (b's moments in slot 1)
         nonlocal calls
         calls += 6
-        return wn.forward_A2T_rhs(a_mu, w)
+        return wn.forward_A2T_rhs_window(a_mu, w, b_hi, w_hi)
 
     w = base * (wsmin + 0.5 * (wsmax - wsmin))
     rk1 = A2Tb(w)   # main_CAGR.py:98 (overwritten at i == n_sd)
+    b_hi = wn.forward_A2T_shared(b, w_hi)
     wn.scatter(b, slot=1)   # b is constant: its moments serve every iteration
     pk = rk1
     r = rk1

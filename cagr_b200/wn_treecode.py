@@ -332,6 +332,31 @@ class WindingNumberTreecode:
         self.scatter3(values3)
         return self.multiply("A2T_RHS", widths, out=out)
 
+    def forward_A2T_rhs_window(self, values3, widths, b_hi: torch.Tensor,
+                               widths_hi: torch.Tensor) -> torch.Tensor:
+        """forward_A2T_rhs(values3, widths) from b_hi = forward_A2T_shared(b, widths_hi)
+        with widths_hi >= widths per point: the walk adds only b's terms with
+        t(widths) <= r^2 < t(widths_hi) to b_hi and subtracts the values3 terms (the
+        acceptance decisions do not depend on the width, so the sum has exactly
+        the terms of forward_A2T_rhs).  b's moments must be in slot 1."""
+        assert len(values3.shape) == 2 and values3.shape[1] == 3
+        n = self.points.shape[0]
+        assert values3.shape[0] == n
+        b_hi = self._check_values(b_hi, "b_hi")
+        if b_hi.shape != (n, 3):
+            raise RuntimeError(f"b_hi must be [{n}, 3]")
+        whi = self._check_values(widths_hi, "widths_hi")
+        if whi.shape != (n,):
+            raise RuntimeError(f"widths_hi must be [{n}]")
+        wt, ws = self._widths(widths, n)
+        self.scatter3(values3)
+        out = b_hi.clone()
+        with torch.cuda.device(self.device):
+            check(_lib.lib().cagr_multiply_rhs_window(
+                self.handle, _ptr(wt), ws, _ptr(whi), _lib.FLAG_ACCUMULATE, _ptr(out),
+                _stream(self.device)), "cagr_multiply_rhs_window")
+        return out
+
     def forward_A2T_shared(self, values, widths, out: torch.Tensor | None = None,
                            accumulate: bool = False):
         """A2T1(s) + A2T2(s) + A2T3(s) -> [N, 3] for one scalar input s [N, 1]

@@ -233,6 +233,20 @@ int cagr_scatter_noalloc(const int64_t* parent_dev, const int64_t* children_dev,
  * b, 1, ...)), the s_k's from cagr_scatter3.  Every input keeps its own
  * moments and acceptance decisions, as in the separate calls; out [N',3]. */
 
+/* CAGR_OP_A2T_RHS on the tree's own points with b's terms restricted to
+ * t(w) <= r^2 < t(w_hi) (widths_dev or `width` give w, widths_hi_dev [n] gives
+ * w_hi >= w per point; t is the reference's `r >= w` test on r^2).  The
+ * acceptance decisions do not depend on the width, so with out holding
+ * sum_k A2Tk(b) at the widths w_hi (cagr_multiply, CAGR_OP_A2T_SUM_SHARED,
+ * b's moments in slot 0) and CAGR_FLAG_ACCUMULATE, out becomes exactly the
+ * CAGR_OP_A2T_RHS value at w, up to summation order: the b terms at r >= w_hi
+ * are the same in both, and those below are added here.  For the CAGR solve,
+ * whose widths shrink or grow along one schedule: b's far terms are evaluated
+ * once per solve instead of once per step.  The tree's points only; out [n,3]
+ * (original order); flags: CAGR_FLAG_ACCUMULATE. */
+int cagr_multiply_rhs_window(const cagr_tree* tree, const void* widths_dev, double width,
+                             const void* widths_hi_dev, int flags, void* out_dev, void* stream);
+
 /* Exact adjoint of CAGR_OP_A2_FUSED on the tree's own points (no counterpart
  * in the reference, whose A2T1..A2T3 are a different operator:
  * wn_treecode_cuda_kernels.cu:263-379 against :113-224).  With the slot-0

@@ -327,3 +327,28 @@ def test_query_grouping_changes_no_bit(cuda_lib, leaf_size):
         pairs.append((op, wn.multiply(op, w), wn.multiply(op, w, queries=P)))
     for op, a, c in pairs:
         assert torch.equal(a, c), op
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_a2t_rhs_window_equals_the_full_walk(cuda_lib, dtype):
+    """b's terms split at the upper widths: sum_k A2Tk(b) at widths_hi plus the
+    window walk (b's terms with t(w) <= r^2 < t(w_hi), minus the s_k terms)
+    equals the full right-hand-side walk at w (same terms, other summation
+    order), for widths below, equal to and well below widths_hi."""
+    torch = _torch()
+    pts = sphere_cloud(3000, seed=113, dtype=dtype)
+    n = len(pts)
+    rng = np.random.default_rng(114)
+    s = torch.from_numpy(random_values(n, 3, seed=115, dtype=dtype)).cuda()
+    b = torch.from_numpy(random_values(n, 1, seed=116, dtype=dtype)).cuda()
+    base = torch.from_numpy(rng.uniform(0.5, 1.5, n).astype(dtype)).cuda()
+    wn = _tree(pts)
+    wn.scatter(b, slot=1)
+    tl2, tmx = TOL[dtype]
+    for lo, hi in [(0.01, 0.04), (0.04, 0.04), (0.004, 0.06)]:
+        w, w_hi = base * lo, base * hi
+        full = wn.forward_A2T_rhs(s, w).cpu().numpy()
+        b_hi = wn.forward_A2T_shared(b, w_hi)
+        win = wn.forward_A2T_rhs_window(s, w, b_hi, w_hi).cpu().numpy()
+        l2, mx = rel_errors(win, full)
+        assert l2 <= tl2 and mx <= tmx, (lo, hi, l2, mx)
