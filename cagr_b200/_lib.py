@@ -54,6 +54,7 @@ _SIGNATURES = {
     "cagr_multiply": (_i32, [_p, _i32, _p, _p, _i64, _p, ctypes.c_double, _i32, _p, _i64, _p]),
     "cagr_forward": (_i32, [_p, _i32, _p, _p, ctypes.c_double, _i32, _p, _p]),
     "cagr_probe_fp32_peak": (_i32, [_i64, ctypes.POINTER(ctypes.c_double), _p]),
+    "cagr_probe_rsqrt64": (_i32, [_p, _p, _i64, _p]),
     "cagr_field_grid": (_i32, [_p, _i32, _i32, _i32, _i32, ctypes.POINTER(ctypes.c_double),
                                ctypes.c_double, _p, ctypes.c_double, _i32, _p, _p]),
     "cagr_marching_cubes": (_i32, [_p, _i32, _i32, _i32, ctypes.POINTER(ctypes.c_double),

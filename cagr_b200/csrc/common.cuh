@@ -123,7 +123,23 @@ __device__ __forceinline__ float rsqrt_t(float a) {
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
     return r;
 }
-__device__ __forceinline__ double rsqrt_t(double a) { return rsqrt(a); }
+// 1/sqrt(a) in double: the hardware approximation rsqrt.approx.f64 (relative
+// error about 2^-22), refined by one third-order step from the series
+// (1 - e)^(-1/2) = 1 + e/2 + 3e^2/8 + O(e^3) with e = 1 - a y^2, which takes
+// the error to the rounding level (measured within 2 ulp of CUDA's
+// rsqrt(double), and 1.3e-16 relative on the traversals' outputs, while the
+// FP64 walks run 6.46 -> 6.05 ms (A2T_SUM) and 3.41 -> 3.09 ms (A2_FUSED) at
+// 1M points).  a = 0 and a = +inf give NaN (CUDA's rsqrt gives inf and 0):
+// the traversals call it only for r^2 >= t(w) > 0, finite; with a width
+// w <= 0 a query on its own point divides by zero in the reference too.
+// (Keeping the approximation's exact 0 and inf by a select cost the whole
+// gain.)
+__device__ __forceinline__ double rsqrt_t(double a) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+    const double e = fma(-a * y, y, 1.0);
+    return fma(y * e, fma(0.375, e, 0.5), y);
+}
 __device__ __forceinline__ float exp_t(float a) { return expf(a); }
 __device__ __forceinline__ double exp_t(double a) { return exp(a); }
 

@@ -1,4 +1,6 @@
-// FP32 FMA throughput probe: the measured denominator of the treecode roofline.
+// FP32 FMA throughput probe: the measured denominator of the treecode roofline;
+// and the double-precision reciprocal square root the FP64 traversals use,
+// applied elementwise so that tests can compare it with CUDA's rsqrt(double).
 #include <string>
 
 #include "../../include/cagr.h"
@@ -25,7 +27,26 @@ __global__ void __launch_bounds__(256) k_fma_probe(int64_t iters, float b, float
     if (s == 1234.5f) sink[blockIdx.x] = s;  // keeps the chains alive; never true in practice
 }
 
+__global__ void k_rsqrt64(const double* __restrict__ in, double* __restrict__ out, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = cagr::rsqrt_t(in[i]);
+}
+
 }  // namespace
+
+extern "C" int cagr_probe_rsqrt64(const double* in_dev, double* out_dev, int64_t n,
+                                  void* stream) {
+    using cagr::set_error;
+    if (n < 0 || (n > 0 && (!in_dev || !out_dev)))
+        return set_error(CAGR_ERR_INVALID, "bad probe arguments");
+    if (n == 0) return CAGR_OK;
+    const int64_t blocks = (n + 255) / 256;
+    if (blocks > 0x7fffffffLL) return set_error(CAGR_ERR_INVALID, "too many values");
+    k_rsqrt64<<<(unsigned)blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(in_dev,
+                                                                                    out_dev, n);
+    CAGR_CUDA(cudaGetLastError());
+    return CAGR_OK;
+}
 
 extern "C" int cagr_probe_fp32_peak(int64_t iters, double* gflops, void* stream) {
     using cagr::set_error;

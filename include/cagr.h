@@ -272,6 +272,13 @@ int cagr_adjoint(cagr_tree* tree, int op, const void* widths_dev, double width, 
  * FP32-bound traversal kernels.  Synchronises `stream`. */
 int cagr_probe_fp32_peak(int64_t iters, double* gflops, void* stream);
 
+/* Diagnostic: out[i] = 1/sqrt(in[i]) for n doubles, computed as the FP64
+ * traversals compute it (a hardware approximation and one third-order
+ * correction), for comparison with CUDA's rsqrt(double): within 2 ulp for
+ * normal positive arguments; 0 and +inf give NaN (the traversals never pass
+ * them). */
+int cagr_probe_rsqrt64(const double* in_dev, double* out_dev, int64_t n, void* stream);
+
 /* Device memory (no counterpart in the reference, whose allocations are
  * torch's): every array the library allocates -- trees, node records, build
  * and marching-cubes scratch -- comes from one stream-ordered pool per device
