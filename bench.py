@@ -333,12 +333,15 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     # uploads while A.mu runs, A.mu's result downloads while A^T.w runs (all of
     # them inside the timed region: the step ends when the side stream is done)
     side = torch.cuda.Stream(device=dev)
-    w_up, a_done = torch.cuda.Event(), torch.cuda.Event()
+    w_up, a_done, mu_up = torch.cuda.Event(), torch.cuda.Event(), torch.cuda.Event()
 
     def e2e_step():
         side.wait_stream(stream)                 # the previous step is done with d_w
         d_mu.copy_(h_mu, non_blocking=True)
+        mu_up.record(stream)
         with torch.cuda.stream(side):
+            # w follows mu over the bus: mu, which A.mu waits for, gets all of it
+            side.wait_event(mu_up)
             d_w.copy_(h_w, non_blocking=True)
             w_up.record(side)
         oa = wn.forward_A2(d_mu, W)
