@@ -44,7 +44,7 @@ L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the two
 # traversals on this workload, from one ncu capture of these kernels
 # (profiles/step_kernels_union8_1M.md); ncu is not run inside the bench
-TRAFFIC_BYTES = {"A2T_SUM": 163_854_848 + 6_910_976, "A2_FUSED": 136_392_192 + 5_505_792}
+TRAFFIC_BYTES = {"A2T_SUM": 165_164_800 + 7_062_784, "A2_FUSED": 136_392_704 + 5_499_904}
 
 
 def parse():
