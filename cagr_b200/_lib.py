@@ -67,6 +67,7 @@ _SIGNATURES = {
     "cagr_pool_reserved": (_i32, [_pi64, _pi64]),
     "cagr_debug_fail_allocations_after": (_i32, [_i64]),
     "cagr_multiply_rhs_window": (_i32, [_p, _p, ctypes.c_double, _p, _i32, _p, _p]),
+    "cagr_b_window_table": (_i32, [_p, _p, _p, _i32, _p, _p]),
 }
 
 _lib = None

@@ -182,6 +182,13 @@ int cagr_multiply_rhs_window(const cagr_tree* tree, const void* widths_dev, doub
     return cagr::traverse(tree->t, a, as_stream(stream));
 }
 
+int cagr_b_window_table(const cagr_tree* tree, const void* base_dev, const void* scales_dev,
+                        int num_scales, void* out_dev, void* stream) {
+    if (int rc = check_tree(tree)) return rc;
+    return cagr::b_window_table(tree->t, base_dev, scales_dev, num_scales, out_dev,
+                                as_stream(stream));
+}
+
 int cagr_adjoint(cagr_tree* tree, int op, const void* widths_dev, double width, int flags,
                  const void* grad_out_dev, void* grad_attrs_dev, void* stream) {
     if (int rc = check_tree(tree)) return rc;

@@ -127,6 +127,13 @@ struct TraverseArgs {
 
 int traverse(const Tree* t, const TraverseArgs& a, cudaStream_t stream);
 
+// For the widths w_i = base * scales[i] (scales ascending, device [S], S <= 64;
+// base device [n], original order) with b's moments in record slot 1:
+// out[i] [n, 3] = b's A2T terms (summed over the three directions) kept at w_i
+// and below w_hi = base * scales[S-1].
+int b_window_table(const Tree* t, const void* base, const void* scales, int S, void* out,
+                   cudaStream_t stream);
+
 // J^T grad for the fused A2 on the tree's points (a.op = kOpA2Fused; a.widths,
 // a.width, a.continuous as in the forward); grad and grad_attrs [n,3] in
 // original point order.

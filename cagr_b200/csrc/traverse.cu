@@ -1027,6 +1027,154 @@ int adjoint_impl(const Tree* t, const TraverseArgs& a, const void* grad, void* g
     return rc;
 }
 
+
+// ---- b's window table for a schedule of widths -------------------------------
+//
+// The CAGR solve forms sum_k A2Tk(b) at the widths w_i = base * s_i of its
+// steepest-descent steps (main_CAGR.py:98,108), b constant.  The acceptance
+// decisions do not depend on the width, and a term is kept at width w iff
+// sqrt_rn(r^2) >= w (the reference's test), so one walk over b's moments can
+// serve every step: each of b's terms with r < w_hi (w_hi = base * s_max; the
+// terms beyond are the same at every step and summed once, at w_hi) goes to
+// the bucket of the number of step widths it passes; out[i] is then the sum of
+// the buckets of the steps >= i (scales ascending), i.e. exactly b's terms at
+// w_i below w_hi.  Each query's buckets are a row of `rows` [nq][S*3] owned by
+// its lane (no atomics), zeroed by the caller.
+template <typename T>
+__device__ __forceinline__ void b_bucket(T* row, const T* sc, int S, T base, T twh, const T* ex,
+                                         const Vec4<T>& r1, T dx, T dy, T dz, T d2) {
+    if (!(d2 < twh)) return;  // r >= w_hi: kept at every step, summed at w_hi
+    const T r = sqrt_rn(d2);
+    int lo = 0, hi = S;       // number of i with base * s_i <= r (s ascending)
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (mul_rn(base, sc[mid]) <= r) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo == 0) return;      // kept at no step
+    const T rinv = rsqrt_t(d2);
+    const T rinv3 = rinv * rinv * rinv;
+    const T hr = T(0.5) * rinv;
+    const T g0 = ex[0] * r1.x * r1.w, g1 = ex[1] * r1.y * r1.w, g2 = ex[2] * r1.z * r1.w;
+    const T c = (g0 + g1 + g2) * rinv3;
+    T* b = row + (lo - 1) * 3;
+    b[0] += dx * c + g0 * hr;
+    b[1] += dy * c + g1 * hr;
+    b[2] += dz * c + g2 * hr;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kWarps * 32) k_b_window(const TravParams<T> p, const T* base,
+                                                          const T* scales, int S, T* rows,
+                                                          T* out) {
+    __shared__ T sc[64];
+    for (int i = threadIdx.x; i < S; i += blockDim.x) sc[i] = scales[i];
+    __syncthreads();
+    const int64_t qi = lane_query();
+    if (__all_sync(kFull, qi >= p.nq)) return;
+    Lane<T> L;
+    int64_t oidx;
+    T w;
+    const bool valid = load_query(p, qi, L, oidx, w);
+    const T bq = valid ? base[oidx] : T(0);
+    const T twh = valid ? width_threshold(mul_rn(bq, sc[S - 1])) : T(0);
+    T* row = rows + (valid ? oidx : 0) * (int64_t)S * 3;
+    const T ex[3] = {exp_t(L.q0 * T(0.5)), exp_t(L.q1 * T(0.5)), exp_t(L.q2 * T(0.5))};
+    const int M = (int)p.M;
+    const T* __restrict__ rec = p.rec[1];
+    int kd = valid ? 0 : -1;
+    int n = 0;
+    while (n < M) {
+        const int4 mt = __ldg(p.meta + n);
+        const int d = node_depth(mt);
+        const bool leaf = node_leaf(mt);
+        const T* r = rec + (int64_t)n * CAGR_REC_STRIDE;
+        const Vec4<T> r0 = ld4(r);
+        T dx = sub_rn(L.q0, r0.x);
+        T dy = sub_rn(L.q1, r0.y);
+        T dz = sub_rn(L.q2, r0.z);
+        T d2 = dist2_exact(dx, dy, dz);
+        const bool active = d <= kd;
+        const bool far = d2 > rec_radius2(r0.w);
+        const bool open = active && !far;
+        if (active) kd = (open && !leaf) ? d + 1 : d;
+        const bool any_open = __any_sync(kFull, open);
+        const T* src = r;
+        if (leaf && open) {
+            src = rec + ((int64_t)M + mt.y) * CAGR_REC_STRIDE;
+            const Vec4<T> s0 = ld4(src);
+            dx = sub_rn(L.q0, s0.x);
+            dy = sub_rn(L.q1, s0.y);
+            dz = sub_rn(L.q2, s0.z);
+            d2 = dist2_exact(dx, dy, dz);
+        }
+        if (active && (far || leaf) && d2 < twh)
+            b_bucket(row, sc, S, bq, twh, ex, ld4(src + 4), dx, dy, dz, d2);
+        if (leaf) {
+            const int np = -mt.z;
+            if (np > 1 && any_open) {
+                const T* pr = rec + ((int64_t)M + mt.y + 1) * CAGR_REC_STRIDE;
+                for (int j = 1; j < np; j++, pr += CAGR_REC_STRIDE) {
+                    if (open) {
+                        const Vec4<T> s0 = ld4(pr);
+                        const T px = sub_rn(L.q0, s0.x);
+                        const T py = sub_rn(L.q1, s0.y);
+                        const T pz = sub_rn(L.q2, s0.z);
+                        const T pd2 = dist2_exact(px, py, pz);
+                        if (pd2 < twh) b_bucket(row, sc, S, bq, twh, ex, ld4(pr + 4), px, py, pz, pd2);
+                    }
+                }
+            }
+            n = mt.x;
+        } else {
+            n = any_open ? n + 1 : mt.x;
+        }
+    }
+    if (!valid) return;
+    // out[i] = sum of the buckets of the steps >= i: the exp(x/2) factors are in g
+    T a0 = T(0), a1 = T(0), a2 = T(0);
+    const int64_t stride = p.nq * 3;
+    for (int i = S - 1; i >= 0; i--) {
+        a0 += row[i * 3];
+        a1 += row[i * 3 + 1];
+        a2 += row[i * 3 + 2];
+        T* o = out + i * stride + oidx * 3;
+        o[0] = a0;
+        o[1] = a1;
+        o[2] = a2;
+    }
+}
+
+template <typename T>
+int b_window_impl(const Tree* t, const void* base, const void* scales, int S, void* out,
+                  cudaStream_t s) {
+    if (!t->rec[1] || t->rec_dim[1] != 1)
+        return set_error(kErrState, "b's window table needs b's moments in slot 1");
+    TravParams<T> p;
+    p.M = t->m;
+    p.N = t->n;
+    p.nq = t->n;
+    p.meta = t->meta;
+    p.spos = (const T*)t->spos;
+    p.perm = t->perm;
+    p.qgroup = t->qgroup;
+    p.rec[1] = (const T*)t->rec[1];
+    p.width = T(0);
+    void* rows = nullptr;
+    const size_t row_bytes = sizeof(T) * (size_t)t->n * S * 3;
+    if (int rc = pool_alloc(&rows, row_bytes, s)) return rc;
+    int rc = kOk;
+    if (cudaMemsetAsync(rows, 0, row_bytes, s) != cudaSuccess) {
+        rc = set_error(kErrCuda, "window table scratch");
+    } else {
+        const int64_t blocks = ((t->n + 31) / 32 + kWarps - 1) / kWarps;
+        k_b_window<T><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p, (const T*)base, (const T*)scales,
+                                                               S, (T*)rows, (T*)out);
+        if (cudaGetLastError() != cudaSuccess) rc = set_error(kErrCuda, "window table launch");
+    }
+    pool_free(rows, s);
+    return rc;
+}
 }  // namespace
 
 int traverse(const Tree* t, const TraverseArgs& a, cudaStream_t stream) {
@@ -1041,6 +1189,14 @@ int traverse(const Tree* t, const TraverseArgs& a, cudaStream_t stream) {
     if (a.widths_hi && !(a.op == kOpA2TFused && a.slots == 4))
         return set_error(kErrInvalid, "upper widths apply to the A2T right-hand side only");
     return t->dtype == 0 ? dispatch<float>(t, a, stream) : dispatch<double>(t, a, stream);
+}
+
+int b_window_table(const Tree* t, const void* base, const void* scales, int S, void* out,
+                   cudaStream_t stream) {
+    if (S < 1 || S > 64) return set_error(kErrInvalid, "1 to 64 scales");
+    if (!base || !scales || !out) return set_error(kErrInvalid, "null buffer");
+    return t->dtype == 0 ? b_window_impl<float>(t, base, scales, S, out, stream)
+                         : b_window_impl<double>(t, base, scales, S, out, stream);
 }
 
 int adjoint(const Tree* t, const TraverseArgs& a, const void* grad, void* grad_attrs,

@@ -97,34 +97,43 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
     def scale(i):
         return wsmin + ((iters - 1 - i) / (iters - 1)) * (wsmax - wsmin)
 
-    # b is constant and the acceptance decisions do not depend on the width: b's
-    # terms at r >= the largest width of the steepest-descent phase are summed
-    # once (b_hi); each step's walk adds only b's terms below it
-    w_hi = base * max(scale(0), scale(min(n_sd, iters - 1)))
-    b_hi = None
+    # b is constant and the acceptance decisions do not depend on the width, so
+    # A2Tb at every steepest-descent width comes from two walks per solve: b's
+    # terms at r >= the largest of those widths (b_hi), and a table of b's terms
+    # below it, bucketed by the step widths they pass (b_window_table).  Those
+    # steps' widths are base * s with s rounded to the points' dtype, as the
+    # table's kernel forms them.
+    sd_steps = range(min(n_sd, iters - 1) + 1)
+    dt = points.dtype
+    s_of = {i: float(torch.tensor(scale(i), dtype=dt)) for i in sd_steps}
+    sd_scales = sorted(set(s_of.values()))
+    sc_t = torch.tensor(sd_scales, dtype=dt, device=dev)
+    slot_of = {i: sd_scales.index(s_of[i]) for i in sd_steps}
+    b_hi = b_table = None
 
-    def RHS(a_mu, w):  # A2Tb(w) - A2T(a_mu) in one traversal (b's moments in slot 1)
+    def RHS(a_mu, i, w):  # A2Tb(w) - A2T(a_mu)
         nonlocal calls
         calls += 6
-        return wn.forward_A2T_rhs_window(a_mu, w, b_hi, w_hi)
+        return (b_hi + b_table[slot_of[i]]) - wn.forward_A2T_sum(a_mu, w)
 
     w = base * (wsmin + 0.5 * (wsmax - wsmin))
     rk1 = A2Tb(w)   # main_CAGR.py:98 (overwritten at i == n_sd)
-    b_hi = wn.forward_A2T_shared(b, w_hi)
-    wn.scatter(b, slot=1)   # b is constant: its moments serve every iteration
+    b_hi = wn.forward_A2T_shared(b, base * sc_t[-1])
+    wn.scatter(b, slot=1)   # b is constant: its moments serve every step
+    b_table = wn.b_window_table(base, sc_t)
     pk = rk1
     r = rk1
     for i in range(iters):
-        w = base * scale(i)
+        w = base * sc_t[slot_of[i]] if i in slot_of else base * scale(i)
         if i <= n_sd:
             A_mu = -A2(normals, w)
-            r = RHS(A_mu.contiguous(), w) - lambda0 * normals   # A2Tb(w) - A2T(A_mu)
+            r = RHS(A_mu.contiguous(), i, w) - lambda0 * normals   # A2Tb(w) - A2T(A_mu)
             A_r = -A2(r.contiguous(), w).sum(1, keepdim=True)
             alpha = (_dot(r, r) / _dot(A_r, A_r)).float()
             normals = normals + alpha * r
             if i == n_sd:
                 A_mu = -A2(normals, w)
-                rk1 = RHS(A_mu.contiguous(), w) - lambda0 * normals
+                rk1 = RHS(A_mu.contiguous(), i, w) - lambda0 * normals
                 pk = rk1
         else:
             A_pk = -A2(pk.contiguous(), w)

@@ -332,6 +332,25 @@ class WindingNumberTreecode:
         self.scatter3(values3)
         return self.multiply("A2T_RHS", widths, out=out)
 
+    def b_window_table(self, base: torch.Tensor, scales: torch.Tensor) -> torch.Tensor:
+        """[S, N, 3]: for each width w_i = base * scales[i] (scales ascending, 1..64),
+        b's sum_k A2Tk terms kept at w_i and below w_hi = base * scales[-1], from one
+        walk (b's moments must be in slot 1).  forward_A2T_shared(b, base * scales[-1])
+        + table[i] = forward_A2T_shared(b, base * scales[i]) up to summation order."""
+        n = self.points.shape[0]
+        base = self._check_values(base, "base")
+        sc = self._check_values(scales, "scales")
+        if base.shape != (n,) or sc.dim() != 1 or not (1 <= sc.shape[0] <= 64):
+            raise RuntimeError(f"base must be [{n}] and scales [S], 1 <= S <= 64")
+        if sc.shape[0] > 1 and bool((sc[1:] < sc[:-1]).any()):
+            raise RuntimeError("scales must be ascending")
+        out = torch.empty(sc.shape[0], n, 3, dtype=self.dtype, device=self.device)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().cagr_b_window_table(self.handle, _ptr(base), _ptr(sc), sc.shape[0],
+                                                 _ptr(out), _stream(self.device)),
+                  "cagr_b_window_table")
+        return out
+
     def forward_A2T_rhs_window(self, values3, widths, b_hi: torch.Tensor,
                                widths_hi: torch.Tensor) -> torch.Tensor:
         """forward_A2T_rhs(values3, widths) from b_hi = forward_A2T_shared(b, widths_hi)

@@ -247,6 +247,20 @@ int cagr_scatter_noalloc(const int64_t* parent_dev, const int64_t* children_dev,
 int cagr_multiply_rhs_window(const cagr_tree* tree, const void* widths_dev, double width,
                              const void* widths_hi_dev, int flags, void* out_dev, void* stream);
 
+/* b's part of the right-hand side for a whole schedule of widths in one walk:
+ * for w_i = base * scales[i] (scales_dev [num_scales] ascending, 1..64 of
+ * them; base_dev [n]; both in the tree dtype on the device, the product
+ * rounded once as the caller's own base * scale), with b's moments in record
+ * slot 1, out_dev [num_scales, n, 3] receives for each i the sum of b's
+ * sum_k A2Tk terms kept at w_i (r >= w_i, the reference's test) with
+ * r < w_hi = base * scales[num_scales - 1].  Adding
+ * cagr_multiply(CAGR_OP_A2T_SUM_SHARED) at w_hi (b's moments in slot 0) gives
+ * sum_k A2Tk(b) at every w_i, up to summation order: the acceptance decisions
+ * do not depend on the width.  Allocates n * num_scales * 3 scalars of
+ * scratch from the pool. */
+int cagr_b_window_table(const cagr_tree* tree, const void* base_dev, const void* scales_dev,
+                        int num_scales, void* out_dev, void* stream);
+
 /* Exact adjoint of CAGR_OP_A2_FUSED on the tree's own points (no counterpart
  * in the reference, whose A2T1..A2T3 are a different operator:
  * wn_treecode_cuda_kernels.cu:263-379 against :113-224).  With the slot-0

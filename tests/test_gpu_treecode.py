@@ -352,3 +352,31 @@ def test_a2t_rhs_window_equals_the_full_walk(cuda_lib, dtype):
         win = wn.forward_A2T_rhs_window(s, w, b_hi, w_hi).cpu().numpy()
         l2, mx = rel_errors(win, full)
         assert l2 <= tl2 and mx <= tmx, (lo, hi, l2, mx)
+
+
+@pytest.mark.parametrize("cloud", ["sphere", "edge"])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_b_window_table_equals_the_walks_at_each_width(cuda_lib, dtype, cloud):
+    """One walk for a schedule of widths: sum_k A2Tk(b) at base * scales[-1]
+    plus row i of the table equals the walk at base * scales[i] (same terms,
+    other summation order); the last row is empty."""
+    torch = _torch()
+    pts = (sphere_cloud(3000, seed=118, dtype=dtype) if cloud == "sphere"
+           else edge_cloud(seed=122, dtype=dtype))
+    n = len(pts)
+    b = torch.from_numpy(random_values(n, 1, seed=119, dtype=dtype)).cuda()
+    base = torch.from_numpy(np.random.default_rng(121).uniform(0.5, 1.5, n).astype(dtype)).cuda()
+    scales = torch.tensor([0.002, 0.005, 0.011, 0.016, 0.04, 0.09], device="cuda",
+                          dtype=base.dtype)
+    wn = _tree(pts)
+    wn.scatter(b, slot=1)
+    table = wn.b_window_table(base, scales)
+    assert table.shape == (len(scales), n, 3)
+    assert torch.equal(table[-1], torch.zeros_like(table[-1]))
+    b_hi = wn.forward_A2T_shared(b, base * scales[-1])
+    tl2, tmx = TOL[dtype]
+    for i in range(len(scales)):
+        want = wn.forward_A2T_shared(b, base * scales[i]).cpu().numpy()
+        got = (b_hi + table[i]).cpu().numpy()
+        l2, mx = rel_errors(got, want)
+        assert l2 <= tl2 and mx <= tmx, (i, l2, mx)
