@@ -48,7 +48,7 @@ def normalize_points(points_unnormalized: np.ndarray, bbox_scale: float = 1.1) -
 
 @dataclasses.dataclass
 class SolveResult:
-    normals: torch.Tensor          # [N, 3] float32, the solved mu (area-weighted normals)
+    normals: torch.Tensor          # [N, 3] in the points' dtype, the solved mu (area-weighted normals)
     residual_norm: float           # |r| after the steepest-descent phase (main_CAGR.py:165)
     rk_norm: float                 # |rk1| after the CG phase (main_CAGR.py:166)
     time_tree_s: float
@@ -74,9 +74,10 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
     wn = tree if tree is not None else WindingNumberTreecode(points, max_tree_depth)
     torch.cuda.synchronize(dev)
     t1 = time.perf_counter()
-    base = torch.ones(n, device=dev) if widths is None else widths
-    normals = torch.zeros(n, 3, device=dev)
-    b = torch.full((n, 1), 0.5, device=dev)   # main_CAGR.py:50
+    dt = points.dtype   # float32 as the reference runs it; float64 works alike
+    base = torch.ones(n, device=dev, dtype=dt) if widths is None else widths
+    normals = torch.zeros(n, 3, device=dev, dtype=dt)
+    b = torch.full((n, 1), 0.5, device=dev, dtype=dt)   # main_CAGR.py:50
     calls = 0
 
     def A2(x, w):   # [A21 | A22 | A23](x)
@@ -104,7 +105,6 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
     # steps' widths are base * s with s rounded to the points' dtype, as the
     # table's kernel forms them.
     sd_steps = range(min(n_sd, iters - 1) + 1)
-    dt = points.dtype
     s_of = {i: float(torch.tensor(scale(i), dtype=dt)) for i in sd_steps}
     sd_scales = sorted(set(s_of.values()))
     sc_t = torch.tensor(sd_scales, dtype=dt, device=dev)
@@ -129,7 +129,7 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
             A_mu = -A2(normals, w)
             r = RHS(A_mu.contiguous(), i, w) - lambda0 * normals   # A2Tb(w) - A2T(A_mu)
             A_r = -A2(r.contiguous(), w).sum(1, keepdim=True)
-            alpha = (_dot(r, r) / _dot(A_r, A_r)).float()
+            alpha = (_dot(r, r) / _dot(A_r, A_r)).to(dt)
             normals = normals + alpha * r
             if i == n_sd:
                 A_mu = -A2(normals, w)
@@ -139,10 +139,10 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
             A_pk = -A2(pk.contiguous(), w)
             AT_A_pk = A2T(A_pk.contiguous(), w)
             den = _dot(AT_A_pk, pk) + lambda0 * _dot(pk, pk)
-            alpha = (_dot(rk1, rk1) / den).float()
+            alpha = (_dot(rk1, rk1) / den).to(dt)
             normals = normals + alpha * pk
             rk20 = rk1 - alpha * AT_A_pk - alpha * lambda0 * pk
-            beta = (_dot(rk20, rk20) / _dot(rk1, rk1)).float()
+            beta = (_dot(rk20, rk20) / _dot(rk1, rk1)).to(dt)
             pk = rk20 + beta * pk
             rk1 = rk20
     r_norm = torch.linalg.norm(r.double())
@@ -153,7 +153,7 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
         g = wn.forward_G(normals.contiguous(), w).double()
         g = g / torch.clamp(torch.linalg.norm(g, dim=-1, keepdim=True), min=1e-12)
         length = torch.linalg.norm(normals.double(), dim=-1, keepdim=True)
-        normals = (g * length).float().contiguous()
+        normals = (g * length).to(dt).contiguous()
     torch.cuda.synchronize(dev)
     t2 = time.perf_counter()
     return SolveResult(normals, float(r_norm), float(rk_norm), t1 - t0, t2 - t1, calls)

@@ -57,3 +57,16 @@ def test_solve_accepts_per_point_widths(cuda_lib):
     a = cagr_solve(pts, 0.01, 0.04, iters=4)
     b = cagr_solve(pts, 0.01, 0.04, iters=4, widths=torch.ones(pts.shape[0], device="cuda"))
     assert torch.equal(a.normals, b.normals)
+
+
+def test_float64_solve_reproduces_the_published_signs(cuda_lib):
+    """The same solve in float64 (points, widths, moments and sums): the
+    published output's signs as in float32."""
+    import torch
+    from cagr_b200.solver import PRESET_WIDTHS, cagr_solve
+    g, pts = _bunny()
+    res = cagr_solve(pts.double(), *PRESET_WIDTHS["l0"], iters=10)
+    assert res.normals.dtype == torch.float64
+    mu = res.normals.cpu().numpy()
+    assert np.isfinite(mu).all()
+    assert _agree(mu, g["mu_reference"]) >= 0.995
