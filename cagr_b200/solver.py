@@ -90,23 +90,20 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
         calls += 3
         return wn.forward_A2T_sum(v3, w)
 
-    def A2Tb(w):     # A2T1(b) + A2T2(b) + A2T3(b): one input, one set of moments
-        nonlocal calls
-        calls += 3
-        return wn.forward_A2T_shared(b, w)
-
     def scale(i):
         return wsmin + ((iters - 1 - i) / (iters - 1)) * (wsmax - wsmin)
 
     # b is constant and the acceptance decisions do not depend on the width, so
     # A2Tb at every steepest-descent width comes from two walks per solve: b's
     # terms at r >= the largest of those widths (b_hi), and a table of b's terms
-    # below it, bucketed by the step widths they pass (b_window_table).  Those
-    # steps' widths are base * s with s rounded to the points' dtype, as the
+    # below it, bucketed by the step widths they pass (b_window_table); the
+    # initial right-hand side, at the middle width, comes from the table too.
+    # These widths are base * s with s rounded to the points' dtype, as the
     # table's kernel forms them.
     sd_steps = range(min(n_sd, iters - 1) + 1)
     s_of = {i: float(torch.tensor(scale(i), dtype=dt)) for i in sd_steps}
-    sd_scales = sorted(set(s_of.values()))
+    s_mid = float(torch.tensor(wsmin + 0.5 * (wsmax - wsmin), dtype=dt))
+    sd_scales = sorted(set(s_of.values()) | {s_mid})
     sc_t = torch.tensor(sd_scales, dtype=dt, device=dev)
     slot_of = {i: sd_scales.index(s_of[i]) for i in sd_steps}
     b_hi = b_table = None
@@ -116,11 +113,11 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
         calls += 6
         return (b_hi + b_table[slot_of[i]]) - wn.forward_A2T_sum(a_mu, w)
 
-    w = base * (wsmin + 0.5 * (wsmax - wsmin))
-    rk1 = A2Tb(w)   # main_CAGR.py:98 (overwritten at i == n_sd)
     b_hi = wn.forward_A2T_shared(b, base * sc_t[-1])
     wn.scatter(b, slot=1)   # b is constant: its moments serve every step
     b_table = wn.b_window_table(base, sc_t)
+    calls += 3   # the reference's A2T1..3(b) at the middle width
+    rk1 = b_hi + b_table[sd_scales.index(s_mid)]   # main_CAGR.py:98 (overwritten at i == n_sd)
     pk = rk1
     r = rk1
     for i in range(iters):
