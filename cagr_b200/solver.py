@@ -27,6 +27,9 @@ import torch
 
 from .wn_treecode import WindingNumberTreecode
 
+# b's window table (cagr_b_window_table) takes at most this many widths
+MAX_TABLE_WIDTHS = 64
+
 # main_CAGR.py:74-82
 PRESET_WIDTHS = {
     "l0": (0.002, 0.016),
@@ -108,16 +111,26 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
     slot_of = {i: sd_scales.index(s_of[i]) for i in sd_steps}
     b_hi = b_table = None
 
+    # more widths than the table takes: each step's four-slot walk adds b's
+    # terms below the largest width itself
+    use_table = len(sd_scales) <= MAX_TABLE_WIDTHS
+    w_hi = base * sc_t[-1]
+
     def RHS(a_mu, i, w):  # A2Tb(w) - A2T(a_mu)
         nonlocal calls
         calls += 6
-        return (b_hi + b_table[slot_of[i]]) - wn.forward_A2T_sum(a_mu, w)
+        if use_table:
+            return (b_hi + b_table[slot_of[i]]) - wn.forward_A2T_sum(a_mu, w)
+        return wn.forward_A2T_rhs_window(a_mu, w, b_hi, w_hi)
 
-    b_hi = wn.forward_A2T_shared(b, base * sc_t[-1])
+    b_hi = wn.forward_A2T_shared(b, w_hi)
     wn.scatter(b, slot=1)   # b is constant: its moments serve every step
-    b_table = wn.b_window_table(base, sc_t)
-    calls += 3   # the reference's A2T1..3(b) at the middle width
-    rk1 = b_hi + b_table[sd_scales.index(s_mid)]   # main_CAGR.py:98 (overwritten at i == n_sd)
+    calls += 3   # the reference's A2T1..3(b) at the middle width (main_CAGR.py:98)
+    if use_table:
+        b_table = wn.b_window_table(base, sc_t)
+        rk1 = b_hi + b_table[sd_scales.index(s_mid)]   # overwritten at i == n_sd
+    else:
+        rk1 = wn.forward_A2T_shared(b, base * sc_t[sd_scales.index(s_mid)])
     pk = rk1
     r = rk1
     for i in range(iters):

@@ -70,3 +70,19 @@ def test_float64_solve_reproduces_the_published_signs(cuda_lib):
     mu = res.normals.cpu().numpy()
     assert np.isfinite(mu).all()
     assert _agree(mu, g["mu_reference"]) >= 0.995
+
+
+def test_width_table_and_its_fallback_give_the_same_solve(cuda_lib, monkeypatch):
+    """b's window table (one walk for all steepest-descent widths) and the
+    fallback for schedules with more widths than the table takes (each step's
+    four-slot walk adds b's window itself) sum the same terms: the same solve
+    up to rounding."""
+    from cagr_b200 import solver
+    _, pts = _bunny()
+    a = solver.cagr_solve(pts, 0.01, 0.04, iters=8, n_sd=5, wnnc_steps=0)
+    monkeypatch.setattr(solver, "MAX_TABLE_WIDTHS", 0)
+    b = solver.cagr_solve(pts, 0.01, 0.04, iters=8, n_sd=5, wnnc_steps=0)
+    mu_a, mu_b = a.normals.cpu().numpy(), b.normals.cpu().numpy()
+    assert a.operator_calls == b.operator_calls
+    assert _agree(mu_a, mu_b) >= 0.999
+    assert np.linalg.norm(mu_a - mu_b) <= 1e-3 * np.linalg.norm(mu_a)
