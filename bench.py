@@ -42,9 +42,13 @@ FLOPS_A2_FUSED = 29      # three directions
 FLOPS_A2T = 22           # d (3) + |d|^2 (5) + r^-3 (2) + e s r^-3 (2) + 3 FMA (6) + e s r^-1/2 (3) + add (1)
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the two
-# traversals on this workload, from one ncu capture of these kernels
-# (profiles/step_kernels_union8_1M.md); ncu is not run inside the bench
+# traversals on this workload, taken from one ncu capture of these kernels with
+# the command below; ncu does not run inside the bench, so these are constants
+# of that capture, reported as such (roofline.traffic_source)
 TRAFFIC_BYTES = {"A2T_SUM": 165_164_800 + 7_062_784, "A2_FUSED": 136_392_704 + 5_499_904}
+TRAFFIC_SOURCE = ("ncu --set full --clock-control none -k regex:k_traverse -c 2 python bench.py "
+                  "--steps 1 --warmup 1 --no-cpu-baseline --no-fp64 --no-solve (one capture, "
+                  "not measured in this run)")
 
 
 def parse():
@@ -59,8 +63,6 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--grid", type=int, default=512, help="field grid for the end-to-end run")
-    ap.add_argument("--cpu-sample", type=int, default=0,
-                    help="queries per operator timed on the CPU (0 = auto)")
     return ap.parse_args()
 
 
@@ -150,22 +152,34 @@ class ClockSampler:
 
 # ------------------------------------------------------------- CPU legs -------
 
-def cpu_reference_step_ms(p, widths, mu, wvals, sample: int, threads: int):
-    """The reference's own CPU-side algorithm for one step on a bounded sample:
-    the reference CUDA kernels compiled for the host (oracle/_ref) when present,
-    else the C restatement.  Per A21/A22/A23/A2T1/A2T2/A2T3 call: |value|
-    weights, full node moments, traversal of `sample` queries; traversal time
-    is scaled to all queries.  Returns (ms per full step, kind, description)."""
-    from oracle.oracle import Oracle, RefOracle, point_weights
-    try:
-        impl, kind = RefOracle(), "reference"
-    except (FileNotFoundError, OSError):
-        impl, kind = Oracle(), "port"
-    n = p.shape[0]
-    tree = impl.build_tree(p)
-    rng = np.random.default_rng(7)
-    sel = np.sort(rng.choice(n, size=min(sample, n), replace=False))
-    q, wq = p[sel], widths[sel]
+class CpuReference:
+    """The reference's own CPU-side algorithm for the step: the reference CUDA
+    kernels compiled for the host (oracle/_ref) when present, else the C
+    restatement, on every host thread (OpenMP over queries).  The tree is built
+    once, as the reference builds it once per solve."""
+
+    def __init__(self, p):
+        from oracle.oracle import Oracle, RefOracle
+        try:
+            self.impl, self.kind = RefOracle(), "reference"
+        except (FileNotFoundError, OSError):
+            self.impl, self.kind = Oracle(), "port"
+        self.tree = self.impl.build_tree(p)
+
+    def step_ms(self, p, widths, mu, wvals, threads: int):
+        """One full step: per A21/A22/A23/A2T1/A2T2/A2T3 call |value| weights,
+        node moments over the whole tree and the traversal of all queries.
+        Returns (ms, description)."""
+        ms = cpu_reference_step_ms(self.impl, self.tree, p, widths, mu, wvals)
+        desc = (f"the whole step: all {p.shape[0]:,} queries per operator, node moments "
+                f"over all {self.tree.num_nodes:,} nodes, 6 operator calls (A21, A22, A23, "
+                f"A2T1, A2T2, A2T3) as main_CAGR.py makes them; {threads} OpenMP threads")
+        return ms, desc
+
+
+def cpu_reference_step_ms(impl, tree, p, widths, mu, wvals):
+    from oracle.oracle import point_weights
+    q, wq = p, widths
     t_scatter = t_trav = 0.0
     for op, vals in (("A21", mu), ("A22", mu), ("A23", mu), ("A2T1", wvals[:, 0:1]),
                      ("A2T2", wvals[:, 1:2]), ("A2T3", wvals[:, 2:3])):
@@ -177,12 +191,7 @@ def cpu_reference_step_ms(p, widths, mu, wvals, sample: int, threads: int):
         t2 = time.perf_counter()
         t_scatter += t1 - t0
         t_trav += t2 - t1
-    ms = (t_scatter + t_trav * (n / len(sel))) * 1e3
-    desc = (f"{len(sel):,} of {n:,} queries per operator (traversal time scaled by "
-            f"{n / len(sel):.1f}); node moments over all {tree.num_nodes:,} nodes; 6 operator "
-            f"calls (A21, A22, A23, A2T1, A2T2, A2T3) as main_CAGR.py makes them; "
-            f"{threads} OpenMP threads")
-    return ms, kind, desc
+    return (t_scatter + t_trav) * 1e3
 
 
 def max_over_ranks(values, world: int, device):
@@ -206,11 +215,12 @@ def run_reference_arm(args, rank: int):
     p, widths, mu = make_workload(args.workload, args.n)
     rng = np.random.default_rng(5)
     wvals = rng.normal(size=(args.n, 3)).astype(np.float32) * 1e-3
-    sample = args.cpu_sample or 100_000
+    cpu = CpuReference(p)
+    kind = cpu.kind
     times = []
-    kind = desc = None
+    desc = None
     for i in range(args.warmup + args.steps):
-        ms, kind, desc = cpu_reference_step_ms(p, widths, mu, wvals, sample, threads)
+        ms, desc = cpu.step_ms(p, widths, mu, wvals, threads)
         if i >= args.warmup:
             times.append(ms)
     v = float(np.mean(times))
@@ -392,37 +402,52 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     # end to end: the whole CAGR normal solve on this cloud (tree build + 40
     # iterations + 8 G steps, main_CAGR.py's schedule, preset l0)
-    solve = None
+    solve = solve64 = None
     if not args.no_solve:
         from cagr_b200.mesh import reconstruct
         from cagr_b200.solver import PRESET_WIDTHS, cagr_solve
 
-        def pipeline():
+        def pipeline(pts):
             torch.cuda.synchronize(dev)
             t0 = time.perf_counter()
-            res = cagr_solve(P, *PRESET_WIDTHS["l0"])
+            res = cagr_solve(pts, *PRESET_WIDTHS["l0"])
             torch.cuda.synchronize(dev)
             t1 = time.perf_counter()
-            rec = reconstruct(P, res.normals, grid=args.grid)
+            rec = reconstruct(pts, res.normals, grid=args.grid)
             torch.cuda.synchronize(dev)
             return res, rec, t1 - t0, time.perf_counter() - t1
+
+        def record(res, rec, t_solve, t_rec, first):
+            return {"total_s": round(t_solve + t_rec, 4), "solve_s": round(t_solve, 4),
+                    "tree_build_s": round(res.time_tree_s, 4),
+                    "iterations_s": round(res.time_main_s, 4),
+                    "operator_calls": res.operator_calls, "preset": "l0",
+                    "reconstruct_s": round(t_rec, 4), "grid": args.grid,
+                    "field_s": round(rec.seconds["field"], 4),
+                    "marching_cubes_s": round(rec.seconds["marching_cubes"], 4),
+                    "vertices": int(rec.vertices.shape[0]), "faces": int(rec.faces.shape[0]),
+                    "first_call_total_s": round(first, 4)}
 
         # the first run pays one-off costs (module loading of the kernels and torch
         # ops it touches, growth of the memory pools to this size): reported apart,
         # the second run is the number
-        _, rec, c_solve, c_rec = pipeline()
+        _, rec, c_solve, c_rec = pipeline(P)
         del rec
-        res, rec, t_solve, t_rec = pipeline()
-        solve = {"total_s": round(t_solve + t_rec, 4), "solve_s": round(t_solve, 4),
-                 "tree_build_s": round(res.time_tree_s, 4),
-                 "iterations_s": round(res.time_main_s, 4),
-                 "operator_calls": res.operator_calls, "preset": "l0",
-                 "reconstruct_s": round(t_rec, 4), "grid": args.grid,
-                 "field_s": round(rec.seconds["field"], 4),
-                 "marching_cubes_s": round(rec.seconds["marching_cubes"], 4),
-                 "vertices": int(rec.vertices.shape[0]), "faces": int(rec.faces.shape[0]),
-                 "first_call_total_s": round(c_solve + c_rec, 4)}
+        res, rec, t_solve, t_rec = pipeline(P)
+        solve = record(res, rec, t_solve, t_rec, c_solve + c_rec)
         del rec
+        if not args.no_fp64:
+            # the same pipeline in float64 throughout (points, widths, moments, pair
+            # sums, Krylov scalars, field; marching cubes on the field rounded to
+            # float32): the FP64 form the mixed-precision pipeline is compared with
+            P64 = P.double()
+            _, rec, c_solve, c_rec = pipeline(P64)
+            del rec
+            res, rec, t_solve, t_rec = pipeline(P64)
+            solve64 = record(res, rec, t_solve, t_rec, c_solve + c_rec)
+            solve64["form"] = ("float64 throughout; 1/sqrt as rsqrt.approx.f64 refined by one "
+                               "third-order step (within 2 ulp of CUDA's rsqrt(double))")
+            del rec
 
     # measured FP32 FMA peak (roofline denominator)
     gf = ctypes.c_double()
@@ -450,13 +475,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if not args.no_cpu_baseline:
         import multiprocessing
         threads = multiprocessing.cpu_count()
-        rng = np.random.default_rng(5)
         wv_host = WV.cpu().numpy()
-        ms, kind, desc = cpu_reference_step_ms(p, widths, mu, wv_host,
-                                               args.cpu_sample or 200_000, threads)
-        cpu = {"value": round(ms, 3), "unit": UNIT, "cores": threads, "kind": kind,
+        ref_cpu = CpuReference(p)
+        ms, desc = ref_cpu.step_ms(p, widths, mu, wv_host, threads)
+        cpu = {"value": round(ms, 3), "unit": UNIT, "cores": threads, "kind": ref_cpu.kind,
                "sample": desc}
-        del rng
     bi = (MU.numel() + WV.numel()) * 4
     bo = (out_a.numel() + out_t.numel()) * 4
     line = {
@@ -470,7 +493,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "roofline": {"bound": "fp32", "kernel": dom, "achieved": round(achieved, 3),
                      "peak": round(peak_tflops, 3), "unit": "TFLOP/s",
                      "frac": round(achieved / peak_tflops, 4), "traffic": traffic,
-                     "traffic_unit": "bytes per launch (ncu capture)",
+                     "traffic_unit": "bytes per launch",
+                     "traffic_source": TRAFFIC_SOURCE if traffic is not None else None,
                      "peak_source": "measured FP32 FMA probe (cagr_probe_fp32_peak)",
                      "pair_terms_per_launch": round(terms_dom), "flops_per_term": fpt},
         "kernels_ms": {"moments_per_step": round(float(np.mean(mom_ms)), 4),
@@ -480,6 +504,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                        "A2T2": round(terms_t[1]), "A2T3": round(terms_t[2])},
         "fp64_ms_per_step": None if fp64_ms is None else round(fp64_ms, 3),
         "end_to_end": solve,
+        "end_to_end_fp64": solve64,
+        "end_to_end_fp64_over_fp32": (round(solve64["total_s"] / solve["total_s"], 3)
+                                      if solve and solve64 else None),
         "clocks": clk,
     }
     if cpu is not None:

@@ -95,3 +95,56 @@ def solve(points: np.ndarray, wsmin: float, wsmax: float, impl=None, iters: int 
 def sign_agreement(mu_a: np.ndarray, mu_b: np.ndarray) -> float:
     """Fraction of points whose two normals point the same way (dot > 0)."""
     return float(((mu_a * mu_b).sum(1) > 0).mean())
+
+
+def solve_torch(points, wsmin: float, wsmax: float, fwd, iters: int = 40, n_sd: int = 30,
+                lambda0: float = 0.0, wnnc_steps: int = 8):
+    """The reference solve in torch float32 on the points' device, line for
+    line as main_CAGR.py:93-174 writes it (its sums, its step lengths, its
+    float32 arithmetic), with every operator call made through
+    ``fwd(op, values, widths) -> tensor`` -- one ``forward_*`` call of the
+    reference (wn_treecode_func.py:122-158), e.g. ``RefGPU.forward`` for the
+    reference's own CUDA kernels.  widths = ones (main_CAGR.py:61)."""
+    import torch
+    import torch.nn.functional as F
+    n = points.shape[0]
+    dev = points.device
+    normals = torch.zeros(n, 3, device=dev)
+    b = torch.ones(n, 1, device=dev) * 0.5
+    widths = torch.ones(n, device=dev)
+
+    def A2T(v1, v2, v3, w):
+        return fwd("A2T1", v1, w) + fwd("A2T2", v2, w) + fwd("A2T3", v3, w)
+
+    width_scale = wsmin + 0.5 * (wsmax - wsmin)
+    rk1 = A2T(b, b, b, widths * width_scale)
+    pk = rk1
+    for i in range(iters):
+        width_scale = wsmin + ((iters - 1 - i) / (iters - 1)) * (wsmax - wsmin)
+        w = widths * width_scale
+        if i <= n_sd:
+            A1, A2_, A3_ = (-fwd(op, normals, w) for op in ("A21", "A22", "A23"))
+            AT_A_mu = A2T(A1, A2_, A3_, w)
+            r = A2T(b, b, b, w) - AT_A_mu - lambda0 * normals
+            A_r = -(fwd("A21", r, w) + fwd("A22", r, w) + fwd("A23", r, w))
+            alpha = (r * r).sum() / (A_r * A_r).sum()
+            normals = normals + alpha * r
+            if i == n_sd:
+                A1, A2_, A3_ = (-fwd(op, normals, w) for op in ("A21", "A22", "A23"))
+                AT_A_mu = A2T(A1, A2_, A3_, w)
+                rk1 = A2T(b, b, b, w) - AT_A_mu - lambda0 * normals
+                pk = rk1
+        else:
+            P1, P2, P3 = (-fwd(op, pk, w) for op in ("A21", "A22", "A23"))
+            T1, T2, T3 = fwd("A2T1", P1, w), fwd("A2T2", P2, w), fwd("A2T3", P3, w)
+            alpha = (rk1 * rk1).sum() / (((T3 * pk) + (T2 * pk) + (T1 * pk)).sum()
+                                         + lambda0 * (pk * pk).sum())
+            normals = normals + alpha * pk
+            rk20 = rk1 - alpha * T1 - alpha * T2 - alpha * T3 - alpha * lambda0 * pk
+            beta = (rk20 * rk20).sum() / (rk1 * rk1).sum()
+            pk = rk20 + beta * pk
+            rk1 = rk20
+    for _ in range(wnnc_steps):
+        g = F.normalize(fwd("G", normals, w), dim=-1).contiguous()
+        normals = g * torch.linalg.norm(normals, dim=-1, keepdim=True)
+    return normals

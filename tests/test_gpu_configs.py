@@ -4,17 +4,17 @@
   1.5 x the mean 10-NN distance: tree bit-exact and operators within the FP32
   tolerance against the reference's own kernels compiled for the host; the
   full solve (repo-default 40 iterations + 8 G steps) agrees in normal sign
-  with the same solve on the host reference; the 128^3 reconstruction is a
-  closed outward sphere.
+  with the same solve on the host reference, at those widths and at 1/4 of
+  them; the 128^3 reconstruction is a closed outward sphere.
 * 100,000 points on a torus, leaf 32: the FP32 treecode field at 20,000
   random queries in [-1.5, 1.5]^3 equals the reference algorithm in FP32
   (same decisions) within FP32 rounding, and its error against the FP64 direct
   sum is the reference algorithm's own (the theta = 1/2 monopole rule, as its
   FP64 treecode shows); the 256^3 field runs.
 * 4,000,000 points on a level set of 32 Gaussian blobs: the full pipeline
-  (solve, 512^3 field, marching cubes) in FP32, and the 512^3 field against
-  its FP64 form: RMS error below 1e-5 and at most 1e-4 of the nodes off by
-  more than 1e-4 (pairs exactly on the kernel's steps, see the test).
+  (solve, 512^3 field, marching cubes) in FP32, and the 512^3 field at 20,000
+  seeded grid nodes against the reference's kernels built for the host with
+  the same normals (and against the FP64 form of the field).
 """
 import numpy as np
 import pytest
@@ -65,10 +65,18 @@ def test_sphere_5k_leaf16_depth8_against_the_reference(cuda_lib):
                for k, op in enumerate(("A2T1", "A2T2", "A2T3")))
     l2, mx = rel_errors(out, want)
     assert l2 <= 2e-5 and mx <= 2e-4, (l2, mx)
-    # the solve on the per-point widths scaled by 1/4 (measured on this cloud:
-    # scale 1, pairs within ~10 neighbours dropped by the discontinuous kernel,
-    # orients 66 % outward -- on the GPU and in the host reference alike --;
-    # scale 1/4 orients 100 %)
+    # the solve at the configuration's widths as written (scale 1: 1.5 x mean
+    # 10-NN).  The reference algorithm itself orients this cloud only partly
+    # there (pairs within ~10 neighbours are dropped by the discontinuous
+    # kernel), so the check is agreement with the host reference's own solve
+    res1 = cagr_solve(P, 1.0, 1.0, widths=W, tree=wn)
+    host1 = host_solve(p, 1.0, 1.0, impl=ref, base_widths=w, max_depth=8, leaf_size=16)
+    mu1 = res1.normals.cpu().numpy()
+    agree1 = sign_agreement(mu1, host1)
+    print(f"sphere 5k at 1.5 x mean 10-NN: agreement with the host reference {agree1:.4f}, "
+          f"outward: ours {sign_agreement(mu1, p):.4f}, reference {sign_agreement(host1, p):.4f}")
+    assert agree1 >= 0.995, agree1
+    # and at the widths scaled by 1/4, where the algorithm orients it fully
     res = cagr_solve(P, 0.25, 0.25, widths=W, tree=wn)
     host = host_solve(p, 0.25, 0.25, impl=ref, base_widths=w, max_depth=8, leaf_size=16)
     mu_gpu = res.normals.cpu().numpy()
@@ -140,19 +148,30 @@ def test_blobs_4m_pipeline_and_fp32_field_against_fp64(cuda_lib):
     assert torch.isfinite(res.normals).all()
     rec = reconstruct(P, res.normals, grid=512, tree=wn)
     assert rec.faces.shape[0] > 100_000
-    # the 512^3 field, FP32 (the mixed-precision pipeline) against the FP64 form.
-    # Measured: RMS 1.5e-6, 99.99th percentile 7e-6, 7e-6 of the nodes above 1e-4
-    # (max 4.4e-3).  Those few are pairs lying on the kernel's steps -- the
-    # width test r >= w (whose two branches differ: exp(d_k/2) vs exp(w)) and
-    # the acceptance test -- decided differently in FP32 and FP64; FP64 running
-    # sums in the FP32 kernel leave them unchanged (measured), so they are not
-    # summation error.
-    f32 = rec.field.float()
+    # the 512^3 field at 20,000 seeded grid nodes against the reference's own
+    # kernels (host build) with the same normals: grid node (i, j, k) at
+    # origin + (i, j, k) * spacing rounded once to float32, as the GPU forms it
+    from oracle.oracle import RefOracle
+    ref = RefOracle()
+    mu = res.normals.cpu().numpy()
+    G = 512
+    h, o = np.float32(2.4 / 511), np.float32(-1.2)
+    idx = np.random.default_rng(90).integers(0, G, size=(20000, 3))
+    q = (idx.astype(np.float64) * np.float64(h) + np.float64(o)).astype(np.float32)
+    tr = ref.build_tree(p)
+    want = -ref.forward("A3", tr, p, mu, np.full(len(q), 0.01, np.float32), queries=q,
+                        continuous=True)[:, 0]
+    got = rec.field.cpu().numpy()[idx[:, 2], idx[:, 1], idx[:, 0]]
+    l2, _ = rel_errors(got, want)
+    # pairs lying exactly on the kernel's steps (the width test r >= w, whose
+    # branches differ, and the acceptance test) may be decided differently by
+    # two float32 builds with different libm rounding: a few nodes at most
+    frac = float((np.abs(got - want) > 1e-4).mean())
+    assert l2 <= 2e-5, l2
+    assert frac <= 1e-3, frac
+    # and the FP64 form of the same field (the plain FP64 pipeline) at the same nodes
     wn64 = WindingNumberTreecode(P.double())
     wn64.scatter(res.normals.double())
-    f64 = field_grid(wn64, (512, 512, 512), (-1.2, -1.2, -1.2), 2.4 / 511, 0.01).neg_()
-    diff = (f32.double() - f64).abs()
-    rms = diff.pow(2).mean().sqrt().item()
-    frac = (diff > 1e-4).double().mean().item()
-    assert rms <= 1e-5, rms
-    assert frac <= 1e-4, frac
+    f64 = field_grid(wn64, (G, G, G), (-1.2, -1.2, -1.2), 2.4 / 511, 0.01).neg_()
+    got64 = f64.cpu().numpy()[idx[:, 2], idx[:, 1], idx[:, 0]]
+    assert float((np.abs(got - got64) > 1e-4).mean()) <= 1e-3
