@@ -23,6 +23,8 @@ CAGR_F32, CAGR_F64 = 0, 1
 OPS = {"A": 0, "AT": 1, "A3": 2, "A21": 3, "A22": 4, "A23": 5, "A2T1": 6, "A2T2": 7,
        "A2T3": 8, "G": 9, "A2_FUSED": 10, "A2T_SUM": 11, "COUNT": 12, "A2T_SUM_SHARED": 13,
        "A2_INSIDE": 14, "A2T_RHS": 15}
+# far-field modes
+FAR_REFERENCE, FAR_INTERP = 0, 1
 # multiply flags
 FLAG_CONTINUOUS = 1
 FLAG_ACCUMULATE = 2
@@ -68,6 +70,11 @@ _SIGNATURES = {
     "cagr_debug_fail_allocations_after": (_i32, [_i64]),
     "cagr_multiply_rhs_window": (_i32, [_p, _p, ctypes.c_double, _p, _i32, _p, _p]),
     "cagr_b_window_table": (_i32, [_p, _p, _p, _i32, _p, _p]),
+    "cagr_tree_set_far_field": (_i32, [_p, _i32, _i32, ctypes.c_double, _i32, _p]),
+    "cagr_tree_far_field": (_i32, [_p, ctypes.POINTER(_i32), ctypes.POINTER(_i32),
+                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i32), _pi64]),
+    "cagr_tree_query_groups": (_i32, [_p, _p, _p]),
+    "cagr_debug_interp_wait_limit": (_i32, [_p, _i64]),
 }
 
 _lib = None

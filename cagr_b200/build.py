@@ -18,7 +18,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libcagr_b200.so")
 SOURCES = ["capi.cu", "tree_build.cu", "moments.cu", "traverse.cu", "diagnostics.cu",
-           "noalloc.cu", "mcubes.cu", "memory.cu"]
+           "noalloc.cu", "mcubes.cu", "memory.cu", "interp.cu"]
 HEADERS = ["common.cuh", "internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

@@ -32,6 +32,15 @@ int check_tree(const cagr_tree* h) {
     return CAGR_OK;
 }
 
+// Entry points that exist in the reference far-field mode only.
+int reference_mode_only(const cagr_tree* h, const char* what) {
+    if (h->t->interp)
+        return set_error(CAGR_ERR_STATE, std::string(what) +
+                                             " needs the reference far-field mode "
+                                             "(cagr_tree_set_far_field(tree, CAGR_FAR_REFERENCE, ...))");
+    return CAGR_OK;
+}
+
 int op_attr_dim(int op) {
     switch (op) {
         case CAGR_OP_AT:
@@ -124,17 +133,23 @@ int cagr_tree_morton_order(const cagr_tree* tree, int32_t* perm_dev, void* strea
 int cagr_scatter(cagr_tree* tree, int slot, const void* attrs_dev, int attr_dim,
                  const void* weights_dev, void* stream) {
     if (int rc = check_tree(tree)) return rc;
+    if (tree->t->interp) {
+        if (slot < 0 || slot > 2) return set_error(CAGR_ERR_INVALID, "slot must be 0..2");
+        return cagr::interp_scatter(tree->t, slot, attrs_dev, attr_dim, as_stream(stream));
+    }
     return cagr::moments(tree->t, slot, attrs_dev, attr_dim, weights_dev, as_stream(stream));
 }
 
 int cagr_scatter3(cagr_tree* tree, const void* values3_dev, void* stream) {
     if (int rc = check_tree(tree)) return rc;
+    if (tree->t->interp) return cagr::interp_scatter(tree->t, 3, values3_dev, 3, as_stream(stream));
     return cagr::moments3(tree->t, values3_dev, as_stream(stream));
 }
 
 int cagr_scatter_export(const cagr_tree* tree, int slot, void* node_attrs_dev,
                         void* reppoints_dev, void* node_weights_dev, void* stream) {
     if (int rc = check_tree(tree)) return rc;
+    if (int rc = reference_mode_only(tree, "cagr_scatter_export")) return rc;
     return cagr::moments_export(tree->t, slot, node_attrs_dev, reppoints_dev, node_weights_dev,
                                 as_stream(stream));
 }
@@ -163,12 +178,14 @@ int cagr_multiply(const cagr_tree* tree, int op, const void* queries_dev,
     a.width = width;
     a.out = out_dev;
     a.out_stride = (int)out_stride;
+    if (tree->t->interp) return cagr::interp_traverse(tree->t, a, as_stream(stream));
     return cagr::traverse(tree->t, a, as_stream(stream));
 }
 
 int cagr_multiply_rhs_window(const cagr_tree* tree, const void* widths_dev, double width,
                              const void* widths_hi_dev, int flags, void* out_dev, void* stream) {
     if (int rc = check_tree(tree)) return rc;
+    if (int rc = reference_mode_only(tree, "cagr_multiply_rhs_window")) return rc;
     if (flags & ~CAGR_FLAG_ACCUMULATE) return set_error(CAGR_ERR_INVALID, "unknown flag bits");
     if (!widths_hi_dev) return set_error(CAGR_ERR_INVALID, "widths_hi must be a device buffer");
     cagr::TraverseArgs a;
@@ -185,6 +202,7 @@ int cagr_multiply_rhs_window(const cagr_tree* tree, const void* widths_dev, doub
 int cagr_b_window_table(const cagr_tree* tree, const void* base_dev, const void* scales_dev,
                         int num_scales, void* out_dev, void* stream) {
     if (int rc = check_tree(tree)) return rc;
+    if (int rc = reference_mode_only(tree, "cagr_b_window_table")) return rc;
     return cagr::b_window_table(tree->t, base_dev, scales_dev, num_scales, out_dev,
                                 as_stream(stream));
 }
@@ -192,6 +210,7 @@ int cagr_b_window_table(const cagr_tree* tree, const void* base_dev, const void*
 int cagr_adjoint(cagr_tree* tree, int op, const void* widths_dev, double width, int flags,
                  const void* grad_out_dev, void* grad_attrs_dev, void* stream) {
     if (int rc = check_tree(tree)) return rc;
+    if (int rc = reference_mode_only(tree, "cagr_adjoint")) return rc;
     if (op != CAGR_OP_A2_FUSED)
         return set_error(CAGR_ERR_INVALID, "the adjoint is implemented for CAGR_OP_A2_FUSED");
     if (flags & ~CAGR_FLAG_CONTINUOUS) return set_error(CAGR_ERR_INVALID, "unknown flag bits");
@@ -228,6 +247,7 @@ int cagr_field_grid(const cagr_tree* tree, int op, int nx, int ny, int nz,
     a.widths = widths_dev;
     a.width = width;
     a.out = out_dev;
+    if (tree->t->interp) return cagr::interp_traverse(tree->t, a, as_stream(stream));
     return cagr::traverse(tree->t, a, as_stream(stream));
 }
 
@@ -249,12 +269,46 @@ int cagr_forward(cagr_tree* tree, int op, const void* values_dev, const void* wi
     const int dim = op_attr_dim(op);
     if (dim <= 0) return set_error(CAGR_ERR_INVALID, "unknown operator for cagr_forward");
     if (op == CAGR_OP_A2T_SUM) {
-        if (int rc = cagr::moments3(tree->t, values_dev, as_stream(stream))) return rc;
-    } else if (int rc = cagr::moments(tree->t, 0, values_dev, dim, nullptr, as_stream(stream))) {
+        if (int rc = cagr_scatter3(tree, values_dev, stream)) return rc;
+    } else if (int rc = cagr_scatter(tree, 0, values_dev, dim, nullptr, stream)) {
         return rc;
     }
     return cagr_multiply(tree, op, nullptr, nullptr, 0, widths_dev, width, flags, out_dev, 0,
                          stream);
+}
+
+int cagr_tree_set_far_field(cagr_tree* tree, int mode, int degree, double theta, int direct_max,
+                            void* stream) {
+    if (int rc = check_tree(tree)) return rc;
+    if (mode == CAGR_FAR_REFERENCE) {
+        if (tree->t->interp) {
+            if (cudaStreamSynchronize(as_stream(stream)) != cudaSuccess)
+                return set_error(CAGR_ERR_CUDA, "stream synchronisation failed");
+            cagr::interp_free(tree->t);
+        }
+        return CAGR_OK;
+    }
+    if (mode != CAGR_FAR_INTERP) return set_error(CAGR_ERR_INVALID, "unknown far-field mode");
+    return cagr::interp_setup(tree->t, degree, theta, direct_max, as_stream(stream));
+}
+
+int cagr_tree_far_field(const cagr_tree* tree, int* mode, int* degree, double* theta,
+                        int* direct_max, int64_t* num_interp_nodes) {
+    if (int rc = check_tree(tree)) return rc;
+    if (mode) *mode = tree->t->interp ? CAGR_FAR_INTERP : CAGR_FAR_REFERENCE;
+    cagr::interp_info(tree->t, degree, theta, direct_max, num_interp_nodes);
+    return cagr::interp_status(tree->t);
+}
+
+int cagr_debug_interp_wait_limit(cagr_tree* tree, int64_t spin) {
+    if (int rc = check_tree(tree)) return rc;
+    return cagr::interp_set_wait_limit(tree->t, spin);
+}
+
+int cagr_tree_query_groups(const cagr_tree* tree, int32_t* order_dev, void* stream) {
+    if (int rc = check_tree(tree)) return rc;
+    if (!order_dev) return set_error(CAGR_ERR_INVALID, "order_dev is null");
+    return cagr::query_groups(tree->t, order_dev, as_stream(stream));
 }
 
 }  // extern "C"

@@ -28,6 +28,8 @@ int set_error(int code, const std::string& msg);
 int pool_alloc(void** p, size_t bytes, cudaStream_t s);
 void pool_free(void* p, cudaStream_t s);
 
+struct Interp;  // interpolated far field (interp.cu), null in the reference mode
+
 // Device arrays owned by one tree.  All pointers are device pointers.
 struct Tree {
     int dtype = 0;  // 0 = float32, 1 = float64
@@ -64,6 +66,10 @@ struct Tree {
     void* adj_sums = nullptr;
     bool adj_valid = false;
     bool slot_adj[3] = {false, false, false};  // slot k's latest moments are the adjoint's
+    // Far-field mode: null = the reference's monopole at the weighted centroid
+    // with per-query acceptance (bit-exact decisions); else the interpolated
+    // far field (Chebyshev proxy grids per node, one acceptance test per warp).
+    Interp* interp = nullptr;
 };
 
 int tree_build(const void* points, int64_t n, int dtype, int max_depth, int leaf_size,
@@ -139,6 +145,26 @@ int b_window_table(const Tree* t, const void* base, const void* scales, int S, v
 // original point order.
 int adjoint(const Tree* t, const TraverseArgs& a, const void* grad, void* grad_attrs,
             cudaStream_t stream);
+
+// Interpolated far field (interp.cu).  interp_setup switches the tree to it
+// (degree 1..8 of the Chebyshev grid per axis, acceptance parameter theta,
+// nodes of at most direct_max points summed directly when near); interp_free
+// returns it to the reference mode.  interp_scatter fills slot 0..2 (cagr_scatter)
+// or 3 (cagr_scatter3's three scalar columns) with point and proxy records;
+// interp_traverse evaluates an operator with them.
+int interp_setup(Tree* t, int degree, double theta, int direct_max, cudaStream_t stream);
+void interp_free(Tree* t);
+int interp_scatter(Tree* t, int slot, const void* attrs, int dim, cudaStream_t stream);
+int interp_traverse(const Tree* t, const TraverseArgs& a, cudaStream_t stream);
+int interp_info(const Tree* t, int* degree, double* theta, int* direct_max, int64_t* num_interp);
+// Reads the walks' error flag (synchronises the device): kErrCuda if a walk
+// abandoned a staging wait since the mode was set up.
+int interp_status(const Tree* t);
+// Test hook: try_wait rounds before a staging wait is abandoned.
+int interp_set_wait_limit(Tree* t, int64_t spin);
+// The original index of the i-th self-query in processing order (consecutive
+// groups of 32 walk together): perm[qgroup[i]].
+int query_groups(const Tree* t, int32_t* order, cudaStream_t stream);
 
 // Marching cubes (mcubes.cu).  The case table: tri[256][36] edge ids (12
 // triangles at most) and ntri[256].

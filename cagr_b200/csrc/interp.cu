@@ -1,0 +1,1201 @@
+// Interpolated far field: the second evaluation mode of the treecode.
+//
+// The reference (mayueji/CAGR CUDA-based/ext/wn_treecode/wn_treecode_cuda/
+// wn_treecode_cuda_kernels.cu:556-1322) approximates an accepted node by ONE
+// term at its |attr|-weighted centroid, accepted per query when
+// |x - c|^2 > (4 half_w)^2 (:595).  That is first order in the node size: on
+// the 100k-point torus workload its field is off the FP64 direct sum by up to
+// 0.4 (field values in [-17, 2.5]).  This mode evaluates the same operators --
+// the exact pair sums the reference approximates -- with a far field whose
+// error falls geometrically with its degree p:
+//
+//  * Far field: barycentric Lagrange interpolation of the pair kernel in the
+//    source position on a (p+1)^3 grid of Chebyshev points of the second kind
+//    spanning the node's tight bounding box (the barycentric Lagrange
+//    treecode of L. Wang, R. Krasny and S. Tlupova, Commun. Comput. Phys. 28
+//    (2020) 1415-1436).  A node's proxy charges are q_m = sum_j L_m(y_j) a_j
+//    over its points; a query's interaction with the node is the same pair
+//    kernel summed over the proxy points.  The convection factor exp(-y_k/2)
+//    is smooth in y and is interpolated with the rest of the kernel, so a
+//    proxy record is exactly a point record (position, exp(-position/2),
+//    charges) and far and near sources run the same inner loop.
+//  * Acceptance: ONE test per warp.  The warp's 32 queries (consecutive along
+//    the Hilbert / Morton curve) form a batch with bounding centre b and
+//    radius r_B; a node with box centre c and radius r_C is far when
+//    r_C + theta r_B < theta |b - c| -- then r_C < theta |x - c| for every
+//    query x of the batch, the interpolation's accuracy condition -- and no
+//    pair can lie within a query's width (|b - c| - r_B - r_C >= the batch's
+//    largest width), so only the smooth outside-width branch of the kernel is
+//    interpolated.  Far nodes with fewer
+//    than (p+1)^3 points are summed directly (exact, and fewer terms); near
+//    nodes with at most direct_max points, and near leaves, are summed
+//    directly with the per-pair width test of the reference kernels.  Every
+//    decision is warp-uniform: no per-lane bookkeeping, and each source
+//    record is loaded once per warp (one broadcast) and used by all 32 lanes.
+//  * Precision: FP32 terms, plain sums within one interaction (one proxy grid
+//    or one node's points), compensated (Kahan) accumulation of the
+//    interactions per query; FP64 with the double build.
+//  * Proxy charges: one block per chunk of <= kChunk points of an
+//    interpolation node (a node with >= (p+1)^3 points), writing chunk
+//    partials that a second kernel sums in chunk order (in double), so the
+//    charges are the same bits on every run.
+//
+// Operators: A, AT, A3, A21..A23, A2T1..A2T3, G, A2_FUSED, A2T_SUM (the three
+// scalar columns of cagr_scatter3 in one walk: the proxy grid is geometric, so
+// the three directions share it), A2T_SUM_SHARED, COUNT.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+
+#include "internal.h"
+
+namespace cagr {
+
+constexpr int kPMax = 9;          // degree <= 8
+constexpr int kChunk = 2048;      // points per proxy-charge block
+constexpr int kRec = 12;          // scalars per point / proxy record
+constexpr unsigned kAll = 0xffffffffu;
+// internal operator codes beside Op: the A2T sums of the interpolated mode
+constexpr int kIOpA2TSum = 100;     // sum_k A2Tk(s_k), three scalar columns (slot 3)
+constexpr int kIOpA2TShared = 101;  // sum_k A2Tk(s), one scalar column
+
+struct Interp {
+    int degree = 5, P = 6, P3 = 216;
+    double theta = 0.5;
+    int direct_max = 64;
+    int64_t num_interp = 0, num_chunks = 0;
+    void* box_c = nullptr;         // [M*4] T: bounding-box centre, radius
+    void* box_h = nullptr;         // [M*4] T: half extents, 0
+    int32_t* iidx = nullptr;       // [M] proxy block of the node, -1 if it has < P3 points
+    int4* chunks = nullptr;        // [num_chunks] {node, first sorted point, count, proxy block}
+    int32_t* chunk_first = nullptr;  // [num_interp + 1]
+    void* part = nullptr;          // [num_chunks * P3 * 4] T: chunk partial charges
+    void* pts[4] = {nullptr, nullptr, nullptr, nullptr};   // [N*12] T point records per slot
+    void* prox[4] = {nullptr, nullptr, nullptr, nullptr};  // [num_interp*P3*12] T proxy records
+    int dim[4] = {0, 0, 0, 0};     // attribute dim held by the slot (0 = empty)
+    double cheb[kPMax] = {}, omega[kPMax] = {};  // Chebyshev points and barycentric weights
+    int* err = nullptr;            // device flag: a walk's staging wait ran out
+    uint32_t spin = 1u << 22;      // try_wait rounds before a staging wait runs out
+};
+
+namespace {
+
+// ---- tree geometry ----------------------------------------------------------
+
+template <typename T>
+__device__ __forceinline__ T warp_min(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(kAll, v, o));
+    return v;
+}
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kAll, v, o));
+    return v;
+}
+
+// One warp per node: the tight bounding box of its points (a contiguous range
+// of the Morton order).  Half extents are floored at 1e-3 of the largest (a
+// flat node still spans a proper interpolation box); the radius is rounded up.
+template <typename T>
+__global__ void k_box(const int4* __restrict__ meta, const T* __restrict__ spos, int64_t M,
+                      T* __restrict__ bc, T* __restrict__ bh) {
+    const int64_t node = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (node >= M) return;  // uniform per warp
+    const int4 mt = meta[node];
+    const int np = node_npts(mt);
+    T lo[3] = {T(INFINITY), T(INFINITY), T(INFINITY)};
+    T hi[3] = {-T(INFINITY), -T(INFINITY), -T(INFINITY)};
+    for (int j = lane; j < np; j += 32) {
+        const T* y = spos + 3 * ((int64_t)mt.y + j);
+        for (int a = 0; a < 3; a++) {
+            lo[a] = fmin(lo[a], y[a]);
+            hi[a] = fmax(hi[a], y[a]);
+        }
+    }
+    for (int a = 0; a < 3; a++) {
+        lo[a] = warp_min(lo[a]);
+        hi[a] = warp_max(hi[a]);
+    }
+    if (lane == 0) {
+        T c[3], h[3], hmax = T(0);
+        for (int a = 0; a < 3; a++) {
+            if (!(lo[a] <= hi[a])) lo[a] = hi[a] = T(0);  // no finite coordinate
+            c[a] = T(0.5) * (lo[a] + hi[a]);
+            // the box must hold every point: half extent from the farther end
+            h[a] = fmax(hi[a] - c[a], c[a] - lo[a]);
+            hmax = fmax(hmax, h[a]);
+        }
+        const T floor_h = fmax(hmax * T(1e-3), T(1e-30));
+        for (int a = 0; a < 3; a++) h[a] = fmax(h[a], floor_h);
+        const T r = sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]) * T(1.0 + 1.0 / 65536);
+        st4<T>(bc + 4 * node, make4(c[0], c[1], c[2], r));
+        st4<T>(bh + 4 * node, make4(h[0], h[1], h[2], T(0)));
+    }
+}
+
+__global__ void k_iflags(const int4* __restrict__ meta, int64_t M, int P3,
+                         int32_t* __restrict__ flag, int32_t* __restrict__ nch) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    const int np = node_npts(meta[i]);
+    const bool f = np >= P3;
+    flag[i] = f ? 1 : 0;
+    nch[i] = f ? (np + kChunk - 1) / kChunk : 0;
+}
+
+// iidx = proxy block (exclusive scan of the flags) or -1; chunk descriptors
+__global__ void k_ichunks(const int4* __restrict__ meta, int64_t M, const int32_t* __restrict__ flag,
+                          const int32_t* __restrict__ pos, const int32_t* __restrict__ chbase,
+                          int32_t* __restrict__ iidx, int4* __restrict__ chunks,
+                          int32_t* __restrict__ chunk_first) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    if (!flag[i]) {
+        iidx[i] = -1;
+        return;
+    }
+    const int ii = pos[i];
+    iidx[i] = ii;
+    const int4 mt = meta[i];
+    const int np = node_npts(mt);
+    const int cb = chbase[i];
+    chunk_first[ii] = cb;
+    for (int c = 0; c * kChunk < np; c++)
+        chunks[cb + c] = make_int4((int)i, mt.y + c * kChunk, min(kChunk, np - c * kChunk), ii);
+}
+
+// ---- records and proxy charges ------------------------------------------------
+
+// Point records in Morton order: (y, c0) (exp(-y/2), c1) (c2, 0, 0, 0), the
+// charges being the point's attribute (dim 3: mu; dim 1: s, 0, 0; the three
+// scalar columns of cagr_scatter3: s_0, s_1, s_2).
+template <typename T>
+__global__ void k_ipoints(const T* __restrict__ spos, const int32_t* __restrict__ perm, int64_t n,
+                          const T* __restrict__ attrs, int dim, T* __restrict__ out) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int64_t j = perm[s];
+    const T y0 = spos[3 * s], y1 = spos[3 * s + 1], y2 = spos[3 * s + 2];
+    const T a0 = attrs[j * dim];
+    const T a1 = dim == 3 ? attrs[j * 3 + 1] : T(0);
+    const T a2 = dim == 3 ? attrs[j * 3 + 2] : T(0);
+    T* r = out + s * kRec;
+    st4<T>(r, make4(y0, y1, y2, a0));
+    st4<T>(r + 4, make4(exp_t(y0 * T(-0.5)), exp_t(y1 * T(-0.5)), exp_t(y2 * T(-0.5)), a1));
+    st4<T>(r + 8, make4(a2, T(0), T(0), T(0)));
+}
+
+template <typename T>
+struct ChargeParams {
+    const int4* chunks = nullptr;
+    const T* bc = nullptr;
+    const T* bh = nullptr;
+    const T* pts = nullptr;
+    T* part = nullptr;
+    int P = 0, P3 = 0;
+    T cheb[kPMax] = {};
+    T omega[kPMax] = {};
+};
+
+// Barycentric Lagrange basis at u (second form; an exact node hit gives the
+// unit vector, as the formula's limit).
+template <typename T>
+__device__ __forceinline__ void lagrange(T u, int P, const T* t, const T* om, T* L) {
+    int hit = -1;
+    for (int k = 0; k < P; k++)
+        if (u == t[k]) hit = k;
+    if (hit >= 0) {
+        for (int k = 0; k < P; k++) L[k] = k == hit ? T(1) : T(0);
+        return;
+    }
+    T sum = T(0);
+    for (int k = 0; k < P; k++) {
+        const T v = om[k] / (u - t[k]);
+        L[k] = v;
+        sum += v;
+    }
+    const T inv = T(1) / sum;
+    for (int k = 0; k < P; k++) L[k] *= inv;
+}
+
+constexpr int kTile = 64;
+constexpr int kChargeThreads = 256;
+constexpr int kMaxPer = (kPMax * kPMax * kPMax + kChargeThreads - 1) / kChargeThreads;
+
+// Partial proxy charges of one chunk: thread m accumulates
+// sum_j Lx_a(y_j) Ly_b(y_j) Lz_c(y_j) charges_j for its proxies m = (a, b, c).
+template <typename T>
+__global__ void __launch_bounds__(kChargeThreads) k_charges(const ChargeParams<T> p) {
+    __shared__ T sL[kTile][3][kPMax];
+    __shared__ T sQ[kTile][4];
+    const int4 cd = p.chunks[blockIdx.x];  // {node, first sorted point, count, proxy block}
+    const T* c = p.bc + 4 * (int64_t)cd.x;
+    const T* h = p.bh + 4 * (int64_t)cd.x;
+    const T cen[3] = {c[0], c[1], c[2]};
+    const T ih[3] = {T(1) / h[0], T(1) / h[1], T(1) / h[2]};
+    const int P = p.P, P3 = p.P3;
+    T acc[kMaxPer][3];
+    int ma[kMaxPer], mb[kMaxPer], mc[kMaxPer];
+#pragma unroll
+    for (int k = 0; k < kMaxPer; k++) {
+        const int m = threadIdx.x + k * kChargeThreads;
+        ma[k] = m / (P * P);
+        mb[k] = (m / P) % P;
+        mc[k] = m % P;
+        acc[k][0] = acc[k][1] = acc[k][2] = T(0);
+    }
+    for (int base = 0; base < cd.z; base += kTile) {
+        const int cnt = min(kTile, cd.z - base);
+        for (int t = threadIdx.x; t < cnt * 3; t += kChargeThreads) {
+            const int j = t / 3, a = t - 3 * j;
+            const T y = p.pts[((int64_t)cd.y + base + j) * kRec + a];
+            T u = (y - cen[a]) * ih[a];
+            u = fmin(fmax(u, T(-1)), T(1));
+            lagrange(u, P, p.cheb, p.omega, &sL[j][a][0]);
+        }
+        for (int j = threadIdx.x; j < cnt; j += kChargeThreads) {
+            const T* r = p.pts + ((int64_t)cd.y + base + j) * kRec;
+            sQ[j][0] = r[3];
+            sQ[j][1] = r[7];
+            sQ[j][2] = r[8];
+        }
+        __syncthreads();
+        for (int j = 0; j < cnt; j++) {
+            const T q0 = sQ[j][0], q1 = sQ[j][1], q2 = sQ[j][2];
+#pragma unroll
+            for (int k = 0; k < kMaxPer; k++) {
+                if (threadIdx.x + k * kChargeThreads < P3) {
+                    const T w = sL[j][0][ma[k]] * sL[j][1][mb[k]] * sL[j][2][mc[k]];
+                    acc[k][0] += w * q0;
+                    acc[k][1] += w * q1;
+                    acc[k][2] += w * q2;
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int k = 0; k < kMaxPer; k++) {
+        const int m = threadIdx.x + k * kChargeThreads;
+        if (m < P3) {
+            T* o = p.part + ((int64_t)blockIdx.x * P3 + m) * 4;
+            st4<T>(o, make4(acc[k][0], acc[k][1], acc[k][2], T(0)));
+        }
+    }
+}
+
+// Proxy records: charges = the node's chunk partials summed in chunk order
+// (in double), position = the Chebyshev grid point of the node's box.
+template <typename T>
+__global__ void k_charges_finish(const int32_t* __restrict__ chunk_first, int64_t num_interp,
+                                 const int4* __restrict__ chunks, const T* __restrict__ part,
+                                 const T* __restrict__ bc, const T* __restrict__ bh,
+                                 const ChargeParams<T> p, T* __restrict__ prox) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int P = p.P, P3 = p.P3;
+    const int64_t ii = idx / P3;
+    const int m = (int)(idx - ii * P3);
+    if (ii >= num_interp) return;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    const int c0 = chunk_first[ii], c1 = chunk_first[ii + 1];
+    for (int ch = c0; ch < c1; ch++) {
+        const T* q = part + ((int64_t)ch * P3 + m) * 4;
+        s0 += (double)q[0];
+        s1 += (double)q[1];
+        s2 += (double)q[2];
+    }
+    const int64_t node = chunks[c0].x;
+    const T* c = bc + 4 * node;
+    const T* h = bh + 4 * node;
+    const int a = m / (P * P), b = (m / P) % P, cc = m % P;
+    const T y0 = c[0] + h[0] * p.cheb[a];
+    const T y1 = c[1] + h[1] * p.cheb[b];
+    const T y2 = c[2] + h[2] * p.cheb[cc];
+    T* r = prox + idx * kRec;
+    st4<T>(r, make4(y0, y1, y2, (T)s0));
+    st4<T>(r + 4, make4(exp_t(y0 * T(-0.5)), exp_t(y1 * T(-0.5)), exp_t(y2 * T(-0.5)), (T)s1));
+    st4<T>(r + 8, make4((T)s2, T(0), T(0), T(0)));
+}
+
+// ---- the walk -------------------------------------------------------------------
+
+template <typename T>
+struct IWalk {
+    int64_t M = 0, nq = 0;
+    const int4* meta = nullptr;
+    const T* bc = nullptr;
+    const int32_t* iidx = nullptr;
+    const T* pts = nullptr;
+    const T* prox = nullptr;
+    int P3 = 0;
+    int direct_max = 0;
+    T theta = T(0.5);
+    // queries: the tree's points (grouped by qgroup), an explicit array
+    // (optional processing order), or the nodes of a regular grid
+    const T* spos = nullptr;
+    const int32_t* perm = nullptr;
+    const int32_t* qgroup = nullptr;
+    const T* queries = nullptr;
+    const int32_t* qorder = nullptr;
+    const T* widths = nullptr;
+    T width = T(0);
+    int grid = 0;
+    int gx = 0, gy = 0, gz = 0;
+    T gox = T(0), goy = T(0), goz = T(0), gh = T(0);
+    T* out = nullptr;
+    int out_stride = 1;
+    int accumulate = 0;
+    unsigned long long* counter = nullptr;  // next group of 32 queries (persistent launch)
+    int* err = nullptr;                     // set when a staging wait runs out
+    uint32_t spin = 0;                      // try_wait rounds before a wait runs out
+};
+
+template <int OP>
+struct IOp {
+    static constexpr bool a2 = OP == kOpA21 || OP == kOpA22 || OP == kOpA23 || OP == kOpA3 ||
+                               OP == kOpA2Fused;
+    static constexpr bool a2t1 = OP == kOpA2T1 || OP == kOpA2T2 || OP == kOpA2T3;
+    static constexpr bool a2tsum = OP == kIOpA2TSum || OP == kIOpA2TShared;
+    static constexpr int k = (OP == kOpA21 || OP == kOpA2T1)   ? 0
+                             : (OP == kOpA22 || OP == kOpA2T2) ? 1
+                             : (OP == kOpA23 || OP == kOpA2T3) ? 2
+                                                                : -1;
+    static constexpr bool s0 = k == 0 || OP == kOpA3 || OP == kOpA2Fused;
+    static constexpr bool s1 = k == 1 || OP == kOpA3 || OP == kOpA2Fused;
+    static constexpr bool s2 = k == 2 || OP == kOpA3 || OP == kOpA2Fused;
+    static constexpr bool query_exp = a2 || a2t1 || a2tsum;
+};
+
+template <typename T>
+struct IQ {
+    T x, y, z;
+    T tw;          // width threshold on r^2
+    T iw, iw3;     // 1/w, 1/w^3 (continuous kernel inside the width)
+    T ex0, ex1, ex2;  // exp(x_k / 2)
+};
+
+template <typename T>
+__device__ __forceinline__ void kahan(T& s, T& c, T v) {
+    const T y = v - c;
+    const T t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
+// One pair term against record r (a point or a proxy).  NEAR: the per-pair
+// width test of the reference kernels; far sources are outside every width.
+template <typename T, int OP, bool CONT, bool NEAR>
+__device__ __forceinline__ void iterm(const IQ<T>& q, const T* __restrict__ r, T& p0, T& p1, T& p2,
+                                      T& i0, T& i1, T& i2) {
+    const Vec4<T> r0 = ld4(r);
+    if constexpr (OP == kOpCount) {
+        p0 += T(1);
+        return;
+    } else {
+        const T dx = q.x - r0.x, dy = q.y - r0.y, dz = q.z - r0.z;
+        const T d2 = dx * dx + dy * dy + dz * dz;
+        bool outside = true;
+        if constexpr (NEAR) outside = d2 >= q.tw;
+        const T rinv = (!NEAR || outside) ? rsqrt_t(d2) : T(0);
+        const T rinv2 = rinv * rinv;
+        const Vec4<T> r1 = ld4(r + 4);  // (e0, e1, e2, c1)
+        if constexpr (OP == kOpA || OP == kOpG || IOp<OP>::a2) {
+            const T m0 = r0.w, m1 = r1.w, m2 = r[8];
+            const T dm = dx * m0 + dy * m1 + dz * m2;
+            if constexpr (OP == kOpA) {
+                p0 += dm * (rinv * rinv2);
+                if constexpr (NEAR && CONT) {
+                    if (!outside) i0 += dm * q.iw3;
+                }
+            } else if constexpr (OP == kOpG) {
+                const T rinv3 = rinv * rinv2;
+                const T c = T(3) * dm * (rinv3 * rinv2);
+                p0 += m0 * rinv3 - dx * c;
+                p1 += m1 * rinv3 - dy * c;
+                p2 += m2 * rinv3 - dz * c;
+            } else {
+                const T t = dm * (rinv * rinv2);
+                const T hh = T(0.5) * rinv;
+                if constexpr (IOp<OP>::s0) p0 += r1.x * (t + hh * m0);
+                if constexpr (IOp<OP>::s1) p1 += r1.y * (t + hh * m1);
+                if constexpr (IOp<OP>::s2) p2 += r1.z * (t + hh * m2);
+                if constexpr (NEAR && CONT) {
+                    if (!outside) {
+                        const T ti = dm * q.iw3;
+                        const T hi = T(0.5) * q.iw;
+                        if constexpr (IOp<OP>::s0) i0 += ti + hi * m0;
+                        if constexpr (IOp<OP>::s1) i1 += ti + hi * m1;
+                        if constexpr (IOp<OP>::s2) i2 += ti + hi * m2;
+                    }
+                }
+            }
+        } else if constexpr (OP == kOpAT) {
+            const T c = r0.w * (rinv * rinv2);
+            p0 += dx * c;
+            p1 += dy * c;
+            p2 += dz * c;
+        } else if constexpr (IOp<OP>::a2t1) {
+            constexpr int k = IOp<OP>::k;
+            const T e = k == 0 ? r1.x : (k == 1 ? r1.y : r1.z);
+            const T gr = e * r0.w * rinv;
+            const T c = gr * rinv2;
+            p0 += dx * c;
+            p1 += dy * c;
+            p2 += dz * c;
+            if constexpr (k == 0) p0 += T(0.5) * gr;
+            if constexpr (k == 1) p1 += T(0.5) * gr;
+            if constexpr (k == 2) p2 += T(0.5) * gr;
+        } else if constexpr (IOp<OP>::a2tsum) {
+            // sum_k exp(x_k/2) exp(-y_k/2) s_k (d / r^3 + e_k / (2r))
+            const T sa = r0.w;
+            const T sb = OP == kIOpA2TSum ? r1.w : r0.w;
+            const T sc = OP == kIOpA2TSum ? r[8] : r0.w;
+            const T g0 = q.ex0 * r1.x * sa, g1 = q.ex1 * r1.y * sb, g2 = q.ex2 * r1.z * sc;
+            const T c = (g0 + g1 + g2) * (rinv * rinv2);
+            const T hr = T(0.5) * rinv;
+            p0 += dx * c + g0 * hr;
+            p1 += dy * c + g1 * hr;
+            p2 += dz * c + g2 * hr;
+        }
+    }
+}
+
+// The sum over `count` consecutive records into this lane's compensated sums.
+// (lanes outside the walking subgroup, active = false, compute and discard)
+template <typename T, int OP, bool CONT, bool NEAR>
+__device__ __forceinline__ void irange(const IQ<T>& q, bool active, const T* __restrict__ r,
+                                       int count, T* s, T* cmp, T* in) {
+    T p0 = T(0), p1 = T(0), p2 = T(0), i0 = T(0), i1 = T(0), i2 = T(0);
+    int j = 0;
+    for (; j + 1 < count; j += 2) {
+        iterm<T, OP, CONT, NEAR>(q, r + (int64_t)j * kRec, p0, p1, p2, i0, i1, i2);
+        iterm<T, OP, CONT, NEAR>(q, r + (int64_t)(j + 1) * kRec, p0, p1, p2, i0, i1, i2);
+    }
+    if (j < count) iterm<T, OP, CONT, NEAR>(q, r + (int64_t)j * kRec, p0, p1, p2, i0, i1, i2);
+    if (!active) return;
+    if constexpr (OP == kOpCount) {
+        s[0] += p0;
+    } else {
+        kahan(s[0], cmp[0], p0);
+        kahan(s[1], cmp[1], p1);
+        kahan(s[2], cmp[2], p2);
+        if constexpr (NEAR && CONT) {
+            in[0] += i0;
+            in[1] += i1;
+            in[2] += i2;
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t icompact3(uint64_t x) {
+    x &= 0x1249249249249249ull;
+    x = (x ^ (x >> 2)) & 0x10c30c30c30c30c3ull;
+    x = (x ^ (x >> 4)) & 0x100f00f00f00f00full;
+    x = (x ^ (x >> 8)) & 0x1f0000ff0000ffull;
+    x = (x ^ (x >> 16)) & 0x1f00000000ffffull;
+    x = (x ^ (x >> 32)) & 0x1fffffull;
+    return (uint32_t)x;
+}
+
+// This lane's query (the same three sources and output rows as the
+// reference-mode walks); false past the end.
+template <typename T>
+__device__ __forceinline__ bool iload(const IWalk<T>& p, int64_t qi, IQ<T>& q, int64_t& oidx,
+                                      T& w) {
+    w = p.width;
+    oidx = 0;
+    q.x = q.y = q.z = T(0);
+    bool valid = qi < p.nq;
+    if (valid && p.grid) {
+        const uint32_t i = icompact3((uint64_t)qi), j = icompact3((uint64_t)qi >> 1),
+                       k = icompact3((uint64_t)qi >> 2);
+        valid = i < (uint32_t)p.gx && j < (uint32_t)p.gy && k < (uint32_t)p.gz;
+        if (valid) {
+            oidx = ((int64_t)k * p.gy + j) * p.gx + i;
+            q.x = fma(T(i), p.gh, p.gox);
+            q.y = fma(T(j), p.gh, p.goy);
+            q.z = fma(T(k), p.gh, p.goz);
+            if (p.widths) w = p.widths[oidx];
+        }
+    } else if (valid) {
+        if (p.queries == nullptr) {
+            const int64_t s = p.qgroup ? (int64_t)p.qgroup[qi] : qi;
+            oidx = p.perm[s];
+            q.x = p.spos[3 * s];
+            q.y = p.spos[3 * s + 1];
+            q.z = p.spos[3 * s + 2];
+        } else {
+            oidx = p.qorder ? (int64_t)p.qorder[qi] : qi;
+            q.x = p.queries[3 * oidx];
+            q.y = p.queries[3 * oidx + 1];
+            q.z = p.queries[3 * oidx + 2];
+        }
+        if (p.widths) w = p.widths[oidx];
+    }
+    q.tw = width_threshold(w);
+    q.iw = T(1) / w;
+    q.iw3 = T(1) / (w * w * w);
+    return valid;
+}
+
+template <typename T>
+__device__ __forceinline__ void iput(T* o, int j, T v, int accumulate) {
+    o[j] = accumulate ? o[j] + v : v;
+}
+
+// A batch of queries: bounding centre, radius and largest width.
+template <typename T>
+struct Batch {
+    T cx, cy, cz, r, w;
+};
+
+// Split factor of the query groups (see lane_batch).
+constexpr float kSplit = 5.0f;
+
+// The batch this lane's query walks in.  The warp's 32 queries are
+// consecutive along a space-filling curve, but a group that straddles a jump
+// of the curve between distant parts of the cloud has a large radius, accepts
+// little as far and sums most of the cloud directly (one such warp dominated
+// a launch).  So the group is split top-down in aligned halves: a group of
+// 2^k lanes is split when its radius exceeds kSplit times the radius of its
+// more compact half (the other half then holds the straggler), and each lane
+// walks with the first group on its path that is not split.  Lanes of one
+// final group reach the same decision (they share the group and its halves);
+// *bits receives log2 of its size.  A compact group keeps all 32 lanes
+// (measured on the 1M-point union-of-primitives cloud: ~8 % of the groups
+// split at all).
+template <typename T>
+__device__ __forceinline__ Batch<T> lane_batch(const IQ<T>& q, bool valid, T w, int* bits) {
+    T lo0 = valid ? q.x : T(INFINITY), hi0 = valid ? q.x : -T(INFINITY);
+    T lo1 = valid ? q.y : T(INFINITY), hi1 = valid ? q.y : -T(INFINITY);
+    T lo2 = valid ? q.z : T(INFINITY), hi2 = valid ? q.z : -T(INFINITY);
+    // a NaN width admits no far node (every pair is then summed directly)
+    T wm = valid ? (w == w ? w : T(INFINITY)) : T(0);
+    Batch<T> b[6];
+    T sib[6];  // radius of the other half of the level-k group (k >= 1)
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        if (k > 0) {
+            const int o = 1 << (k - 1);
+            sib[k] = __shfl_xor_sync(kAll, b[k - 1].r, o);
+            lo0 = fmin(lo0, __shfl_xor_sync(kAll, lo0, o));
+            hi0 = fmax(hi0, __shfl_xor_sync(kAll, hi0, o));
+            lo1 = fmin(lo1, __shfl_xor_sync(kAll, lo1, o));
+            hi1 = fmax(hi1, __shfl_xor_sync(kAll, hi1, o));
+            lo2 = fmin(lo2, __shfl_xor_sync(kAll, lo2, o));
+            hi2 = fmax(hi2, __shfl_xor_sync(kAll, hi2, o));
+            wm = fmax(wm, __shfl_xor_sync(kAll, wm, o));
+        }
+        // (a group without a valid query gets the zero batch)
+        const bool any = lo0 <= hi0;
+        b[k].cx = any ? T(0.5) * (lo0 + hi0) : T(0);
+        b[k].cy = any ? T(0.5) * (lo1 + hi1) : T(0);
+        b[k].cz = any ? T(0.5) * (lo2 + hi2) : T(0);
+        const T hx = any ? fmax(hi0 - b[k].cx, b[k].cx - lo0) : T(0);
+        const T hy = any ? fmax(hi1 - b[k].cy, b[k].cy - lo1) : T(0);
+        const T hz = any ? fmax(hi2 - b[k].cz, b[k].cz - lo2) : T(0);
+        b[k].r = sqrt(hx * hx + hy * hy + hz * hz) * T(1.0 + 1.0 / 65536);
+        b[k].w = any ? fmax(wm, T(0)) * T(1.0 + 1.0 / 65536) : T(0);
+    }
+    int k = 5;
+#pragma unroll
+    for (int j = 5; j > 0; j--) {
+        if (k == j && b[j].r > T(kSplit) * fmin(b[j - 1].r, sib[j])) k = j - 1;
+    }
+    *bits = k;
+    Batch<T> out = b[0];
+#pragma unroll
+    for (int j = 1; j < 6; j++)
+        if (k == j) out = b[j];
+    return out;
+}
+
+// ---- the pipelined walk ----------------------------------------------------------
+//
+// Every interaction is a contiguous run of source records (a node's points in
+// Morton order, or a node's proxy grid), so it is staged into shared memory
+// with one-dimensional TMA bulk copies (cp.async.bulk, completion counted on
+// an mbarrier) and the warp's 32 lanes read each record with a broadcast
+// shared-memory load.  Each warp keeps kSlots tiles in flight: the tree walk
+// runs ahead of the arithmetic, issuing the copies of the next tiles while
+// the current one is summed, so the L2 latency of the records (they are
+// streamed: every warp reads its own interaction list) is hidden.  The launch
+// is persistent: its warps take groups of 32 queries from an atomic counter,
+// in curve order, so a warp that drew an expensive group does not hold back
+// the others.  Every wait is bounded: a wait that runs out sets the error
+// flag, waits (bounded again) for the warp's copies still in flight and ends
+// the warp.
+constexpr int kSlots = 4;            // tiles in flight per warp
+constexpr int kTileBytes = 3072;     // per tile: 64 float records, 32 double records
+constexpr int kPWarps = 4;           // warps per block
+constexpr uint32_t kDrainSpin = 1u << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// bytes from global src to shared dst (both 16-byte aligned, bytes a multiple
+// of 16), completing on bar's current phase
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, uint32_t bytes,
+                                            uint64_t* bar) {
+    // the slot's previous contents were read through the generic proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t spin) {
+    for (uint32_t it = 0; it < spin; it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+template <typename T>
+constexpr int tile_records() {
+    return kTileBytes / (kRec * (int)sizeof(T));
+}
+
+template <typename T>
+constexpr size_t walk_smem_bytes() {
+    return (size_t)kPWarps * kSlots * (kTileBytes + sizeof(uint64_t));
+}
+
+template <typename T, int OP, bool CONT>
+__global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
+    extern __shared__ __align__(128) unsigned char dsm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* tiles = dsm + (size_t)warp * kSlots * kTileBytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(dsm + (size_t)kPWarps * kSlots * kTileBytes) +
+                     warp * kSlots;
+    if (lane == 0) {
+        for (int sl = 0; sl < kSlots; sl++) mbar_init(bars + sl);
+        mbar_init_fence();
+    }
+    __syncwarp();
+    constexpr int kTR = tile_records<T>();
+    // warp-uniform pipeline state: next slot to consume, tiles in flight, the
+    // parity of each slot's next completion, and each slot's tile (count | near << 7)
+    int head = 0, inflight = 0;
+    uint32_t phase = 0, tinfo = 0;
+    const int M = (int)p.M;
+    const int64_t ngroups = (p.nq + 31) / 32;
+    for (;;) {
+        unsigned long long grp = 0;
+        if (lane == 0) grp = atomicAdd(p.counter, 1ull);
+        grp = __shfl_sync(kAll, grp, 0);
+        if ((int64_t)grp >= ngroups) break;
+        const int64_t qi = (int64_t)grp * 32 + lane;
+        IQ<T> q;
+        int64_t oidx;
+        T w;
+        const bool valid = iload(p, qi, q, oidx, w);
+        if (__all_sync(kAll, !valid)) continue;  // grid lanes outside the grid
+        if constexpr (IOp<OP>::query_exp) {
+            q.ex0 = exp_t(q.x * T(0.5));
+            q.ex1 = exp_t(q.y * T(0.5));
+            q.ex2 = exp_t(q.z * T(0.5));
+        } else {
+            q.ex0 = q.ex1 = q.ex2 = T(1);
+        }
+        int bits;
+        const Batch<T> mine = lane_batch(q, valid, w, &bits);
+        T s[3] = {T(0), T(0), T(0)}, cmp[3] = {T(0), T(0), T(0)}, in[3] = {T(0), T(0), T(0)};
+        for (int g = 0; g < 32;) {
+            // the group starting at lane g (every lane of it holds the same batch)
+            const int kg = __shfl_sync(kAll, bits, g);
+            const bool active = valid && (lane >> kg) == (g >> kg);
+            const int gnext = g + (1 << kg);
+            if (!__any_sync(kAll, active)) {
+                g = gnext;
+                continue;
+            }
+            const T bcx = __shfl_sync(kAll, mine.cx, g), bcy = __shfl_sync(kAll, mine.cy, g),
+                    bcz = __shfl_sync(kAll, mine.cz, g), br = __shfl_sync(kAll, mine.r, g),
+                    wm = __shfl_sync(kAll, mine.w, g);
+            // producer: the walk, one interaction (a run of records) at a time
+            int n = 0, left = 0, near = 0;
+            const T* src = nullptr;
+            bool more = true;
+            for (;;) {
+                while (more && inflight < kSlots) {
+                    while (left == 0 && n < M) {
+                        const int4 mt = __ldg(p.meta + n);
+                        const Vec4<T> bx = ld4(p.bc + 4 * (int64_t)n);
+                        const T dx = bcx - bx.x, dy = bcy - bx.y, dz = bcz - bx.z;
+                        const T R2 = dx * dx + dy * dy + dz * dz;
+                        // every query x of the batch sees the node at |x - c| >= R - r_B,
+                        // so r_C + theta r_B < theta R gives r_C < theta |x - c| for each
+                        const T sr = br + bx.w;
+                        const T sw = sr + wm;
+                        const T a = bx.w + p.theta * br;
+                        const bool far = a * a < (p.theta * p.theta) * R2 && R2 >= sw * sw;
+                        const int np = node_npts(mt);
+                        if (far) {
+                            const int ii = __ldg(p.iidx + n);
+                            if (ii >= 0) {
+                                src = p.prox + (int64_t)ii * p.P3 * kRec;
+                                left = p.P3;
+                            } else {
+                                src = p.pts + (int64_t)mt.y * kRec;
+                                left = np;
+                            }
+                            near = 0;
+                            n = mt.x;
+                        } else if (node_leaf(mt) || np <= p.direct_max) {
+                            src = p.pts + (int64_t)mt.y * kRec;
+                            left = np;
+                            near = 1;
+                            n = mt.x;
+                        } else {
+                            n = n + 1;
+                        }
+                    }
+                    if (left == 0) {
+                        more = false;
+                        break;
+                    }
+                    const int cnt = min(left, kTR);
+                    const int slot = (head + inflight) % kSlots;
+                    if (lane == 0)
+                        tma_load_1d(tiles + (size_t)slot * kTileBytes, src,
+                                    (uint32_t)(cnt * kRec * sizeof(T)), bars + slot);
+                    tinfo = (tinfo & ~(0xffu << (8 * slot))) |
+                            ((uint32_t)(cnt | (near << 7)) << (8 * slot));
+                    src += (int64_t)cnt * kRec;
+                    left -= cnt;
+                    inflight++;
+                }
+                if (inflight == 0) break;
+                // consumer: the oldest tile
+                if (!mbar_wait(bars + head, (phase >> head) & 1u, p.spin)) {
+                    // a copy did not arrive: report, let the copies in flight land, stop
+                    if (lane == 0) atomicOr(p.err, 1);
+                    for (int k2 = 0; k2 < inflight; k2++) {
+                        const int sl = (head + k2) % kSlots;
+                        mbar_wait(bars + sl, (phase >> sl) & 1u, kDrainSpin);
+                    }
+                    return;
+                }
+                phase ^= 1u << head;
+                const uint32_t inf = (tinfo >> (8 * head)) & 0xffu;
+                const T* r = reinterpret_cast<const T*>(tiles + (size_t)head * kTileBytes);
+                if (inf >> 7)
+                    irange<T, OP, CONT, true>(q, active, r, (int)(inf & 0x7fu), s, cmp, in);
+                else
+                    irange<T, OP, CONT, false>(q, active, r, (int)(inf & 0x7fu), s, cmp, in);
+                __syncwarp();  // every lane has read the slot before it is refilled
+                head = (head + 1) % kSlots;
+                inflight--;
+            }
+            g = gnext;
+        }
+        if (!valid) continue;
+        T* o = p.out + oidx * (int64_t)p.out_stride;
+        const int acc = p.accumulate;
+        // the compensated sums (Kahan: cmp holds what the last additions rounded away)
+        const T v0 = s[0] - cmp[0], v1 = s[1] - cmp[1], v2 = s[2] - cmp[2];
+        if constexpr (IOp<OP>::a2) {
+            const T ew = CONT ? exp_t(w) : T(0);
+            const T u0 = q.ex0 * v0 + ew * in[0];
+            const T u1 = q.ex1 * v1 + ew * in[1];
+            const T u2 = q.ex2 * v2 + ew * in[2];
+            if constexpr (OP == kOpA21) iput(o, 0, u0, acc);
+            if constexpr (OP == kOpA22) iput(o, 0, u1, acc);
+            if constexpr (OP == kOpA23) iput(o, 0, u2, acc);
+            if constexpr (OP == kOpA3) iput(o, 0, (u0 + u1 + u2) / T(3), acc);
+            if constexpr (OP == kOpA2Fused) {
+                iput(o, 0, u0, acc);
+                iput(o, 1, u1, acc);
+                iput(o, 2, u2, acc);
+            }
+        } else if constexpr (IOp<OP>::a2t1) {
+            constexpr int k = IOp<OP>::k;
+            const T ek = k == 0 ? q.ex0 : (k == 1 ? q.ex1 : q.ex2);
+            iput(o, 0, ek * v0, acc);
+            iput(o, 1, ek * v1, acc);
+            iput(o, 2, ek * v2, acc);
+        } else if constexpr (OP == kOpA) {
+            iput(o, 0, v0 + in[0], acc);
+        } else if constexpr (OP == kOpCount) {
+            iput(o, 0, v0, acc);
+        } else {
+            iput(o, 0, v0, acc);
+            iput(o, 1, v1, acc);
+            iput(o, 2, v2, acc);
+        }
+    }
+}
+
+template <typename T, int OP, bool CONT>
+int ilaunch(IWalk<T> p, cudaStream_t s) {
+    const int64_t groups = (p.nq + 31) / 32;
+    if (groups == 0) return kOk;
+    auto kern = k_iwalk<T, OP, CONT>;
+    const size_t smem = walk_smem_bytes<T>();
+    // per instantiation and device: the shared-memory limit and the resident blocks
+    static int blocks_per_sm[64] = {0};
+    int dev = 0, sms = 0;
+    CAGR_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(kErrInvalid, "device index too large");
+    CAGR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (blocks_per_sm[dev] == 0) {
+        CAGR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int nb = 0;
+        CAGR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kPWarps * 32, smem));
+        blocks_per_sm[dev] = nb > 0 ? nb : 1;
+    }
+    const int64_t want = (groups + kPWarps - 1) / kPWarps;
+    const int64_t blocks = std::min<int64_t>(want, (int64_t)blocks_per_sm[dev] * sms);
+    void* ctr = nullptr;
+    if (int rc = pool_alloc(&ctr, sizeof(unsigned long long), s)) return rc;
+    int rc = kOk;
+    if (cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), s) != cudaSuccess) {
+        rc = set_error(kErrCuda, "walk counter");
+    } else {
+        p.counter = (unsigned long long*)ctr;
+        kern<<<(unsigned)blocks, kPWarps * 32, smem, s>>>(p);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = set_error(kErrCuda, std::string("walk launch: ") + cudaGetErrorString(e));
+    }
+    pool_free(ctr, s);
+    return rc;
+}
+
+template <typename T, int OP>
+int ilaunch_cont(const IWalk<T>& p, int cont, cudaStream_t s) {
+    return cont ? ilaunch<T, OP, true>(p, s) : ilaunch<T, OP, false>(p, s);
+}
+
+// ---- host side ----------------------------------------------------------------
+
+template <typename F>
+int cub_run(F&& f, cudaStream_t s) {
+    size_t bytes = 0;
+    CAGR_CUDA(f(nullptr, bytes));
+    void* tmp = nullptr;
+    if (int rc = pool_alloc(&tmp, bytes, s)) return rc;
+    const cudaError_t e = f(tmp, bytes);
+    pool_free(tmp, s);
+    if (e != cudaSuccess) return set_error(kErrCuda, std::string("cub: ") + cudaGetErrorString(e));
+    return kOk;
+}
+
+unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+template <typename T>
+int setup_impl(Tree* t, Interp* I, cudaStream_t s) {
+    const int64_t M = t->m;
+    if (int rc = pool_alloc(&I->box_c, sizeof(T) * 4 * M, s)) return rc;
+    if (int rc = pool_alloc(&I->box_h, sizeof(T) * 4 * M, s)) return rc;
+    if (int rc = pool_alloc((void**)&I->iidx, sizeof(int32_t) * M, s)) return rc;
+    if (int rc = pool_alloc((void**)&I->err, sizeof(int), s)) return rc;
+    CAGR_CUDA(cudaMemsetAsync(I->err, 0, sizeof(int), s));
+    k_box<T><<<blocks_for(M * 32, 128), 128, 0, s>>>(t->meta, (const T*)t->spos, M, (T*)I->box_c,
+                                                     (T*)I->box_h);
+    void *flag = nullptr, *nch = nullptr, *pos = nullptr, *chb = nullptr;
+    int rc = pool_alloc(&flag, sizeof(int32_t) * M, s);
+    if (!rc) rc = pool_alloc(&nch, sizeof(int32_t) * M, s);
+    if (!rc) rc = pool_alloc(&pos, sizeof(int32_t) * M, s);
+    if (!rc) rc = pool_alloc(&chb, sizeof(int32_t) * M, s);
+    if (!rc) {
+        k_iflags<<<blocks_for(M, 256), 256, 0, s>>>(t->meta, M, I->P3, (int32_t*)flag, (int32_t*)nch);
+        rc = cub_run([&](void* tp, size_t& b) {
+            return cub::DeviceScan::ExclusiveSum(tp, b, (const int32_t*)flag, (int32_t*)pos, (int)M, s);
+        }, s);
+    }
+    if (!rc)
+        rc = cub_run([&](void* tp, size_t& b) {
+            return cub::DeviceScan::ExclusiveSum(tp, b, (const int32_t*)nch, (int32_t*)chb, (int)M, s);
+        }, s);
+    int32_t last[4] = {0, 0, 0, 0};
+    if (!rc) {
+        // totals = last exclusive prefix + last element
+        cudaMemcpyAsync(&last[0], (int32_t*)pos + (M - 1), 4, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&last[1], (int32_t*)flag + (M - 1), 4, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&last[2], (int32_t*)chb + (M - 1), 4, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&last[3], (int32_t*)nch + (M - 1), 4, cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) rc = set_error(kErrCuda, "interp setup sync");
+    }
+    if (!rc) {
+        I->num_interp = (int64_t)last[0] + last[1];
+        I->num_chunks = (int64_t)last[2] + last[3];
+        const int64_t ni = I->num_interp, nc = I->num_chunks;
+        rc = pool_alloc((void**)&I->chunks, sizeof(int4) * (nc > 0 ? nc : 1), s);
+        if (!rc) rc = pool_alloc((void**)&I->chunk_first, sizeof(int32_t) * (ni + 1), s);
+        if (!rc) rc = pool_alloc(&I->part, sizeof(T) * 4 * (size_t)(nc > 0 ? nc : 1) * I->P3, s);
+        if (!rc) {
+            const int32_t ncl = (int32_t)nc;
+            cudaMemcpyAsync(I->chunk_first + ni, &ncl, 4, cudaMemcpyHostToDevice, s);
+            k_ichunks<<<blocks_for(M, 256), 256, 0, s>>>(t->meta, M, (const int32_t*)flag,
+                                                         (const int32_t*)pos, (const int32_t*)chb,
+                                                         I->iidx, I->chunks, I->chunk_first);
+            // the copy above reads a host variable: finish it before returning
+            if (cudaStreamSynchronize(s) != cudaSuccess) rc = set_error(kErrCuda, "interp setup");
+        }
+    }
+    pool_free(flag, s);
+    pool_free(nch, s);
+    pool_free(pos, s);
+    pool_free(chb, s);
+    if (!rc && cudaGetLastError() != cudaSuccess) rc = set_error(kErrCuda, "interp setup launch");
+    return rc;
+}
+
+template <typename T>
+ChargeParams<T> charge_params(const Interp* I) {
+    ChargeParams<T> p;
+    p.P = I->P;
+    p.P3 = I->P3;
+    for (int k = 0; k < kPMax; k++) {
+        p.cheb[k] = (T)I->cheb[k];
+        p.omega[k] = (T)I->omega[k];
+    }
+    return p;
+}
+
+template <typename T>
+int scatter_impl(Tree* t, Interp* I, int slot, const void* attrs, int dim, cudaStream_t s) {
+    const int64_t N = t->n;
+    if (!I->pts[slot]) {
+        if (int rc = pool_alloc(&I->pts[slot], sizeof(T) * kRec * N, s)) return rc;
+    }
+    if (!I->prox[slot]) {
+        const size_t np = (size_t)(I->num_interp > 0 ? I->num_interp : 1) * I->P3;
+        if (int rc = pool_alloc(&I->prox[slot], sizeof(T) * kRec * np, s)) return rc;
+    }
+    I->dim[slot] = 0;
+    k_ipoints<T><<<blocks_for(N, 256), 256, 0, s>>>((const T*)t->spos, t->perm, N, (const T*)attrs,
+                                                    dim, (T*)I->pts[slot]);
+    if (I->num_chunks > 0) {
+        ChargeParams<T> cp = charge_params<T>(I);
+        cp.chunks = I->chunks;
+        cp.bc = (const T*)I->box_c;
+        cp.bh = (const T*)I->box_h;
+        cp.pts = (const T*)I->pts[slot];
+        cp.part = (T*)I->part;
+        k_charges<T><<<(unsigned)I->num_chunks, kChargeThreads, 0, s>>>(cp);
+        k_charges_finish<T><<<blocks_for(I->num_interp * I->P3, 256), 256, 0, s>>>(
+            I->chunk_first, I->num_interp, I->chunks, (const T*)I->part, (const T*)I->box_c,
+            (const T*)I->box_h, cp, (T*)I->prox[slot]);
+    }
+    CAGR_CUDA(cudaGetLastError());
+    I->dim[slot] = dim;
+    return kOk;
+}
+
+template <typename T>
+int traverse_impl(const Tree* t, const Interp* I, const TraverseArgs& a, cudaStream_t s) {
+    IWalk<T> p;
+    p.M = t->m;
+    p.nq = a.queries ? a.nq : t->n;
+    if (a.grid) {
+        int bits = 0;
+        while ((1 << bits) < a.gx || (1 << bits) < a.gy || (1 << bits) < a.gz) bits++;
+        p.grid = 1;
+        p.gx = a.gx;
+        p.gy = a.gy;
+        p.gz = a.gz;
+        p.gox = (T)a.gorigin[0];
+        p.goy = (T)a.gorigin[1];
+        p.goz = (T)a.gorigin[2];
+        p.gh = (T)a.gspacing;
+        p.nq = int64_t(1) << (3 * bits);
+    }
+    p.meta = t->meta;
+    p.bc = (const T*)I->box_c;
+    p.iidx = I->iidx;
+    p.P3 = I->P3;
+    p.direct_max = I->direct_max;
+    p.theta = (T)I->theta;
+    p.spos = (const T*)t->spos;
+    p.perm = t->perm;
+    p.qgroup = t->qgroup;   // self-queries in Hilbert groups: compact batches
+    p.queries = (const T*)a.queries;
+    p.qorder = a.qorder;
+    p.widths = (const T*)a.widths;
+    p.width = (T)a.width;
+    p.out = (T*)a.out;
+    p.accumulate = a.accumulate;
+    p.err = I->err;
+    p.spin = I->spin;
+    // which slot and attribute dim the operator reads
+    int op = a.op;
+    if (a.op == kOpA2TFused) {
+        if (a.slots == 3) op = kIOpA2TSum;
+        else if (a.slots == 1) op = kIOpA2TShared;
+        else return set_error(kErrInvalid, "the A2T right-hand side walk is not available with the "
+                                           "interpolated far field: sum its two parts");
+    }
+    const int slot = op == kIOpA2TSum ? 3 : 0;
+    const bool scalar_in = op == kOpAT || op == kOpA2T1 || op == kOpA2T2 || op == kOpA2T3 ||
+                           op == kIOpA2TShared;
+    const int need = op == kOpCount ? I->dim[0] : (op == kIOpA2TSum ? 3 : (scalar_in ? 1 : 3));
+    if (I->dim[slot] == 0 || I->dim[slot] != need)
+        return set_error(kErrState, "the charges of the right attribute dim are not computed "
+                                    "(cagr_scatter / cagr_scatter3 first)");
+    p.pts = (const T*)I->pts[slot];
+    p.prox = (const T*)I->prox[slot];
+    const int out_dim = (op == kOpA || op == kOpA3 || op == kOpA21 || op == kOpA22 ||
+                         op == kOpA23 || op == kOpCount) ? 1 : 3;
+    p.out_stride = a.out_stride > 0 ? a.out_stride : out_dim;
+    if (p.nq == 0) return kOk;
+    const int c = a.continuous;
+    switch (op) {
+        case kOpA: return ilaunch_cont<T, kOpA>(p, c, s);
+        case kOpA3: return ilaunch_cont<T, kOpA3>(p, c, s);
+        case kOpA21: return ilaunch_cont<T, kOpA21>(p, c, s);
+        case kOpA22: return ilaunch_cont<T, kOpA22>(p, c, s);
+        case kOpA23: return ilaunch_cont<T, kOpA23>(p, c, s);
+        case kOpA2Fused: return ilaunch_cont<T, kOpA2Fused>(p, c, s);
+        case kOpAT: return ilaunch<T, kOpAT, false>(p, s);
+        case kOpA2T1: return ilaunch<T, kOpA2T1, false>(p, s);
+        case kOpA2T2: return ilaunch<T, kOpA2T2, false>(p, s);
+        case kOpA2T3: return ilaunch<T, kOpA2T3, false>(p, s);
+        case kOpG: return ilaunch<T, kOpG, false>(p, s);
+        case kIOpA2TSum: return ilaunch<T, kIOpA2TSum, false>(p, s);
+        case kIOpA2TShared: return ilaunch<T, kIOpA2TShared, false>(p, s);
+        case kOpCount: return ilaunch<T, kOpCount, false>(p, s);
+        default:
+            return set_error(kErrInvalid, "operator " + std::to_string(a.op) +
+                                              " is not available with the interpolated far field");
+    }
+}
+
+}  // namespace
+
+void interp_free(Tree* t) {
+    Interp* I = t ? t->interp : nullptr;
+    if (!I) return;
+    void* arrays[] = {I->box_c, I->box_h, I->iidx, I->chunks, I->chunk_first, I->part, I->err,
+                      I->pts[0], I->pts[1], I->pts[2], I->pts[3],
+                      I->prox[0], I->prox[1], I->prox[2], I->prox[3]};
+    for (void* p : arrays) pool_free(p, nullptr);
+    delete I;
+    t->interp = nullptr;
+}
+
+int interp_setup(Tree* t, int degree, double theta, int direct_max, cudaStream_t stream) {
+    if (degree < 1 || degree > kPMax - 1) return set_error(kErrInvalid, "degree must be in [1, 8]");
+    if (!(theta > 0.0 && theta < 1.0)) return set_error(kErrInvalid, "theta must be in (0, 1)");
+    if (direct_max < 1 || direct_max > 65536)
+        return set_error(kErrInvalid, "direct_max must be in [1, 65536]");
+    if (t->m >= (int64_t(1) << 31) / 32) return set_error(kErrOverflow, "too many nodes");
+    // the device may still use the previous mode's arrays
+    if (t->interp) {
+        if (cudaStreamSynchronize(stream) != cudaSuccess) return set_error(kErrCuda, "sync");
+        interp_free(t);
+    }
+    Interp* I = new Interp();
+    I->degree = degree;
+    I->P = degree + 1;
+    I->P3 = I->P * I->P * I->P;
+    I->theta = theta;
+    I->direct_max = direct_max;
+    // Chebyshev points of the second kind t_k = cos(pi k / p) and their
+    // barycentric weights (-1)^k, halved at both ends
+    for (int k = 0; k <= degree; k++) {
+        I->cheb[k] = std::cos(M_PI * (double)k / (double)degree);
+        I->omega[k] = ((k & 1) ? -1.0 : 1.0) * ((k == 0 || k == degree) ? 0.5 : 1.0);
+    }
+    t->interp = I;
+    const int rc = t->dtype == 0 ? setup_impl<float>(t, I, stream) : setup_impl<double>(t, I, stream);
+    if (rc != kOk) {
+        cudaStreamSynchronize(stream);
+        interp_free(t);
+    }
+    return rc;
+}
+
+int interp_scatter(Tree* t, int slot, const void* attrs, int dim, cudaStream_t stream) {
+    Interp* I = t->interp;
+    if (!I) return set_error(kErrState, "the interpolated far field is not set up");
+    if (slot < 0 || slot > 3) return set_error(kErrInvalid, "slot must be 0..2");
+    if (dim != 1 && dim != 3) return set_error(kErrInvalid, "attr_dim must be 1 or 3");
+    if (!attrs) return set_error(kErrInvalid, "attrs is null");
+    return t->dtype == 0 ? scatter_impl<float>(t, I, slot, attrs, dim, stream)
+                         : scatter_impl<double>(t, I, slot, attrs, dim, stream);
+}
+
+int interp_traverse(const Tree* t, const TraverseArgs& a, cudaStream_t stream) {
+    const Interp* I = t->interp;
+    if (!I) return set_error(kErrState, "the interpolated far field is not set up");
+    if (!a.out) return set_error(kErrInvalid, "output is null");
+    if (a.queries && a.nq < 0) return set_error(kErrInvalid, "negative query count");
+    if (!a.widths && !(a.width == a.width)) return set_error(kErrInvalid, "width is NaN");
+    if (a.grid && (a.queries || a.qorder || a.gx <= 0 || a.gy <= 0 || a.gz <= 0 ||
+                   a.gx > (1 << 20) || a.gy > (1 << 20) || a.gz > (1 << 20)))
+        return set_error(kErrInvalid, "grid queries need positive dims <= 2^20 and no query array");
+    if (a.qorder && !a.queries) return set_error(kErrInvalid, "a query order needs explicit queries");
+    if (a.widths_hi) return set_error(kErrInvalid, "upper widths apply to the reference mode only");
+    return t->dtype == 0 ? traverse_impl<float>(t, I, a, stream)
+                         : traverse_impl<double>(t, I, a, stream);
+}
+
+namespace {
+__global__ void k_group_order(const int32_t* __restrict__ perm, const int32_t* __restrict__ qgroup,
+                              int64_t n, int32_t* __restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = perm[qgroup[i]];
+}
+}  // namespace
+
+int query_groups(const Tree* t, int32_t* order, cudaStream_t stream) {
+    k_group_order<<<blocks_for(t->n, 256), 256, 0, stream>>>(t->perm, t->qgroup, t->n, order);
+    CAGR_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+int interp_status(const Tree* t) {
+    const Interp* I = t->interp;
+    if (!I) return kOk;
+    int flag = 0;
+    CAGR_CUDA(cudaMemcpy(&flag, I->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag)
+        return set_error(kErrCuda, "a walk of the interpolated far field abandoned a staging wait "
+                                   "(its outputs are incomplete)");
+    return kOk;
+}
+
+int interp_set_wait_limit(Tree* t, int64_t spin) {
+    Interp* I = t->interp;
+    if (!I) return set_error(kErrState, "the interpolated far field is not set up");
+    if (spin < 0 || spin > 0xffffffffLL) return set_error(kErrInvalid, "wait limit out of range");
+    I->spin = (uint32_t)spin;
+    return kOk;
+}
+
+int interp_info(const Tree* t, int* degree, double* theta, int* direct_max, int64_t* num_interp) {
+    const Interp* I = t->interp;
+    if (degree) *degree = I ? I->degree : 0;
+    if (theta) *theta = I ? I->theta : 0.0;
+    if (direct_max) *direct_max = I ? I->direct_max : 0;
+    if (num_interp) *num_interp = I ? I->num_interp : 0;
+    return kOk;
+}
+
+}  // namespace cagr

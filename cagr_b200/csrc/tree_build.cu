@@ -576,6 +576,7 @@ void tree_free(Tree* t) {
                       t->qgroup,   t->counters, t->rec[0],    t->rec[1], t->rec[2],
                       t->adj_nodes, t->adj_points, t->adj_sums};
     for (void* p : arrays) pool_free(p, nullptr);
+    interp_free(t);
     if (prev >= 0) cudaSetDevice(prev);
     delete t;
 }

@@ -121,18 +121,21 @@ class Reconstruction:
 def reconstruct(points: torch.Tensor, mu: torch.Tensor, grid: int = 128,
                 lo: float = -1.2, hi: float = 1.2, width: float = 0.01,
                 area: float | None = None, tree: WindingNumberTreecode | None = None,
-                max_tree_depth: int = 15) -> Reconstruction:
+                max_tree_depth: int = 15, far_field: str = "reference", degree: int = 5,
+                theta: float = 0.5) -> Reconstruction:
     """Surface of oriented points on a regular grid**3 over [lo, hi]^3.
 
     points [N,3] float32 CUDA (normalised), mu [N,3] area-weighted normals (the
     CAGR solve's output).  area: if given, normals are rescaled to n / |n| * area
     with that weight per point, as the GaussRecon driver does (area 1e-5,
     main_GaussRecon_cuda.cu:276-288); if None, mu is used as it is (weights |mu|).
+    far_field / degree / theta: the far-field mode of a tree built here.
     """
     dev = points.device
     sec = {}
     t0 = time.perf_counter()
-    wn = tree if tree is not None else WindingNumberTreecode(points, max_tree_depth)
+    wn = tree if tree is not None else WindingNumberTreecode(
+        points, max_tree_depth, far_field=far_field, degree=degree, theta=theta)
     torch.cuda.synchronize(dev)
     sec["tree"] = time.perf_counter() - t0
     t0 = time.perf_counter()

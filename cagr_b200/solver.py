@@ -66,15 +66,18 @@ def _dot(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
 def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40,
                n_sd: int = 30, lambda0: float = 0.0, wnnc_steps: int = 8,
                widths: torch.Tensor | None = None, max_tree_depth: int = 15,
-               tree: WindingNumberTreecode | None = None) -> SolveResult:
+               tree: WindingNumberTreecode | None = None, far_field: str = "reference",
+               degree: int = 5, theta: float = 0.5) -> SolveResult:
     """Solve for mu on normalised float32 CUDA points [N, 3].
 
     widths: per-point base widths (main_CAGR.py:61 uses ones); each iteration
-    uses widths * width_scale."""
+    uses widths * width_scale.  far_field / degree / theta: the tree's far-field
+    mode when the tree is built here ("interp": the interpolated far field)."""
     dev = points.device
     n = points.shape[0]
     t0 = time.perf_counter()
-    wn = tree if tree is not None else WindingNumberTreecode(points, max_tree_depth)
+    wn = tree if tree is not None else WindingNumberTreecode(
+        points, max_tree_depth, far_field=far_field, degree=degree, theta=theta)
     torch.cuda.synchronize(dev)
     t1 = time.perf_counter()
     dt = points.dtype   # float32 as the reference runs it; float64 works alike
@@ -115,22 +118,30 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
     # terms below the largest width itself
     use_table = len(sd_scales) <= MAX_TABLE_WIDTHS
     w_hi = base * sc_t[-1]
+    # the interpolated far field has no per-query decisions to share between
+    # widths: there each step evaluates A2Tb at its width
+    interp = wn.far_field == "interp"
 
     def RHS(a_mu, i, w):  # A2Tb(w) - A2T(a_mu)
         nonlocal calls
         calls += 6
+        if interp:
+            return wn.forward_A2T_shared(b, w) - wn.forward_A2T_sum(a_mu, w)
         if use_table:
             return (b_hi + b_table[slot_of[i]]) - wn.forward_A2T_sum(a_mu, w)
         return wn.forward_A2T_rhs_window(a_mu, w, b_hi, w_hi)
 
-    b_hi = wn.forward_A2T_shared(b, w_hi)
-    wn.scatter(b, slot=1)   # b is constant: its moments serve every step
     calls += 3   # the reference's A2T1..3(b) at the middle width (main_CAGR.py:98)
-    if use_table:
-        b_table = wn.b_window_table(base, sc_t)
-        rk1 = b_hi + b_table[sd_scales.index(s_mid)]   # overwritten at i == n_sd
-    else:
+    if interp:
         rk1 = wn.forward_A2T_shared(b, base * sc_t[sd_scales.index(s_mid)])
+    else:
+        b_hi = wn.forward_A2T_shared(b, w_hi)
+        wn.scatter(b, slot=1)   # b is constant: its moments serve every step
+        if use_table:
+            b_table = wn.b_window_table(base, sc_t)
+            rk1 = b_hi + b_table[sd_scales.index(s_mid)]   # overwritten at i == n_sd
+        else:
+            rk1 = wn.forward_A2T_shared(b, base * sc_t[sd_scales.index(s_mid)])
     pk = rk1
     r = rk1
     for i in range(iters):

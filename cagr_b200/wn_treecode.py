@@ -13,7 +13,12 @@ device memory.  Differences, all additive:
 * ``forward_A2`` evaluates A21, A22 and A23 in one traversal ([N, 3]);
 * ``forward_A3`` (the GaussRecon field operator) and ``multiply`` evaluate at
   arbitrary query points;
-* ``leaf_size`` is a constructor argument (the reference hard-codes 1).
+* ``leaf_size`` is a constructor argument (the reference hard-codes 1);
+* ``far_field="interp"`` (or ``set_far_field``) switches to the interpolated
+  far field: the same operators with Chebyshev proxy grids per node and one
+  acceptance test per warp of 32 queries, whose error against the exact sums
+  falls geometrically with ``degree`` (the reference's monopole rule stays
+  the default, ``far_field="reference"``).
 
 There is no CPU path: a CPU tensor raises, and so does a missing library.
 """
@@ -51,11 +56,32 @@ def _ptr(t: torch.Tensor | None) -> ctypes.c_void_p | None:
     return None if t is None else ctypes.c_void_p(t.data_ptr())
 
 
+def morton_order(queries: torch.Tensor, bits: int = 10) -> torch.Tensor:
+    """int32 permutation sorting [n, 3] points along a Morton curve over their
+    bounding box (2^bits cells per axis): a spatially coherent processing
+    order for explicit queries."""
+    if queries.shape[0] == 0:
+        return torch.empty(0, dtype=torch.int32, device=queries.device)
+    q = queries.double()
+    lo = q.min(0).values
+    span = torch.clamp((q.max(0).values - lo).max(), min=1e-300)
+    u = ((q - lo) / span * ((1 << bits) - 1)).round().long().clamp_(0, (1 << bits) - 1)
+    code = torch.zeros(q.shape[0], dtype=torch.long, device=q.device)
+    for b in range(bits):
+        for a in range(3):
+            code |= ((u[:, a] >> b) & 1) << (3 * b + a)
+    return torch.argsort(code, stable=True).to(torch.int32)
+
+
 class WindingNumberTreecode:
     """Treecode operators over a fixed point set (wn_treecode_func.py:3-43)."""
 
-    def __init__(self, points: torch.Tensor, max_tree_depth: int = 15, leaf_size: int = 1):
-        """points: [N, 3] CUDA tensor (float32 or float64)."""
+    def __init__(self, points: torch.Tensor, max_tree_depth: int = 15, leaf_size: int = 1,
+                 far_field: str = "reference", degree: int = 5, theta: float = 0.5,
+                 direct_max: int = 64):
+        """points: [N, 3] CUDA tensor (float32 or float64).  far_field: "reference"
+        (the reference's algorithm, bit-exact decisions) or "interp" (see
+        set_far_field)."""
         assert len(points.shape) == 2
         assert points.shape[1] == 3
         if not points.is_cuda:
@@ -85,6 +111,47 @@ class WindingNumberTreecode:
         self.num_nodes, self.num_leaves = m.value, nl.value
         self.depth, self.n2p_len = d.value, ln.value
         self._layout = None
+        self.far_field = "reference"
+        if far_field != "reference":
+            self.set_far_field(far_field, degree, theta, direct_max)
+
+    def set_far_field(self, mode: str = "interp", degree: int = 5, theta: float = 0.5,
+                      direct_max: int = 64) -> None:
+        """Switches the far-field mode.  "interp": the kernel interpolated on a
+        (degree+1)^3 Chebyshev grid of each node's bounding box, accepted per
+        group of queries when r_node + theta * r_group < theta * distance (so
+        r_node < theta * |x - c| for each query x) and no pair is within a
+        width; near nodes of <= direct_max points summed directly.  "reference": back to the reference's algorithm.  Moments
+        (charges) must be recomputed after a switch."""
+        code = {"reference": _lib.FAR_REFERENCE, "interp": _lib.FAR_INTERP}.get(mode)
+        if code is None:
+            raise RuntimeError(f"unknown far-field mode {mode!r}")
+        with torch.cuda.device(self.device):
+            check(_lib.lib().cagr_tree_set_far_field(self.handle, code, int(degree), float(theta),
+                                                     int(direct_max), _stream(self.device)),
+                  "cagr_tree_set_far_field")
+        self.far_field = mode
+        self.far_degree, self.far_theta, self.far_direct_max = int(degree), float(theta), int(direct_max)
+
+    def far_field_info(self) -> dict:
+        """The tree's far-field mode and parameters, and its number of proxy grids."""
+        mode, deg, dm = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        th, ni = ctypes.c_double(), ctypes.c_int64()
+        check(_lib.lib().cagr_tree_far_field(self.handle, ctypes.byref(mode), ctypes.byref(deg),
+                                             ctypes.byref(th), ctypes.byref(dm), ctypes.byref(ni)),
+              "cagr_tree_far_field")
+        return {"mode": "interp" if mode.value == _lib.FAR_INTERP else "reference",
+                "degree": deg.value, "theta": th.value, "direct_max": dm.value,
+                "proxy_grids": ni.value}
+
+    def query_groups(self) -> torch.Tensor:
+        """Original index of the i-th self-query in processing order (groups of
+        32 consecutive ones walk together), int32 [N]."""
+        out = torch.empty(self.points.shape[0], dtype=torch.int32, device=self.device)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().cagr_tree_query_groups(self.handle, _ptr(out), _stream(self.device)),
+                  "cagr_tree_query_groups")
+        return out
 
     # ---- lifetime -----------------------------------------------------------
     def close(self) -> None:
@@ -188,11 +255,17 @@ class WindingNumberTreecode:
             if query_order.dtype != torch.int32 or query_order.shape != (n,):
                 raise RuntimeError("query_order must be int32 [num_queries]")
             query_order = query_order.contiguous()
+        elif queries is not None and self.far_field == "interp":
+            # the interpolated mode accepts nodes per group of 32 queries: walk
+            # explicit queries in Morton order (outputs stay in the caller's order)
+            query_order = morton_order(queries)
         wt, ws = self._widths(widths, n)
         if out is None:
             if accumulate:
                 raise RuntimeError("accumulate needs an output tensor")
             out = torch.empty(n, OUT_DIM[op], dtype=self.dtype, device=self.device)
+        if n == 0:
+            return out   # no queries (an empty tensor has no device pointer to pass)
         elif (not out.is_cuda or out.dtype != self.dtype or out.shape[0] != n
               or out.dim() != 2 or out.shape[1] < OUT_DIM[op] or out.stride(1) != 1):
             raise RuntimeError(f"out must be a {self.dtype} CUDA tensor [{n}, >= {OUT_DIM[op]}] "

@@ -309,6 +309,62 @@ int cagr_pool_reserved(int64_t* reserved_bytes, int64_t* used_bytes);
  * this off (the default).  Process-wide. */
 int cagr_debug_fail_allocations_after(int64_t n);
 
+/* Far-field modes of a tree (no counterpart in the reference, whose treecode
+ * has the first one only).
+ *
+ * CAGR_FAR_REFERENCE (the default): the reference's algorithm,
+ * wn_treecode_cuda_kernels.cu:556-1322 -- one term per accepted node at its
+ * |attr|-weighted centroid, accepted per query when |x - c|^2 > (4 half_w)^2;
+ * every query sums exactly the reference's pair set (the parity mode).
+ *
+ * CAGR_FAR_INTERP: the same operators with an interpolated far field -- the
+ * pair kernel interpolated in the source position on a (degree+1)^3
+ * Chebyshev grid of each node's bounding box (proxy charges from the node's
+ * points), accepted once per group of queries (32 consecutive ones, split
+ * when they straddle a jump of the curve) when r_node + theta * r_group <
+ * theta * distance -- so r_node < theta * |x - c| for every query x -- and no
+ * pair lies within a query's width; near nodes of at most direct_max points
+ * are summed directly.  Its error against the exact
+ * (direct) sums falls geometrically with the degree.  In this mode
+ * cagr_scatter / cagr_scatter3 compute proxy charges (weights_dev is
+ * ignored: there are no centroids); cagr_multiply, cagr_forward and
+ * cagr_field_grid evaluate A, AT, A3, A21..A23, A2T1..A2T3, G, A2_FUSED,
+ * A2T_SUM, A2T_SUM_SHARED and COUNT; cagr_scatter_export, cagr_adjoint,
+ * cagr_multiply_rhs_window, cagr_b_window_table, CAGR_OP_A2T_RHS and
+ * CAGR_OP_A2_INSIDE return CAGR_ERR_STATE / CAGR_ERR_INVALID.  Explicit
+ * queries should come in a spatially coherent order (query_order_dev: e.g.
+ * Morton order), since the acceptance test is per group of 32. */
+enum { CAGR_FAR_REFERENCE = 0, CAGR_FAR_INTERP = 1 };
+
+/* Sets the far-field mode (degree 1..8, theta in (0, 1), direct_max >= 1 are
+ * used by CAGR_FAR_INTERP only).  Switching to CAGR_FAR_INTERP computes the
+ * nodes' bounding boxes and proxy layout (synchronises `stream`); the
+ * moments / charges must be recomputed after any switch. */
+int cagr_tree_set_far_field(cagr_tree* tree, int mode, int degree, double theta, int direct_max,
+                            void* stream);
+
+/* The current mode and its parameters; num_interp_nodes = nodes with proxy
+ * grids.  Any output may be NULL.  Synchronises the device and returns
+ * CAGR_ERR_CUDA if a walk of the interpolated far field abandoned one of its
+ * bounded waits for the records it stages into shared memory (its outputs are
+ * then incomplete); such a wait is bounded so that no kernel can hang. */
+int cagr_tree_far_field(const cagr_tree* tree, int* mode, int* degree, double* theta,
+                        int* direct_max, int64_t* num_interp_nodes);
+
+/* Test hook (no counterpart in the reference): the number of try_wait rounds
+ * after which a walk of the interpolated far field abandons a staging wait
+ * (default 4194304).  0 makes every walk abandon its first wait at once: it
+ * sets the error flag that cagr_tree_far_field reports, waits for the copies
+ * it has in flight and stops, so the error path can be tested without a
+ * fault. */
+int cagr_debug_interp_wait_limit(cagr_tree* tree, int64_t spin);
+
+/* The order in which self-queries (queries_dev NULL) are processed: order_dev
+ * [n] int32 receives the original index of the i-th one; each consecutive
+ * group of 32 walks the tree together (a 3-D Hilbert order of the points).
+ * No counterpart in the reference (one thread per query there). */
+int cagr_tree_query_groups(const cagr_tree* tree, int32_t* order_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -551,3 +551,263 @@ int oracle_marching_cubes(const float* v, int nx, int ny, int nz, double ox, dou
     free(vbase);
     return 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* The interpolated far-field mode of the library (CAGR_FAR_INTERP), FP64    */
+/* ------------------------------------------------------------------------ */
+
+/* The checker of cagr_b200's second evaluation mode, which has no
+ * counterpart in the reference: the same operators (the exact pair sums of
+ * the pair terms above) with the far field of the barycentric Lagrange
+ * treecode (L. Wang, R. Krasny, S. Tlupova, Commun. Comput. Phys. 28 (2020)):
+ *  - box of a node = the tight bounding box of its points (centre (lo+hi)/2,
+ *    half extents floored at 1e-3 of the largest), radius |half extents|;
+ *  - nodes with >= (p+1)^3 points carry proxy charges
+ *    q_m = sum_j L_a(u_x) L_b(u_y) L_c(u_z) a_j on the tensor grid of
+ *    Chebyshev points of the second kind cos(pi k / p) scaled to the box
+ *    (barycentric Lagrange basis L, weights (-1)^k halved at both ends);
+ *  - queries are processed in groups of 32 (in `order`), split top-down
+ *    into aligned subgroups: a group of 2^k is split when its radius
+ *    exceeds 5 times that of its more compact half (ip_group); a final
+ *    subgroup's batch is the bounding box of its
+ *    queries (centre, radius r_B) and its largest width w_B, walked on its
+ *    own; a node is far when r_C + theta r_B < theta R and
+ *    R >= r_B + r_C + w_B (R = distance of the centres; radii and w_B scaled
+ *    by 1 + 2^-16 as the library scales them); the walk is the preorder of
+ *    the tree: far -> proxy grid (nodes with proxies) or the node's points;
+ *    near leaves and near nodes of <= direct_max points -> their points;
+ *    otherwise the children.
+ * Operators: the ten above plus 10 = A2_FUSED (A21, A22, A23 as three
+ * columns), 11 = A2T_SUM (sum_k A2Tk of the k-th of three scalar columns),
+ * 12 = COUNT (pair terms per query), 13 = A2T_SUM_SHARED (sum_k A2Tk(s)).
+ * kind: 0 = attrs [n,3] vectors, 1 = [n,1] scalars, 2 = [n,3] three scalar
+ * columns.  terms (optional): pair terms per query. */
+enum { OP_A2_FUSED = 10, OP_A2T_SUM = 11, OP_COUNT = 12, OP_A2T_SHARED = 13 };
+
+static void ip_pair(int op, const double* d, const double* a, double w, int cont, double* acc) {
+    switch (op) {
+        case OP_A2_FUSED:
+            pair_f64(OP_A21, d, a, w, cont, acc);
+            pair_f64(OP_A22, d, a, w, cont, acc + 1);
+            pair_f64(OP_A23, d, a, w, cont, acc + 2);
+            break;
+        case OP_A2T_SUM:
+            for (int k = 0; k < 3; k++) pair_f64(OP_A2T1 + k, d, a + k, w, 0, acc);
+            break;
+        case OP_A2T_SHARED:
+            for (int k = 0; k < 3; k++) pair_f64(OP_A2T1 + k, d, a, w, 0, acc);
+            break;
+        case OP_COUNT: break;
+        default: pair_f64(op, d, a, w, cont, acc);
+    }
+}
+
+static void ip_lagrange(double u, int P, const double* t, const double* om, double* L) {
+    for (int k = 0; k < P; k++)
+        if (u == t[k]) {
+            for (int l = 0; l < P; l++) L[l] = l == k ? 1.0 : 0.0;
+            return;
+        }
+    double sum = 0.0;
+    for (int k = 0; k < P; k++) {
+        L[k] = om[k] / (u - t[k]);
+        sum += L[k];
+    }
+    for (int k = 0; k < P; k++) L[k] /= sum;
+}
+
+/* Box of the queries [a, min(b, end)) in `order`: centre c, radius r (half
+ * extents from the farther end, |h| * (1 + 2^-16)), largest width w (NaN ->
+ * inf, scaled alike); r = w = 0 for an empty range. */
+static void ip_group(const double* q, const double* qw, const idx_t* order, idx_t a, idx_t b,
+                     idx_t end, double* c, double* r, double* w) {
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    double wm = 0.0;
+    if (b > end) b = end;
+    for (idx_t k = a; k < b; k++) {
+        const idx_t qi = order ? order[k] : k;
+        for (int x = 0; x < 3; x++) {
+            lo[x] = fmin(lo[x], q[3 * qi + x]);
+            hi[x] = fmax(hi[x], q[3 * qi + x]);
+        }
+        wm = fmax(wm, qw[qi] == qw[qi] ? qw[qi] : INFINITY);
+    }
+    if (!(lo[0] <= hi[0])) {
+        c[0] = c[1] = c[2] = 0.0;
+        *r = *w = 0.0;
+        return;
+    }
+    double h[3];
+    for (int x = 0; x < 3; x++) {
+        c[x] = 0.5 * (lo[x] + hi[x]);
+        h[x] = fmax(hi[x] - c[x], c[x] - lo[x]);
+    }
+    *r = sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]) * (1.0 + 1.0 / 65536);
+    *w = wm * (1.0 + 1.0 / 65536);
+}
+
+int oracle_interp_f64(int op, int cont, const double* q, const double* qw, const idx_t* order,
+                      idx_t nq, const double* pts, const double* attrs, idx_t n, int kind,
+                      const idx_t* children, const unsigned char* is_leaf, const idx_t* npts,
+                      const idx_t* n2p, const idx_t* n2p_start, idx_t M, int degree,
+                      double theta, int direct_max, double* out, idx_t* terms) {
+    (void)n;
+    if (degree < 1 || degree > 8) return -1;
+    const int P = degree + 1, P3 = P * P * P;
+    const int ca = kind == 1 ? 1 : 3;
+    const int co = (op == OP_A || op == OP_A3 || op == OP_A21 || op == OP_A22 || op == OP_A23 ||
+                    op == OP_COUNT) ? 1 : 3;
+    double tch[9], om[9];
+    for (int k = 0; k <= degree; k++) {
+        tch[k] = cos(acos(-1.0) * (double)k / (double)degree);
+        om[k] = ((k & 1) ? -1.0 : 1.0) * ((k == 0 || k == degree) ? 0.5 : 1.0);
+    }
+    double* box = malloc(sizeof(double) * 7 * M);   /* c[3], h[3], r */
+    idx_t* iidx = malloc(sizeof(idx_t) * M);
+    if (!box || !iidx) {
+        free(box);
+        free(iidx);
+        return -1;
+    }
+    idx_t ni = 0;
+    for (idx_t i = 0; i < M; i++) {
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (idx_t j = 0; j < npts[i]; j++) {
+            const double* y = pts + 3 * n2p[n2p_start[i] + j];
+            for (int a = 0; a < 3; a++) {
+                lo[a] = fmin(lo[a], y[a]);
+                hi[a] = fmax(hi[a], y[a]);
+            }
+        }
+        double* b = box + 7 * i;
+        double hmax = 0.0;
+        for (int a = 0; a < 3; a++) {
+            if (!(lo[a] <= hi[a])) lo[a] = hi[a] = 0.0;
+            b[a] = 0.5 * (lo[a] + hi[a]);
+            b[3 + a] = fmax(hi[a] - b[a], b[a] - lo[a]);
+            hmax = fmax(hmax, b[3 + a]);
+        }
+        const double fl = fmax(hmax * 1e-3, 1e-30);
+        for (int a = 0; a < 3; a++) b[3 + a] = fmax(b[3 + a], fl);
+        b[6] = sqrt(b[3] * b[3] + b[4] * b[4] + b[5] * b[5]) * (1.0 + 1.0 / 65536);
+        iidx[i] = npts[i] >= P3 ? ni++ : -1;
+    }
+    /* proxy grids: positions [ni][P3][3], charges [ni][P3][3] */
+    double* ppos = malloc(sizeof(double) * 3 * (size_t)(ni > 0 ? ni : 1) * P3);
+    double* pchg = calloc(3 * (size_t)(ni > 0 ? ni : 1) * P3, sizeof(double));
+    if (!ppos || !pchg) {
+        free(box);
+        free(iidx);
+        free(ppos);
+        free(pchg);
+        return -1;
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (idx_t i = 0; i < M; i++) {
+        if (iidx[i] < 0) continue;
+        const double* b = box + 7 * i;
+        double* pp = ppos + 3 * (size_t)iidx[i] * P3;
+        double* pc = pchg + 3 * (size_t)iidx[i] * P3;
+        for (int m = 0; m < P3; m++) {
+            const int ia = m / (P * P), ib = (m / P) % P, ic = m % P;
+            pp[3 * m] = b[0] + b[3] * tch[ia];
+            pp[3 * m + 1] = b[1] + b[4] * tch[ib];
+            pp[3 * m + 2] = b[2] + b[5] * tch[ic];
+        }
+        for (idx_t j = 0; j < npts[i]; j++) {
+            const idx_t pj = n2p[n2p_start[i] + j];
+            double L[3][9];
+            for (int a = 0; a < 3; a++) {
+                double u = (pts[3 * pj + a] - b[a]) / b[3 + a];
+                u = fmin(fmax(u, -1.0), 1.0);
+                ip_lagrange(u, P, tch, om, L[a]);
+            }
+            const double* aj = attrs + ca * pj;
+            for (int m = 0; m < P3; m++) {
+                const double wgt = L[0][m / (P * P)] * L[1][(m / P) % P] * L[2][m % P];
+                for (int c = 0; c < ca; c++) pc[3 * m + c] += wgt * aj[c];
+            }
+        }
+    }
+    const double th2 = theta * theta;
+    const idx_t ngroups = (nq + 31) / 32;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (idx_t g = 0; g < ngroups; g++) {
+        const idx_t q0 = g * 32, q1 = q0 + 32 < nq ? q0 + 32 : nq;
+        /* each query's group, top-down: the aligned group of 2^k queries is
+         * split when its radius exceeds 5 times that of its more compact half */
+        int kq_of[32];
+        for (idx_t i = q0; i < q1; i++) {
+            int k = 5;
+            while (k > 0) {
+                const idx_t a = q0 + (((i - q0) >> k) << k), h = (idx_t)1 << (k - 1);
+                double c[3], r, r0, r1, w;
+                ip_group(q, qw, order, a, a + 2 * h, q1, c, &r, &w);
+                ip_group(q, qw, order, a, a + h, q1, c, &r0, &w);
+                ip_group(q, qw, order, a + h, a + 2 * h, q1, c, &r1, &w);
+                if (!(r > 5.0 * fmin(r0, r1))) break;
+                k--;
+            }
+            kq_of[i - q0] = k;
+        }
+        double acc[32][3];
+        idx_t cnt[32];
+        memset(acc, 0, sizeof(acc));
+        memset(cnt, 0, sizeof(cnt));
+        for (idx_t sa = q0; sa < q1; sa += (idx_t)1 << kq_of[sa - q0]) {
+            const idx_t sb = sa + ((idx_t)1 << kq_of[sa - q0]) < q1 ? sa + ((idx_t)1 << kq_of[sa - q0]) : q1;
+            double bc[3], br, wm;
+            ip_group(q, qw, order, sa, sb, q1, bc, &br, &wm);
+            idx_t stack[8 * 64];
+            int sp = 0;
+            stack[sp++] = 0;
+            while (sp > 0) {
+                const idx_t nd = stack[--sp];
+                const double* b = box + 7 * nd;
+                const double dx = bc[0] - b[0], dy = bc[1] - b[1], dz = bc[2] - b[2];
+                const double R2 = dx * dx + dy * dy + dz * dz;
+                const double sr = br + b[6], sw = sr + wm, a = b[6] + theta * br;
+                const int far = a * a < th2 * R2 && R2 >= sw * sw;
+                if (far && iidx[nd] >= 0) {
+                    const double* pp = ppos + 3 * (size_t)iidx[nd] * P3;
+                    const double* pc = pchg + 3 * (size_t)iidx[nd] * P3;
+                    for (idx_t kq = sa; kq < sb; kq++) {
+                        const idx_t qi = order ? order[kq] : kq;
+                        for (int m = 0; m < P3; m++) {
+                            const double d[3] = {q[3 * qi] - pp[3 * m], q[3 * qi + 1] - pp[3 * m + 1],
+                                                 q[3 * qi + 2] - pp[3 * m + 2]};
+                            ip_pair(op, d, pc + 3 * m, qw[qi], cont, acc[kq - q0]);
+                        }
+                        cnt[kq - q0] += P3;
+                    }
+                } else if (far || is_leaf[nd] || npts[nd] <= direct_max) {
+                    for (idx_t kq = sa; kq < sb; kq++) {
+                        const idx_t qi = order ? order[kq] : kq;
+                        for (idx_t j = 0; j < npts[nd]; j++) {
+                            const idx_t pj = n2p[n2p_start[nd] + j];
+                            const double d[3] = {q[3 * qi] - pts[3 * pj], q[3 * qi + 1] - pts[3 * pj + 1],
+                                                 q[3 * qi + 2] - pts[3 * pj + 2]};
+                            ip_pair(op, d, attrs + ca * pj, qw[qi], cont, acc[kq - q0]);
+                        }
+                        cnt[kq - q0] += npts[nd];
+                    }
+                } else {
+                    for (int c = 7; c >= 0; c--)
+                        if (children[8 * nd + c] >= 0) stack[sp++] = children[8 * nd + c];
+                }
+            }
+        }
+        for (idx_t kq = q0; kq < q1; kq++) {
+            const idx_t qi = order ? order[kq] : kq;
+            if (op == OP_A3) acc[kq - q0][0] /= 3.0;
+            if (op == OP_COUNT) acc[kq - q0][0] = (double)cnt[kq - q0];
+            for (int j = 0; j < co; j++) out[co * qi + j] = acc[kq - q0][j];
+            if (terms) terms[qi] = cnt[kq - q0];
+        }
+    }
+    free(box);
+    free(iidx);
+    free(ppos);
+    free(pchg);
+    return 0;
+}

@@ -204,6 +204,40 @@ class Oracle:
             raise RuntimeError("oracle direct sum failed")
         return out
 
+    def interp(self, op: str, queries: np.ndarray, widths: np.ndarray, points: np.ndarray,
+               attrs: np.ndarray, tree: Tree, degree: int = 5, theta: float = 0.5,
+               direct_max: int = 64, order: np.ndarray | None = None,
+               continuous: bool = False, kind: str | None = None, counts: bool = False):
+        """The library's interpolated far-field mode (CAGR_FAR_INTERP) in FP64:
+        Chebyshev proxy grids of degree `degree` per node, acceptance per group
+        of 32 queries taken in `order` (oracle_interp_f64 in cagr_oracle.c).
+        op: one of OPS or "A2_FUSED", "A2T_SUM" (attrs [n,3]: three scalar
+        columns), "A2T_SUM_SHARED" (attrs [n,1]), "COUNT"."""
+        code = {**OPS, "A2_FUSED": 10, "A2T_SUM": 11, "COUNT": 12, "A2T_SUM_SHARED": 13}[op]
+        q = np.ascontiguousarray(queries, np.float64)
+        w = np.ascontiguousarray(widths, np.float64)
+        p = np.ascontiguousarray(points, np.float64)
+        a = np.ascontiguousarray(attrs, np.float64).reshape(p.shape[0], -1)
+        if kind is None:
+            kind = "triple" if op == "A2T_SUM" else ("scalar" if a.shape[1] == 1 else "vec")
+        k = {"vec": 0, "scalar": 1, "triple": 2}[kind]
+        nq = q.shape[0]
+        co = 1 if op in ("A", "A3", "A21", "A22", "A23", "COUNT") else 3
+        out = np.zeros((nq, co), np.float64)
+        terms = np.zeros(nq, np.int64)
+        o = None if order is None else np.ascontiguousarray(order, np.int64)
+        f = self.lib.oracle_interp_f64
+        f.restype = ctypes.c_int
+        f.argtypes = [ctypes.c_int, ctypes.c_int, _p, _p, _p, _i64, _p, _p, _i64, ctypes.c_int] + \
+            [_p] * 5 + [_i64, ctypes.c_int, ctypes.c_double, ctypes.c_int, _p, _p]
+        rc = f(code, int(continuous), _ptr(q), _ptr(w), _ptr(o), nq, _ptr(p), _ptr(a), p.shape[0], k,
+               _ptr(tree.children), _ptr(np.ascontiguousarray(tree.is_leaf, np.uint8)),
+               _ptr(tree.npts), _ptr(tree.n2p), _ptr(tree.n2p_start), tree.num_nodes, int(degree),
+               float(theta), int(direct_max), _ptr(out), _ptr(terms))
+        if rc != 0:
+            raise RuntimeError("oracle interpolated traversal failed")
+        return (out, terms) if counts else out
+
     def marching_cubes(self, values: np.ndarray, origin, spacing: float, iso: float,
                        tri: np.ndarray, ntri: np.ndarray):
         """Regular-grid marching cubes with a given case table (the checker of
