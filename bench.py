@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-interp", action="store_true",
+                    help="skip the interpolated far-field mode's leg")
+    ap.add_argument("--interp-degree", type=int, default=5)
     ap.add_argument("--grid", type=int, default=512, help="field grid for the end-to-end run")
     return ap.parse_args()
 
@@ -239,6 +242,86 @@ def run_reference_arm(args, rank: int):
 
 
 # ------------------------------------------------------------------ GPU arm ---
+
+def field_error_sample(p, rng, n_grid=400, n_self=400, grid=512, lo=-1.2, hi=1.2):
+    """Queries for the field error against the FP64 direct sum: random nodes of
+    the reconstruction grid (A3, continuous kernel, width 0.01, as the field
+    evaluation runs) and random input points (the solve's self-queries)."""
+    h = np.float32((hi - lo) / (grid - 1))
+    idx = rng.integers(0, grid, size=(n_grid, 3))
+    qg = (idx.astype(np.float64) * np.float64(h) + np.float64(np.float32(lo))).astype(np.float32)
+    sel = np.sort(rng.choice(p.shape[0], size=n_self, replace=False))
+    return qg, sel
+
+
+def interp_leg(args, P, W, MU, WV, p, widths, mu, dev, stream, flush, rank):
+    import torch
+
+    from cagr_b200 import WindingNumberTreecode
+    from oracle.oracle import Oracle
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    wn = WindingNumberTreecode(P, far_field="interp", degree=args.interp_degree, theta=0.5)
+    out_a = torch.empty(P.shape[0], 3, device=dev)
+    out_t = torch.empty(P.shape[0], 3, device=dev)
+    wn.scatter(MU)
+    terms = float(wn.multiply("COUNT", W).sum().item())
+
+    def step(marks):
+        marks[0].record(stream)
+        wn.scatter(MU)
+        marks[1].record(stream)
+        wn.multiply("A2_FUSED", W, out=out_a)
+        marks[2].record(stream)
+        wn.scatter3(WV)
+        marks[3].record(stream)
+        wn.multiply("A2T_SUM", W, out=out_t)
+        marks[4].record(stream)
+
+    for _ in range(max(1, args.warmup)):
+        step([ev() for _ in range(5)])
+    torch.cuda.synchronize(dev)
+    st, a2, a2t = [], [], []
+    for _ in range(max(3, min(args.steps, 10))):
+        flush.fill_(1.0)
+        m = [ev() for _ in range(5)]
+        step(m)
+        torch.cuda.synchronize(dev)
+        st.append(m[0].elapsed_time(m[4]))
+        a2.append(m[1].elapsed_time(m[2]))
+        a2t.append(m[3].elapsed_time(m[4]))
+    leg = {"degree": args.interp_degree, "theta": 0.5,
+           "proxy_grids": wn.far_field_info()["proxy_grids"],
+           "step_ms": round(float(np.mean(st)), 3),
+           "A2_FUSED_walk_ms": round(float(np.mean(a2)), 3),
+           "A2T_SUM_walk_ms": round(float(np.mean(a2t)), 3),
+           "pair_terms_A2": round(terms), "pair_terms_per_query": round(terms / P.shape[0])}
+    if rank != 0 or args.n > 2_000_000:
+        return leg
+    # the A3 field (continuous kernel, width 0.01) of both modes against the FP64
+    # direct sum, at random reconstruction-grid nodes and at random input points
+    rng = np.random.default_rng(11)
+    qg, sel = field_error_sample(p, rng)
+    o = Oracle()
+    ref_tree = WindingNumberTreecode(P)
+    errs = {}
+    for name, t in (("interp", wn), ("reference_mode", ref_tree)):
+        t.scatter(MU)
+        fg = t.multiply("A3", 0.01, queries=torch.from_numpy(qg).to(dev), continuous=True)
+        fs = t.multiply("A3", 0.01, continuous=True)[torch.from_numpy(sel).to(dev)]
+        errs[name] = (fg.cpu().numpy()[:, 0].astype(np.float64), fs.cpu().numpy()[:, 0].astype(np.float64))
+    dg = o.direct("A3", qg, np.full(len(qg), 0.01), p, mu, continuous=True)[:, 0]
+    ds = o.direct("A3", p[sel], np.full(len(sel), 0.01), p, mu, continuous=True)[:, 0]
+    leg["field_error_vs_fp64_direct"] = {
+        "queries": f"{len(qg)} random nodes of the 512^3 grid over [-1.2, 1.2]^3 and {len(sel)} "
+                   "random input points; A3, continuous kernel, width 0.01",
+        "field_range": [round(float(min(dg.min(), ds.min())), 4), round(float(max(dg.max(), ds.max())), 4)],
+        **{f"max_abs_{k}": float(f"{max(np.abs(v[0] - dg).max(), np.abs(v[1] - ds).max()):.3e}")
+           for k, v in errs.items()},
+    }
+    ref_tree.close()
+    wn.close()
+    return leg
+
 
 def run_ours(args, rank: int, world: int, local_rank: int):
     import ctypes
@@ -449,6 +532,13 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                                "third-order step (within 2 ulp of CUDA's rsqrt(double))")
             del rec
 
+    # the interpolated far-field mode: the same step with the far field
+    # interpolated on Chebyshev proxy grids (degree --interp-degree, theta 0.5),
+    # and the field error of both modes against the FP64 direct sum
+    interp = None
+    if not args.no_interp:
+        interp = interp_leg(args, P, W, MU, WV, p, widths, mu, dev, stream, flush, rank)
+
     # measured FP32 FMA peak (roofline denominator)
     gf = ctypes.c_double()
     _lib.check(_lib.lib().cagr_probe_fp32_peak(20000, ctypes.byref(gf),
@@ -456,6 +546,13 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                "cagr_probe_fp32_peak")
     peak_tflops = gf.value / 1e3
 
+    if interp is not None:
+        # FP32 work of the interpolated walks (the same flops per pair term as the
+        # reference-mode walks; a proxy term is a point term)
+        ta = interp["pair_terms_A2"] * FLOPS_A2_FUSED / (interp["A2_FUSED_walk_ms"] * 1e-3) / 1e12
+        tt = interp["pair_terms_A2"] * FLOPS_A2T / (interp["A2T_SUM_walk_ms"] * 1e-3) / 1e12
+        interp["A2_FUSED_tflops"], interp["A2_FUSED_fp32_frac"] = round(ta, 3), round(ta / peak_tflops, 4)
+        interp["A2T_SUM_tflops"], interp["A2T_SUM_fp32_frac"] = round(tt, 3), round(tt / peak_tflops, 4)
     T, E = max_over_ranks([float(np.mean(step_ms)), float(np.mean(e2e_ms))], world, dev)
     if rank != 0:
         return
@@ -503,6 +600,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "pair_terms": {"A2_FUSED": round(terms_a2), "A2T1": round(terms_t[0]),
                        "A2T2": round(terms_t[1]), "A2T3": round(terms_t[2])},
         "fp64_ms_per_step": None if fp64_ms is None else round(fp64_ms, 3),
+        "interp": interp,
         "end_to_end": solve,
         "end_to_end_fp64": solve64,
         "end_to_end_fp64_over_fp32": (round(solve64["total_s"] / solve["total_s"], 3)

@@ -28,6 +28,7 @@ FAR_REFERENCE, FAR_INTERP = 0, 1
 # multiply flags
 FLAG_CONTINUOUS = 1
 FLAG_ACCUMULATE = 2
+FLAG_NEGATE = 4
 ATTR_DIM = {"A": 3, "AT": 1, "A3": 3, "A21": 3, "A22": 3, "A23": 3, "A2T1": 1, "A2T2": 1,
             "A2T3": 1, "G": 3, "A2_FUSED": 3, "A2T_SUM": 3, "A2T_SUM_SHARED": 1, "A2_INSIDE": 3,
             "A2T_RHS": 3}
@@ -52,6 +53,7 @@ _SIGNATURES = {
     "cagr_tree_morton_order": (_i32, [_p, _p, _p]),
     "cagr_scatter": (_i32, [_p, _i32, _p, _i32, _p, _p]),
     "cagr_scatter3": (_i32, [_p, _p, _p]),
+    "cagr_scatter_import": (_i32, [_p, _i32, _p, _p, _p, _i32, _p]),
     "cagr_scatter_export": (_i32, [_p, _i32, _p, _p, _p, _p]),
     "cagr_multiply": (_i32, [_p, _i32, _p, _p, _i64, _p, ctypes.c_double, _i32, _p, _i64, _p]),
     "cagr_forward": (_i32, [_p, _i32, _p, _p, ctypes.c_double, _i32, _p, _p]),

@@ -17,6 +17,9 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libcagr_b200.so")
+BIN_DIR = os.path.join(PKG, "bin")
+# the GaussRecon driver on the C ABI (cli/main_gaussrecon.cpp), linked to the library
+GAUSSRECON_PATH = os.path.join(BIN_DIR, "main_GaussReconCUDA")
 SOURCES = ["capi.cu", "tree_build.cu", "moments.cu", "traverse.cu", "diagnostics.cu",
            "noalloc.cu", "mcubes.cu", "memory.cu", "interp.cu"]
 HEADERS = ["common.cuh", "internal.h"]
@@ -36,6 +39,9 @@ def _stale() -> bool:
     t = os.path.getmtime(LIB_PATH)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
     deps.append(os.path.join(ROOT, "include", "cagr.h"))
+    deps.append(os.path.join(PKG, "cli", "main_gaussrecon.cpp"))
+    if not os.path.exists(GAUSSRECON_PATH):
+        return True
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
@@ -61,7 +67,23 @@ def build(force: bool = False, verbose: bool = False) -> str:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)
     os.replace(tmp, LIB_PATH)
+    build_gaussrecon(verbose)
     return LIB_PATH
+
+
+def build_gaussrecon(verbose: bool = False) -> str:
+    """The C++ main_GaussReconCUDA, linked to libcagr_b200.so (found next to it
+    through its rpath: ../lib)."""
+    os.makedirs(BIN_DIR, exist_ok=True)
+    tmp = GAUSSRECON_PATH + ".tmp"
+    cmd = [nvcc(), *ARCH, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"),
+           os.path.join(PKG, "cli", "main_gaussrecon.cpp"), "-o", tmp, "-L", LIB_DIR, "-lcagr_b200",
+           "-Xlinker", "-rpath=$ORIGIN/../lib"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+    os.replace(tmp, GAUSSRECON_PATH)
+    return GAUSSRECON_PATH
 
 
 if __name__ == "__main__":

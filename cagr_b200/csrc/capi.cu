@@ -140,6 +140,15 @@ int cagr_scatter(cagr_tree* tree, int slot, const void* attrs_dev, int attr_dim,
     return cagr::moments(tree->t, slot, attrs_dev, attr_dim, weights_dev, as_stream(stream));
 }
 
+int cagr_scatter_import(cagr_tree* tree, int slot, const void* node_attrs_dev,
+                        const void* reppoints_dev, const void* attrs_dev, int attr_dim,
+                        void* stream) {
+    if (int rc = check_tree(tree)) return rc;
+    if (int rc = reference_mode_only(tree, "cagr_scatter_import")) return rc;
+    return cagr::moments_import(tree->t, slot, node_attrs_dev, reppoints_dev, attrs_dev, attr_dim,
+                                as_stream(stream));
+}
+
 int cagr_scatter3(cagr_tree* tree, const void* values3_dev, void* stream) {
     if (int rc = check_tree(tree)) return rc;
     if (tree->t->interp) return cagr::interp_scatter(tree->t, 3, values3_dev, 3, as_stream(stream));
@@ -159,7 +168,7 @@ int cagr_multiply(const cagr_tree* tree, int op, const void* queries_dev,
                   double width, int flags, void* out_dev, int64_t out_stride, void* stream) {
     if (int rc = check_tree(tree)) return rc;
     if (op_attr_dim(op) == 0) return set_error(CAGR_ERR_INVALID, "unknown operator");
-    if (flags & ~(CAGR_FLAG_CONTINUOUS | CAGR_FLAG_ACCUMULATE))
+    if (flags & ~(CAGR_FLAG_CONTINUOUS | CAGR_FLAG_ACCUMULATE | CAGR_FLAG_NEGATE))
         return set_error(CAGR_ERR_INVALID, "unknown flag bits");
     if (out_stride < 0 || out_stride > (1 << 20))
         return set_error(CAGR_ERR_INVALID, "out_stride out of range");
@@ -171,6 +180,7 @@ int cagr_multiply(const cagr_tree* tree, int op, const void* queries_dev,
     }
     a.continuous = (flags & CAGR_FLAG_CONTINUOUS) ? 1 : 0;
     a.accumulate = (flags & CAGR_FLAG_ACCUMULATE) ? 1 : 0;
+    a.negate = (flags & CAGR_FLAG_NEGATE) ? 1 : 0;
     a.queries = queries_dev;
     a.qorder = query_order_dev;
     a.nq = nq;
@@ -232,12 +242,13 @@ int cagr_field_grid(const cagr_tree* tree, int op, int nx, int ny, int nz,
         op == CAGR_OP_A2T_RHS)
         return set_error(CAGR_ERR_INVALID, "unsupported operator for grid queries");
     if (!origin) return set_error(CAGR_ERR_INVALID, "origin is null");
-    if (flags & ~(CAGR_FLAG_CONTINUOUS | CAGR_FLAG_ACCUMULATE))
+    if (flags & ~(CAGR_FLAG_CONTINUOUS | CAGR_FLAG_ACCUMULATE | CAGR_FLAG_NEGATE))
         return set_error(CAGR_ERR_INVALID, "unknown flag bits");
     cagr::TraverseArgs a;
     a.op = op;
     a.continuous = (flags & CAGR_FLAG_CONTINUOUS) ? 1 : 0;
     a.accumulate = (flags & CAGR_FLAG_ACCUMULATE) ? 1 : 0;
+    a.negate = (flags & CAGR_FLAG_NEGATE) ? 1 : 0;
     a.grid = 1;
     a.gx = nx;
     a.gy = ny;

@@ -86,6 +86,10 @@ int moments(Tree* t, int slot, const void* attrs, int dim, const void* weights,
 // Three scalar attributes at once (values3: [N, 3], column k -> slot k, weights |v_k|):
 // the node moments of the reference's three A2Tk calls, in one launch.
 int moments3(Tree* t, const void* values3, cudaStream_t stream);
+// The records of slot `slot` from moments given in the reference layout
+// (node_attrs [M, dim], reppoints [M, 3]) and point attributes [N, dim].
+int moments_import(Tree* t, int slot, const void* node_attrs, const void* reppoints,
+                   const void* attrs, int dim, cudaStream_t stream);
 // Copy node moments of a slot out in the reference layout:
 // node_attrs [M, dim], reppoints [M, 3], weights [M].
 int moments_export(const Tree* t, int slot, void* node_attrs, void* reppoints, void* weights,
@@ -113,6 +117,7 @@ struct TraverseArgs {
     int op = 0;
     int continuous = 0;
     int accumulate = 0;
+    int negate = 0;                    // write (or add) -op
     int slots = 1;                     // kOpA2TFused: 3 = slot k holds s_k, 1 = shared slot 0
     const void* queries = nullptr;     // [nq, 3] T or null (= the tree's points)
     const int32_t* qorder = nullptr;   // [nq] processing order or null

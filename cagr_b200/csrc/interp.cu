@@ -57,6 +57,26 @@ constexpr int kPMax = 9;          // degree <= 8
 constexpr int kChunk = 2048;      // points per proxy-charge block
 constexpr int kRec = 12;          // scalars per point / proxy record
 constexpr unsigned kAll = 0xffffffffu;
+// the pipelined walk's shape (see k_iwalk)
+#ifndef CAGR_IW_SLOTS
+#define CAGR_IW_SLOTS 3
+#endif
+#ifndef CAGR_IW_TILE
+#define CAGR_IW_TILE 3072
+#endif
+#ifndef CAGR_IW_WARPS
+#define CAGR_IW_WARPS 4
+#endif
+#ifndef CAGR_IW_UNROLL
+#define CAGR_IW_UNROLL 4
+#endif
+constexpr int kSlots = CAGR_IW_SLOTS;       // tiles in flight per warp
+constexpr int kTileBytes = CAGR_IW_TILE;    // per tile (3072: 64 float / 32 double records)
+// (measured at 1M points, A2_FUSED / A2T_SUM walk: 4 slots, unroll 2: 43.3 / 53.1 ms;
+// 3 slots: 40.2 / 46.0; unroll 4: 40.6 / 48.4; 2048-byte tiles: 42.6 / 51.6;
+// 3 slots and unroll 4: 38.0 / 45.8 ms)
+constexpr int kPWarps = CAGR_IW_WARPS;      // warps per block
+constexpr int kUnroll = CAGR_IW_UNROLL;     // pair terms per inner-loop iteration
 // internal operator codes beside Op: the A2T sums of the interpolated mode
 constexpr int kIOpA2TSum = 100;     // sum_k A2Tk(s_k), three scalar columns (slot 3)
 constexpr int kIOpA2TShared = 101;  // sum_k A2Tk(s), one scalar column
@@ -472,11 +492,12 @@ __device__ __forceinline__ void irange(const IQ<T>& q, bool active, const T* __r
                                        int count, T* s, T* cmp, T* in) {
     T p0 = T(0), p1 = T(0), p2 = T(0), i0 = T(0), i1 = T(0), i2 = T(0);
     int j = 0;
-    for (; j + 1 < count; j += 2) {
-        iterm<T, OP, CONT, NEAR>(q, r + (int64_t)j * kRec, p0, p1, p2, i0, i1, i2);
-        iterm<T, OP, CONT, NEAR>(q, r + (int64_t)(j + 1) * kRec, p0, p1, p2, i0, i1, i2);
+    for (; j + kUnroll <= count; j += kUnroll) {
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++)
+            iterm<T, OP, CONT, NEAR>(q, r + (int64_t)(j + u) * kRec, p0, p1, p2, i0, i1, i2);
     }
-    if (j < count) iterm<T, OP, CONT, NEAR>(q, r + (int64_t)j * kRec, p0, p1, p2, i0, i1, i2);
+    for (; j < count; j++) iterm<T, OP, CONT, NEAR>(q, r + (int64_t)j * kRec, p0, p1, p2, i0, i1, i2);
     if (!active) return;
     if constexpr (OP == kOpCount) {
         s[0] += p0;
@@ -543,9 +564,11 @@ __device__ __forceinline__ bool iload(const IWalk<T>& p, int64_t qi, IQ<T>& q, i
     return valid;
 }
 
+// mode bit 0: add into the output; bit 1: write -op
 template <typename T>
-__device__ __forceinline__ void iput(T* o, int j, T v, int accumulate) {
-    o[j] = accumulate ? o[j] + v : v;
+__device__ __forceinline__ void iput(T* o, int j, T v, int mode) {
+    const T u = (mode & 2) ? -v : v;
+    o[j] = (mode & 1) ? o[j] + u : u;
 }
 
 // A batch of queries: bounding centre, radius and largest width.
@@ -630,9 +653,6 @@ __device__ __forceinline__ Batch<T> lane_batch(const IQ<T>& q, bool valid, T w, 
 // the others.  Every wait is bounded: a wait that runs out sets the error
 // flag, waits (bounded again) for the warp's copies still in flight and ends
 // the warp.
-constexpr int kSlots = 4;            // tiles in flight per warp
-constexpr int kTileBytes = 3072;     // per tile: 64 float records, 32 double records
-constexpr int kPWarps = 4;           // warps per block
 constexpr uint32_t kDrainSpin = 1u << 24;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -1040,7 +1060,7 @@ int traverse_impl(const Tree* t, const Interp* I, const TraverseArgs& a, cudaStr
     p.widths = (const T*)a.widths;
     p.width = (T)a.width;
     p.out = (T*)a.out;
-    p.accumulate = a.accumulate;
+    p.accumulate = (a.accumulate ? 1 : 0) | (a.negate ? 2 : 0);
     p.err = I->err;
     p.spin = I->spin;
     // which slot and attribute dim the operator reads

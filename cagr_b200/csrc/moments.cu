@@ -382,7 +382,70 @@ int launch_moments3(Tree* t, const void* values3, cudaStream_t s) {
     return kOk;
 }
 
+
+// Records of slot from moments given in the reference layout -- node_attrs
+// [M, DIM] and reppoints [M, 3] as scatter_point_attrs_to_nodes returns them,
+// and the point attributes [N, DIM] -- exactly as the moment pass writes them
+// from the same values (node weights are not carried: no traversal reads them).
+template <typename T, int DIM>
+__global__ void k_import(const int4* __restrict__ meta, const T* __restrict__ spos,
+                         const int32_t* __restrict__ perm, int64_t M, int64_t N,
+                         const T* __restrict__ node_attrs, const T* __restrict__ rep,
+                         const T* __restrict__ attrs, T* __restrict__ rec) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < M) {
+        const int4 mt = meta[i];
+        const T c[3] = {rep[3 * i], rep[3 * i + 1], rep[3 * i + 2]};
+        T e[3], a[3] = {T(0), T(0), T(0)};
+        exps(c, e);
+        for (int d = 0; d < DIM; d++) a[d] = node_attrs[i * DIM + d];
+        T r0w = mac_radius2<T>(node_depth(mt));
+        if (node_npts(mt) == 1) {
+            const int64_t s = mt.y;
+            if (c[0] == spos[3 * s] && c[1] == spos[3 * s + 1] && c[2] == spos[3 * s + 2])
+                r0w = -r0w;
+        }
+        write_record<T, DIM>(rec + i * CAGR_REC_STRIDE, c, e, a, T(0), r0w);
+    } else if (i < M + N) {
+        const int64_t s = i - M;
+        const int64_t pt = perm[s];
+        const T pos[3] = {spos[3 * s], spos[3 * s + 1], spos[3 * s + 2]};
+        T e[3], a[3] = {T(0), T(0), T(0)};
+        exps(pos, e);
+        for (int d = 0; d < DIM; d++) a[d] = attrs[pt * DIM + d];
+        write_record<T, DIM>(rec + i * CAGR_REC_STRIDE, pos, e, a, weight_of(a, DIM), T(0));
+    }
+}
+
+template <typename T>
+int launch_import(Tree* t, int slot, const void* node_attrs, const void* rep, const void* attrs,
+                  int dim, cudaStream_t s) {
+    if (int rc = ensure_slot(t, slot, sizeof(T), s)) return rc;
+    const int64_t total = t->m + t->n;
+    const unsigned grid = (unsigned)((total + kBlock - 1) / kBlock);
+    if (dim == 3)
+        k_import<T, 3><<<grid, kBlock, 0, s>>>(t->meta, (const T*)t->spos, t->perm, t->m, t->n,
+                                               (const T*)node_attrs, (const T*)rep,
+                                               (const T*)attrs, (T*)t->rec[slot]);
+    else
+        k_import<T, 1><<<grid, kBlock, 0, s>>>(t->meta, (const T*)t->spos, t->perm, t->m, t->n,
+                                               (const T*)node_attrs, (const T*)rep,
+                                               (const T*)attrs, (T*)t->rec[slot]);
+    CAGR_CUDA(cudaGetLastError());
+    t->rec_dim[slot] = dim;
+    t->slot_adj[slot] = false;
+    return kOk;
+}
 }  // namespace
+
+int moments_import(Tree* t, int slot, const void* node_attrs, const void* reppoints,
+                   const void* attrs, int dim, cudaStream_t stream) {
+    if (slot < 0 || slot > 2) return set_error(kErrInvalid, "moment slot must be 0, 1 or 2");
+    if (dim != 1 && dim != 3) return set_error(kErrInvalid, "attribute dim must be 1 or 3");
+    if (!node_attrs || !reppoints || !attrs) return set_error(kErrInvalid, "null buffer");
+    return t->dtype == 0 ? launch_import<float>(t, slot, node_attrs, reppoints, attrs, dim, stream)
+                         : launch_import<double>(t, slot, node_attrs, reppoints, attrs, dim, stream);
+}
 
 int moments(Tree* t, int slot, const void* attrs, int dim, const void* weights,
             cudaStream_t stream) {

@@ -72,15 +72,16 @@ struct TravParams {
     T gox = T(0), goy = T(0), goz = T(0), gh = T(0);
     T* out = nullptr;
     int out_stride = 1;
-    int accumulate = 0;  // add into `out` instead of overwriting it
+    int accumulate = 0;  // bit 0: add into `out` instead of overwriting it; bit 1: write -op
     const T* g = nullptr;  // adjoint: d loss / d out per query [nq, 3], original order
     T* accn = nullptr;     // adjoint: per-node accumulators [M, 3]
     T* accp = nullptr;     // adjoint: per-point accumulators [N, 3], Morton order
 };
 
 template <typename T>
-__device__ __forceinline__ void put(T* o, int j, T v, int accumulate) {
-    o[j] = accumulate ? o[j] + v : v;
+__device__ __forceinline__ void put(T* o, int j, T v, int mode) {
+    const T u = (mode & 2) ? -v : v;
+    o[j] = (mode & 1) ? o[j] + u : u;
 }
 
 template <int OP>
@@ -774,7 +775,7 @@ int dispatch(const Tree* t, const TraverseArgs& a, cudaStream_t s) {
     p.width = (T)a.width;
     p.widths_hi = (const T*)a.widths_hi;
     p.out = (T*)a.out;
-    p.accumulate = a.accumulate;
+    p.accumulate = (a.accumulate ? 1 : 0) | (a.negate ? 2 : 0);
     const bool scalar_in = a.op == kOpAT || a.op == kOpA2T1 || a.op == kOpA2T2 ||
                            a.op == kOpA2T3 || a.op == kOpA2TFused;
     const int slots = a.op == kOpA2TFused ? a.slots : 1;

@@ -87,7 +87,9 @@ enum {
 /* cagr_multiply / cagr_forward flags. */
 enum {
     CAGR_FLAG_CONTINUOUS = 1, /* the reference's continuous_kernel argument (A, A3, A2x) */
-    CAGR_FLAG_ACCUMULATE = 2  /* add into out_dev instead of overwriting it */
+    CAGR_FLAG_ACCUMULATE = 2, /* add into out_dev instead of overwriting it */
+    CAGR_FLAG_NEGATE = 4      /* write (or add) -op: the GaussRecon driver's grid value -A3
+                                 (main_GaussRecon_cuda.cu:478); cagr_multiply, cagr_field_grid */
 };
 
 /* Library identification. */
@@ -132,6 +134,18 @@ int cagr_tree_morton_order(const cagr_tree* tree, int32_t* perm_dev, void* strea
  * the reference kernels :419-553 evaluated in IEEE arithmetic. */
 int cagr_scatter(cagr_tree* tree, int slot, const void* attrs_dev, int attr_dim,
                  const void* weights_dev, void* stream);
+
+/* Loads node moments given in the reference layout into record slot `slot`
+ * (0..2): node_attrs_dev [M, attr_dim] and reppoints_dev [M, 3] as
+ * scatter_point_attrs_to_nodes returns them (node ids = the reference's
+ * preorder ids, which are this tree's), and the point attributes attrs_dev
+ * [n, attr_dim] (original order).  The reference's multiply_by_* take these
+ * arrays as arguments (wn_treecode_cuda_torch_interface.cu:137-777): this is
+ * how a caller holding them evaluates with them.  With the moments of
+ * cagr_scatter_export the records are those of cagr_scatter (same bits). */
+int cagr_scatter_import(cagr_tree* tree, int slot, const void* node_attrs_dev,
+                        const void* reppoints_dev, const void* attrs_dev, int attr_dim,
+                        void* stream);
 
 /* Node moments of three scalar attributes at once: column k of values3_dev
  * ([n,3], original point order) is scattered with weights |v_k| -- the three

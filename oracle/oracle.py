@@ -30,7 +30,20 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_LIB_PATH = os.path.join(HERE, "_ref", "libwnref.so")
-REF_ROOT = os.environ.get("CAGR_REFERENCE_ROOT", "/root/reference")
+def _reference_root() -> str | None:
+    """The reference checkout to compile from: $CAGR_REFERENCE_ROOT, else the
+    one the build recipe (oracle/Makefile) names; None when neither exists."""
+    root = os.environ.get("CAGR_REFERENCE_ROOT")
+    if not root:
+        try:
+            root = subprocess.run(["make", "-s", "-C", HERE, "ref-root"], capture_output=True,
+                                  text=True, timeout=30).stdout.strip()
+        except (OSError, subprocess.SubprocessError):
+            root = None
+    return root if root and os.path.isdir(root) else None
+
+
+REF_ROOT = _reference_root()
 
 # Operator codes shared by both libraries.
 OPS = {"A": 0, "AT": 1, "A3": 2, "A21": 3, "A22": 4, "A23": 5,
@@ -50,10 +63,10 @@ def build_oracle(force: bool = False) -> None:
     if force or not os.path.exists(LIB_PATH) or (
             os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, "cagr_oracle.c"))):
         subprocess.check_call(["make", "-s", "-C", HERE, "all"])
-    if os.path.isdir(REF_ROOT) and (force or not os.path.exists(REF_LIB_PATH)):
+    if REF_ROOT and (force or not os.path.exists(REF_LIB_PATH)):
         subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF_ROOT={REF_ROOT}"])
     gpu_lib = os.path.join(HERE, "_ref", "libwnref_gpu.so")
-    if os.path.isdir(REF_ROOT) and (force or not os.path.exists(gpu_lib)):
+    if REF_ROOT and (force or not os.path.exists(gpu_lib)):
         subprocess.check_call(["make", "-s", "-C", HERE, "ref-gpu", f"REF_ROOT={REF_ROOT}"])
 
 

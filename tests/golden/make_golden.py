@@ -24,10 +24,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from oracle.oracle import OPS, RefOracle, point_weights  # noqa: E402
+from oracle.oracle import OPS, REF_ROOT, RefOracle, point_weights  # noqa: E402
 from tests._cases import edge_cloud, random_values, smooth_normals, sphere_cloud  # noqa: E402
 
-REF_ROOT = os.environ.get("CAGR_REFERENCE_ROOT", "/root/reference")
+if REF_ROOT is None:
+    sys.exit("make_golden.py reads the reference checkout: set CAGR_REFERENCE_ROOT "
+             "(or REF_ROOT in oracle/Makefile)")
 
 CASES = {
     # name: (points factory, max_depth, leaf_size, run operators)

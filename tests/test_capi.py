@@ -66,3 +66,35 @@ def test_no_cpu_fallback_in_the_product():
             if f.endswith(".py"):
                 text = open(os.path.join(root, f)).read()
                 assert "import oracle" not in text and "from oracle" not in text, f
+
+
+def test_reference_extension_names_are_served():
+    """Every function the reference's operator object calls on its extension
+    modules (wn_treecode_func.py, read with ast where a checkout is given by
+    CAGR_REFERENCE_ROOT; else the pybind tables' names) exists in
+    cagr_b200._cuda / cagr_b200._cpu."""
+    import ast
+    import os
+
+    from cagr_b200 import _cpu, _cuda
+    names = {"scatter_point_attrs_to_nodes", "multiply_by_A", "multiply_by_A3", "multiply_by_AT",
+             "multiply_by_G", "multiply_by_A2", "multiply_by_A21", "multiply_by_A22",
+             "multiply_by_A23", "multiply_by_A2T1", "multiply_by_A2T2", "multiply_by_A2T3"}
+    root = os.environ.get("CAGR_REFERENCE_ROOT")
+    if root:
+        src = open(os.path.join(root, "CUDA-based", "ext", "wn_treecode",
+                                "wn_treecode_func.py")).read()
+        called = {}
+        for node in ast.walk(ast.parse(src)):
+            if isinstance(node, ast.Call) and isinstance(node.func, ast.Attribute):
+                base = node.func.value
+                if isinstance(base, ast.Attribute) and base.attr == "treecode_package":
+                    called[node.func.attr] = len(node.args)
+        assert called, "no treecode_package calls found"
+        for name, nargs in called.items():
+            assert hasattr(_cuda, name), name
+            assert nargs == (10 if name == "scatter_point_attrs_to_nodes" else 12), name
+        names |= set(called)
+    for name in names:
+        assert callable(getattr(_cuda, name)), name
+    assert callable(_cpu.build_tree)
