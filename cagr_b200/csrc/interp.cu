@@ -98,6 +98,16 @@ struct Interp {
     double cheb[kPMax] = {}, omega[kPMax] = {};  // Chebyshev points and barycentric weights
     int* err = nullptr;            // device flag: a walk's staging wait ran out
     uint32_t spin = 1u << 22;      // try_wait rounds before a staging wait runs out
+    // Self-query walks run their groups longest first: each walk records every
+    // group's cost (tiles summed), and the groups are sorted by it for the next.
+    int64_t ngroups = 0;
+    uint32_t* gcost = nullptr;     // [ngroups] tiles of each group in the last self walk
+    uint32_t* gcost_sorted = nullptr;
+    int32_t* giota = nullptr;      // [ngroups] 0, 1, 2, ...
+    int32_t* gorder = nullptr;     // [ngroups] groups, most expensive first
+    void* gsort_tmp = nullptr;
+    size_t gsort_bytes = 0;
+    bool gorder_valid = false;
 };
 
 namespace {
@@ -371,6 +381,8 @@ struct IWalk {
     int out_stride = 1;
     int accumulate = 0;
     unsigned long long* counter = nullptr;  // next group of 32 queries (persistent launch)
+    const int32_t* gorder = nullptr;        // the order groups are taken in (null: their own)
+    uint32_t* gcost = nullptr;              // tiles summed per group, when non-null
     int* err = nullptr;                     // set when a staging wait runs out
     uint32_t spin = 0;                      // try_wait rounds before a wait runs out
 };
@@ -725,16 +737,21 @@ __global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
     const int M = (int)p.M;
     const int64_t ngroups = (p.nq + 31) / 32;
     for (;;) {
-        unsigned long long grp = 0;
-        if (lane == 0) grp = atomicAdd(p.counter, 1ull);
-        grp = __shfl_sync(kAll, grp, 0);
-        if ((int64_t)grp >= ngroups) break;
-        const int64_t qi = (int64_t)grp * 32 + lane;
+        unsigned long long ticket = 0;
+        if (lane == 0) ticket = atomicAdd(p.counter, 1ull);
+        ticket = __shfl_sync(kAll, ticket, 0);
+        if ((int64_t)ticket >= ngroups) break;
+        const int64_t grp = p.gorder ? (int64_t)__ldg(p.gorder + ticket) : (int64_t)ticket;
+        uint32_t ntiles = 0;  // this group's tiles (its cost, for the next walk's order)
+        const int64_t qi = grp * 32 + lane;
         IQ<T> q;
         int64_t oidx;
         T w;
         const bool valid = iload(p, qi, q, oidx, w);
-        if (__all_sync(kAll, !valid)) continue;  // grid lanes outside the grid
+        if (__all_sync(kAll, !valid)) {  // grid lanes outside the grid
+            if (p.gcost && lane == 0) p.gcost[grp] = 0;
+            continue;
+        }
         if constexpr (IOp<OP>::query_exp) {
             q.ex0 = exp_t(q.x * T(0.5));
             q.ex1 = exp_t(q.y * T(0.5));
@@ -831,9 +848,11 @@ __global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
                 __syncwarp();  // every lane has read the slot before it is refilled
                 head = (head + 1) % kSlots;
                 inflight--;
+                ntiles++;
             }
             g = gnext;
         }
+        if (p.gcost && lane == 0) p.gcost[grp] = ntiles;
         if (!valid) continue;
         T* o = p.out + oidx * (int64_t)p.out_stride;
         const int acc = p.accumulate;
@@ -1029,7 +1048,12 @@ int scatter_impl(Tree* t, Interp* I, int slot, const void* attrs, int dim, cudaS
 }
 
 template <typename T>
-int traverse_impl(const Tree* t, const Interp* I, const TraverseArgs& a, cudaStream_t s) {
+int ensure_group_order(const Tree* t, Interp* I, cudaStream_t s);
+template <typename T>
+int launch_walk(const IWalk<T>& p, int op, int c, cudaStream_t s);
+
+template <typename T>
+int traverse_impl(const Tree* t, Interp* I, const TraverseArgs& a, cudaStream_t s) {
     IWalk<T> p;
     p.M = t->m;
     p.nq = a.queries ? a.nq : t->n;
@@ -1084,7 +1108,50 @@ int traverse_impl(const Tree* t, const Interp* I, const TraverseArgs& a, cudaStr
                          op == kOpA23 || op == kOpCount) ? 1 : 3;
     p.out_stride = a.out_stride > 0 ? a.out_stride : out_dim;
     if (p.nq == 0) return kOk;
-    const int c = a.continuous;
+    const bool self = !a.queries && !a.grid;
+    if (self) {
+        if (int rc = ensure_group_order<T>(t, I, s)) return rc;
+        p.gorder = I->gorder_valid ? I->gorder : nullptr;
+        p.gcost = I->gcost;
+    }
+    const int rc = launch_walk<T>(p, op, a.continuous, s);
+    if (rc || !self) return rc;
+    // the next self walk takes the groups longest first (same outputs: a query's
+    // sum does not depend on the warp that walks it)
+    CAGR_CUDA(cub::DeviceRadixSort::SortPairsDescending(I->gsort_tmp, I->gsort_bytes, I->gcost,
+                                                        I->gcost_sorted, I->giota, I->gorder,
+                                                        (int)I->ngroups, 0, 32, s));
+    I->gorder_valid = true;
+    return kOk;
+}
+
+__global__ void k_iota(int32_t* a, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = (int32_t)i;
+}
+
+// The self-query groups' cost and order arrays (once per tree).
+template <typename T>
+int ensure_group_order(const Tree* t, Interp* I, cudaStream_t s) {
+    if (I->gcost) return kOk;
+    const int64_t G = (t->n + 31) / 32;
+    if (int rc = pool_alloc((void**)&I->gcost, sizeof(uint32_t) * G, s)) return rc;
+    if (int rc = pool_alloc((void**)&I->gcost_sorted, sizeof(uint32_t) * G, s)) return rc;
+    if (int rc = pool_alloc((void**)&I->giota, sizeof(int32_t) * G, s)) return rc;
+    if (int rc = pool_alloc((void**)&I->gorder, sizeof(int32_t) * G, s)) return rc;
+    size_t bytes = 0;
+    CAGR_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, I->gcost, I->gcost_sorted,
+                                                        I->giota, I->gorder, (int)G, 0, 32, s));
+    if (int rc = pool_alloc(&I->gsort_tmp, bytes > 0 ? bytes : 1, s)) return rc;
+    I->gsort_bytes = bytes;
+    k_iota<<<blocks_for(G, 256), 256, 0, s>>>(I->giota, G);
+    CAGR_CUDA(cudaGetLastError());
+    I->ngroups = G;
+    return kOk;
+}
+
+template <typename T>
+int launch_walk(const IWalk<T>& p, int op, int c, cudaStream_t s) {
     switch (op) {
         case kOpA: return ilaunch_cont<T, kOpA>(p, c, s);
         case kOpA3: return ilaunch_cont<T, kOpA3>(p, c, s);
@@ -1101,7 +1168,7 @@ int traverse_impl(const Tree* t, const Interp* I, const TraverseArgs& a, cudaStr
         case kIOpA2TShared: return ilaunch<T, kIOpA2TShared, false>(p, s);
         case kOpCount: return ilaunch<T, kOpCount, false>(p, s);
         default:
-            return set_error(kErrInvalid, "operator " + std::to_string(a.op) +
+            return set_error(kErrInvalid, "operator " + std::to_string(op) +
                                               " is not available with the interpolated far field");
     }
 }
@@ -1113,7 +1180,8 @@ void interp_free(Tree* t) {
     if (!I) return;
     void* arrays[] = {I->box_c, I->box_h, I->iidx, I->chunks, I->chunk_first, I->part, I->err,
                       I->pts[0], I->pts[1], I->pts[2], I->pts[3],
-                      I->prox[0], I->prox[1], I->prox[2], I->prox[3]};
+                      I->prox[0], I->prox[1], I->prox[2], I->prox[3], I->gcost,
+                      I->gcost_sorted, I->giota, I->gorder, I->gsort_tmp};
     for (void* p : arrays) pool_free(p, nullptr);
     delete I;
     t->interp = nullptr;
@@ -1162,7 +1230,7 @@ int interp_scatter(Tree* t, int slot, const void* attrs, int dim, cudaStream_t s
 }
 
 int interp_traverse(const Tree* t, const TraverseArgs& a, cudaStream_t stream) {
-    const Interp* I = t->interp;
+    Interp* I = t->interp;
     if (!I) return set_error(kErrState, "the interpolated far field is not set up");
     if (!a.out) return set_error(kErrInvalid, "output is null");
     if (a.queries && a.nq < 0) return set_error(kErrInvalid, "negative query count");
