@@ -55,7 +55,15 @@ namespace cagr {
 
 constexpr int kPMax = 9;          // degree <= 8
 constexpr int kChunk = 2048;      // points per proxy-charge block
-constexpr int kRec = 12;          // scalars per point / proxy record
+// Source records (points and proxies alike) are stored in pairs: records 2b
+// and 2b + 1 form block b of kBlk scalars, component c of record 2b + h at
+// block[2c + h], components (y0, y1, y2, q0, e0, e1, e2, q1, q2) = 0..8 (the
+// position y, the charges q, e = exp(-y/2)), block[18..19] = 0.  A block is
+// 80 bytes in float: five 16-byte loads give every component as an adjacent
+// pair of registers, the operands of the packed f32x2 instructions that
+// evaluate two records per instruction.
+constexpr int kBlk = 20;
+constexpr int kComp = 9;
 constexpr unsigned kAll = 0xffffffffu;
 // the pipelined walk's shape (see k_iwalk)
 #ifndef CAGR_IW_SLOTS
@@ -77,6 +85,7 @@ constexpr int kTileBytes = CAGR_IW_TILE;    // per tile (3072: 64 float / 32 dou
 // 3 slots and unroll 4: 38.0 / 45.8 ms)
 constexpr int kPWarps = CAGR_IW_WARPS;      // warps per block
 constexpr int kUnroll = CAGR_IW_UNROLL;     // pair terms per inner-loop iteration
+constexpr int kUnrollB = kUnroll > 1 ? kUnroll / 2 : 1;  // blocks (two terms each) per iteration
 // internal operator codes beside Op: the A2T sums of the interpolated mode
 constexpr int kIOpA2TSum = 100;     // sum_k A2Tk(s_k), three scalar columns (slot 3)
 constexpr int kIOpA2TShared = 101;  // sum_k A2Tk(s), one scalar column
@@ -201,23 +210,38 @@ __global__ void k_ichunks(const int4* __restrict__ meta, int64_t M, const int32_
 
 // ---- records and proxy charges ------------------------------------------------
 
-// Point records in Morton order: (y, c0) (exp(-y/2), c1) (c2, 0, 0, 0), the
-// charges being the point's attribute (dim 3: mu; dim 1: s, 0, 0; the three
-// scalar columns of cagr_scatter3: s_0, s_1, s_2).
+// Writes record r (position y, charges q) into the paired layout; the record
+// that ends an odd-sized array also writes its partner's half as zeros.
+template <typename T>
+__device__ __forceinline__ void write_rec(T* base, int64_t r, int64_t nrec, T y0, T y1, T y2, T q0,
+                                          T q1, T q2) {
+    T* b = base + (r >> 1) * kBlk + (r & 1);
+    const T v[kComp] = {y0, y1, y2, q0, exp_t(y0 * T(-0.5)), exp_t(y1 * T(-0.5)),
+                        exp_t(y2 * T(-0.5)), q1, q2};
+#pragma unroll
+    for (int c = 0; c < kComp; c++) b[2 * c] = v[c];
+    b[18] = T(0);
+    if ((r & 1) == 0 && r + 1 >= nrec)
+        for (int c = 0; c < 10; c++) b[2 * c + 1] = T(0);
+}
+template <typename T>
+__device__ __forceinline__ T rec_comp(const T* base, int64_t r, int c) {
+    return base[(r >> 1) * kBlk + 2 * c + (r & 1)];
+}
+
+// Point records in Morton order, the charges being the point's attribute
+// (dim 3: mu; dim 1: s, 0, 0; the three scalar columns of cagr_scatter3:
+// s_0, s_1, s_2).
 template <typename T>
 __global__ void k_ipoints(const T* __restrict__ spos, const int32_t* __restrict__ perm, int64_t n,
                           const T* __restrict__ attrs, int dim, T* __restrict__ out) {
     const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const int64_t j = perm[s];
-    const T y0 = spos[3 * s], y1 = spos[3 * s + 1], y2 = spos[3 * s + 2];
     const T a0 = attrs[j * dim];
     const T a1 = dim == 3 ? attrs[j * 3 + 1] : T(0);
     const T a2 = dim == 3 ? attrs[j * 3 + 2] : T(0);
-    T* r = out + s * kRec;
-    st4<T>(r, make4(y0, y1, y2, a0));
-    st4<T>(r + 4, make4(exp_t(y0 * T(-0.5)), exp_t(y1 * T(-0.5)), exp_t(y2 * T(-0.5)), a1));
-    st4<T>(r + 8, make4(a2, T(0), T(0), T(0)));
+    write_rec(out, s, n, spos[3 * s], spos[3 * s + 1], spos[3 * s + 2], a0, a1, a2);
 }
 
 template <typename T>
@@ -227,7 +251,7 @@ struct ChargeParams {
     const T* bh = nullptr;
     const T* pts = nullptr;
     T* part = nullptr;
-    int P = 0, P3 = 0;
+    int P = 0, P3 = 0, P3e = 0;  // P3e: P3 rounded up to even (whole record pairs per grid)
     T cheb[kPMax] = {};
     T omega[kPMax] = {};
 };
@@ -283,16 +307,16 @@ __global__ void __launch_bounds__(kChargeThreads) k_charges(const ChargeParams<T
         const int cnt = min(kTile, cd.z - base);
         for (int t = threadIdx.x; t < cnt * 3; t += kChargeThreads) {
             const int j = t / 3, a = t - 3 * j;
-            const T y = p.pts[((int64_t)cd.y + base + j) * kRec + a];
+            const T y = rec_comp(p.pts, (int64_t)cd.y + base + j, a);
             T u = (y - cen[a]) * ih[a];
             u = fmin(fmax(u, T(-1)), T(1));
             lagrange(u, P, p.cheb, p.omega, &sL[j][a][0]);
         }
         for (int j = threadIdx.x; j < cnt; j += kChargeThreads) {
-            const T* r = p.pts + ((int64_t)cd.y + base + j) * kRec;
-            sQ[j][0] = r[3];
-            sQ[j][1] = r[7];
-            sQ[j][2] = r[8];
+            const int64_t r = (int64_t)cd.y + base + j;
+            sQ[j][0] = rec_comp(p.pts, r, 3);
+            sQ[j][1] = rec_comp(p.pts, r, 7);
+            sQ[j][2] = rec_comp(p.pts, r, 8);
         }
         __syncthreads();
         for (int j = 0; j < cnt; j++) {
@@ -327,10 +351,15 @@ __global__ void k_charges_finish(const int32_t* __restrict__ chunk_first, int64_
                                  const T* __restrict__ bc, const T* __restrict__ bh,
                                  const ChargeParams<T> p, T* __restrict__ prox) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int P = p.P, P3 = p.P3;
-    const int64_t ii = idx / P3;
-    const int m = (int)(idx - ii * P3);
+    const int P = p.P, P3 = p.P3, P3e = p.P3e;
+    const int64_t ii = idx / P3e;
+    const int m = (int)(idx - ii * P3e);
     if (ii >= num_interp) return;
+    const int64_t nrec = num_interp * P3e;
+    if (m >= P3) {  // the padding record of an odd grid: zero charges
+        write_rec(prox, idx, nrec, T(0), T(0), T(0), T(0), T(0), T(0));
+        return;
+    }
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
     const int c0 = chunk_first[ii], c1 = chunk_first[ii + 1];
     for (int ch = c0; ch < c1; ch++) {
@@ -346,10 +375,7 @@ __global__ void k_charges_finish(const int32_t* __restrict__ chunk_first, int64_
     const T y0 = c[0] + h[0] * p.cheb[a];
     const T y1 = c[1] + h[1] * p.cheb[b];
     const T y2 = c[2] + h[2] * p.cheb[cc];
-    T* r = prox + idx * kRec;
-    st4<T>(r, make4(y0, y1, y2, (T)s0));
-    st4<T>(r + 4, make4(exp_t(y0 * T(-0.5)), exp_t(y1 * T(-0.5)), exp_t(y2 * T(-0.5)), (T)s1));
-    st4<T>(r + 8, make4((T)s2, T(0), T(0), T(0)));
+    write_rec(prox, idx, nrec, y0, y1, y2, (T)s0, (T)s1, (T)s2);
 }
 
 // ---- the walk -------------------------------------------------------------------
@@ -362,7 +388,7 @@ struct IWalk {
     const int32_t* iidx = nullptr;
     const T* pts = nullptr;
     const T* prox = nullptr;
-    int P3 = 0;
+    int P3 = 0, P3e = 0;  // records per proxy grid; its stride (P3 rounded up to even)
     int direct_max = 0;
     T theta = T(0.5);
     // queries: the tree's points (grouped by qgroup), an explicit array
@@ -419,104 +445,204 @@ __device__ __forceinline__ void kahan(T& s, T& c, T v) {
     s = t;
 }
 
-// One pair term against record r (a point or a proxy).  NEAR: the per-pair
-// width test of the reference kernels; far sources are outside every width.
-template <typename T, int OP, bool CONT, bool NEAR>
-__device__ __forceinline__ void iterm(const IQ<T>& q, const T* __restrict__ r, T& p0, T& p1, T& p2,
-                                      T& i0, T& i1, T& i2) {
-    const Vec4<T> r0 = ld4(r);
+// ---- the pair term ------------------------------------------------------------
+//
+// One block = two source records; every quantity of the term is a pair, one
+// value per record, computed with the packed f32x2 instructions of sm_100
+// (fma/mul/add.rn.f32x2: one issue slot for two FP32 operations, the same
+// rounding as the scalar ones) -- the walk is issue-bound, and this halves its
+// FP32 instructions.  In double the pairs are two scalars.
+template <typename T>
+struct Pair;
+template <>
+struct Pair<float> {
+    using type = float2;
+};
+template <>
+struct Pair<double> {
+    using type = double2;
+};
+template <typename T>
+using P2 = typename Pair<T>::type;
+
+__device__ __forceinline__ float2 pk(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 pk(double a, double b) { return make_double2(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ double2 fma2(double2 a, double2 b, double2 c) {
+    return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y));
+}
+__device__ __forceinline__ double2 mul2(double2 a, double2 b) {
+    return make_double2(a.x * b.x, a.y * b.y);
+}
+__device__ __forceinline__ double2 add2(double2 a, double2 b) {
+    return make_double2(a.x + b.x, a.y + b.y);
+}
+
+// The nine component pairs of a block (y0, y1, y2, q0, e0, e1, e2, q1, q2).
+template <typename T>
+struct Blk {
+    P2<T> c[kComp];
+};
+__device__ __forceinline__ Blk<float> load_blk(const float* b) {
+    const float4 A = ld4(b), B = ld4(b + 4), C = ld4(b + 8), D = ld4(b + 12), E = ld4(b + 16);
+    Blk<float> k;
+    k.c[0] = pk(A.x, A.y);
+    k.c[1] = pk(A.z, A.w);
+    k.c[2] = pk(B.x, B.y);
+    k.c[3] = pk(B.z, B.w);
+    k.c[4] = pk(C.x, C.y);
+    k.c[5] = pk(C.z, C.w);
+    k.c[6] = pk(D.x, D.y);
+    k.c[7] = pk(D.z, D.w);
+    k.c[8] = pk(E.x, E.y);
+    return k;
+}
+__device__ __forceinline__ Blk<double> load_blk(const double* b) {
+    Blk<double> k;
+#pragma unroll
+    for (int c = 0; c < kComp; c++) k.c[c] = *reinterpret_cast<const double2*>(b + 2 * c);
+    return k;
+}
+
+// The query's values as pairs (both halves equal).
+template <typename T>
+struct IQ2 {
+    P2<T> x, y, z, ex0, ex1, ex2;
+};
+
+// One block's two pair terms into the pair sums p0..p2 (inside-width sums of
+// the continuous kernel into i0..i2).  NEAR: the per-pair width test of the
+// reference kernels; far sources are outside every width.  MASKED: only the
+// halves in `mask` are taken (bit 0: the block's first record, bit 1: its
+// second) -- a range that starts or ends inside a block.  A half not taken
+// gets 1/r = 0, so its finite data contributes exactly zero.
+template <typename T, int OP, bool CONT, bool NEAR, bool MASKED>
+__device__ __forceinline__ void pterm(const IQ<T>& q, const IQ2<T>& q2, const T* __restrict__ b,
+                                      uint32_t mask, P2<T>& p0, P2<T>& p1, P2<T>& p2, T& i0,
+                                      T& i1, T& i2) {
+    const bool ra = !MASKED || (mask & 1u), rb = !MASKED || (mask & 2u);  // in the range
     if constexpr (OP == kOpCount) {
-        p0 += T(1);
+        p0 = add2(p0, pk(ra ? T(1) : T(0), rb ? T(1) : T(0)));
         return;
     } else {
-        const T dx = q.x - r0.x, dy = q.y - r0.y, dz = q.z - r0.z;
-        const T d2 = dx * dx + dy * dy + dz * dz;
-        bool outside = true;
-        if constexpr (NEAR) outside = d2 >= q.tw;
-        const T rinv = (!NEAR || outside) ? rsqrt_t(d2) : T(0);
-        const T rinv2 = rinv * rinv;
-        const Vec4<T> r1 = ld4(r + 4);  // (e0, e1, e2, c1)
+        const Blk<T> k = load_blk(b);
+        const P2<T> m1 = pk(T(-1), T(-1));
+        const P2<T> dx = fma2(k.c[0], m1, q2.x);
+        const P2<T> dy = fma2(k.c[1], m1, q2.y);
+        const P2<T> dz = fma2(k.c[2], m1, q2.z);
+        const P2<T> d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+        const bool oa = ra && (!NEAR || d2.x >= q.tw), ob = rb && (!NEAR || d2.y >= q.tw);
+        const P2<T> r = (NEAR || MASKED) ? pk(oa ? rsqrt_t(d2.x) : T(0), ob ? rsqrt_t(d2.y) : T(0))
+                                         : pk(rsqrt_t(d2.x), rsqrt_t(d2.y));
+        const P2<T> r2 = mul2(r, r);
+        const P2<T> r3 = mul2(r2, r);
+        const P2<T> half = pk(T(0.5), T(0.5));
+        // continuous kernel, inside the width: the pairs in the range that fail the test
+        const bool ia = NEAR && CONT && ra && !oa, ib = NEAR && CONT && rb && !ob;
         if constexpr (OP == kOpA || OP == kOpG || IOp<OP>::a2) {
-            const T m0 = r0.w, m1 = r1.w, m2 = r[8];
-            const T dm = dx * m0 + dy * m1 + dz * m2;
+            const P2<T> dm = fma2(dz, k.c[8], fma2(dy, k.c[7], mul2(dx, k.c[3])));
             if constexpr (OP == kOpA) {
-                p0 += dm * (rinv * rinv2);
+                p0 = fma2(dm, r3, p0);
                 if constexpr (NEAR && CONT) {
-                    if (!outside) i0 += dm * q.iw3;
+                    if (ia) i0 += dm.x * q.iw3;
+                    if (ib) i0 += dm.y * q.iw3;
                 }
             } else if constexpr (OP == kOpG) {
-                const T rinv3 = rinv * rinv2;
-                const T c = T(3) * dm * (rinv3 * rinv2);
-                p0 += m0 * rinv3 - dx * c;
-                p1 += m1 * rinv3 - dy * c;
-                p2 += m2 * rinv3 - dz * c;
+                const P2<T> cc = mul2(mul2(pk(T(-3), T(-3)), dm), mul2(r3, r2));
+                p0 = fma2(dx, cc, fma2(k.c[3], r3, p0));
+                p1 = fma2(dy, cc, fma2(k.c[7], r3, p1));
+                p2 = fma2(dz, cc, fma2(k.c[8], r3, p2));
             } else {
-                const T t = dm * (rinv * rinv2);
-                const T hh = T(0.5) * rinv;
-                if constexpr (IOp<OP>::s0) p0 += r1.x * (t + hh * m0);
-                if constexpr (IOp<OP>::s1) p1 += r1.y * (t + hh * m1);
-                if constexpr (IOp<OP>::s2) p2 += r1.z * (t + hh * m2);
+                const P2<T> t = mul2(dm, r3);
+                const P2<T> hh = mul2(half, r);
+                if constexpr (IOp<OP>::s0) p0 = fma2(k.c[4], fma2(hh, k.c[3], t), p0);
+                if constexpr (IOp<OP>::s1) p1 = fma2(k.c[5], fma2(hh, k.c[7], t), p1);
+                if constexpr (IOp<OP>::s2) p2 = fma2(k.c[6], fma2(hh, k.c[8], t), p2);
                 if constexpr (NEAR && CONT) {
-                    if (!outside) {
-                        const T ti = dm * q.iw3;
-                        const T hi = T(0.5) * q.iw;
-                        if constexpr (IOp<OP>::s0) i0 += ti + hi * m0;
-                        if constexpr (IOp<OP>::s1) i1 += ti + hi * m1;
-                        if constexpr (IOp<OP>::s2) i2 += ti + hi * m2;
+                    const T hi = T(0.5) * q.iw;
+                    if (ia) {
+                        const T ti = dm.x * q.iw3;
+                        if constexpr (IOp<OP>::s0) i0 += ti + hi * k.c[3].x;
+                        if constexpr (IOp<OP>::s1) i1 += ti + hi * k.c[7].x;
+                        if constexpr (IOp<OP>::s2) i2 += ti + hi * k.c[8].x;
+                    }
+                    if (ib) {
+                        const T ti = dm.y * q.iw3;
+                        if constexpr (IOp<OP>::s0) i0 += ti + hi * k.c[3].y;
+                        if constexpr (IOp<OP>::s1) i1 += ti + hi * k.c[7].y;
+                        if constexpr (IOp<OP>::s2) i2 += ti + hi * k.c[8].y;
                     }
                 }
             }
         } else if constexpr (OP == kOpAT) {
-            const T c = r0.w * (rinv * rinv2);
-            p0 += dx * c;
-            p1 += dy * c;
-            p2 += dz * c;
+            const P2<T> c = mul2(k.c[3], r3);
+            p0 = fma2(dx, c, p0);
+            p1 = fma2(dy, c, p1);
+            p2 = fma2(dz, c, p2);
         } else if constexpr (IOp<OP>::a2t1) {
-            constexpr int k = IOp<OP>::k;
-            const T e = k == 0 ? r1.x : (k == 1 ? r1.y : r1.z);
-            const T gr = e * r0.w * rinv;
-            const T c = gr * rinv2;
-            p0 += dx * c;
-            p1 += dy * c;
-            p2 += dz * c;
-            if constexpr (k == 0) p0 += T(0.5) * gr;
-            if constexpr (k == 1) p1 += T(0.5) * gr;
-            if constexpr (k == 2) p2 += T(0.5) * gr;
+            constexpr int K = IOp<OP>::k;
+            const P2<T> gr = mul2(mul2(k.c[4 + K], k.c[3]), r);
+            const P2<T> c = mul2(gr, r2);
+            p0 = fma2(dx, c, p0);
+            p1 = fma2(dy, c, p1);
+            p2 = fma2(dz, c, p2);
+            if constexpr (K == 0) p0 = fma2(half, gr, p0);
+            if constexpr (K == 1) p1 = fma2(half, gr, p1);
+            if constexpr (K == 2) p2 = fma2(half, gr, p2);
         } else if constexpr (IOp<OP>::a2tsum) {
             // sum_k exp(x_k/2) exp(-y_k/2) s_k (d / r^3 + e_k / (2r))
-            const T sa = r0.w;
-            const T sb = OP == kIOpA2TSum ? r1.w : r0.w;
-            const T sc = OP == kIOpA2TSum ? r[8] : r0.w;
-            const T g0 = q.ex0 * r1.x * sa, g1 = q.ex1 * r1.y * sb, g2 = q.ex2 * r1.z * sc;
-            const T c = (g0 + g1 + g2) * (rinv * rinv2);
-            const T hr = T(0.5) * rinv;
-            p0 += dx * c + g0 * hr;
-            p1 += dy * c + g1 * hr;
-            p2 += dz * c + g2 * hr;
+            const P2<T> sa = k.c[3];
+            const P2<T> sb = OP == kIOpA2TSum ? k.c[7] : k.c[3];
+            const P2<T> sc = OP == kIOpA2TSum ? k.c[8] : k.c[3];
+            const P2<T> g0 = mul2(q2.ex0, mul2(k.c[4], sa));
+            const P2<T> g1 = mul2(q2.ex1, mul2(k.c[5], sb));
+            const P2<T> g2 = mul2(q2.ex2, mul2(k.c[6], sc));
+            const P2<T> c = mul2(add2(add2(g0, g1), g2), r3);
+            const P2<T> hr = mul2(half, r);
+            p0 = fma2(dx, c, fma2(g0, hr, p0));
+            p1 = fma2(dy, c, fma2(g1, hr, p1));
+            p2 = fma2(dz, c, fma2(g2, hr, p2));
         }
     }
 }
 
-// The sum over `count` consecutive records into this lane's compensated sums.
-// (lanes outside the walking subgroup, active = false, compute and discard)
+// A tile of nb blocks into this lane's compensated sums: the first block's
+// first record is skipped when sf, the last block's second when sl.  (Lanes
+// outside the walking subgroup, active = false, compute and discard.)
 template <typename T, int OP, bool CONT, bool NEAR>
-__device__ __forceinline__ void irange(const IQ<T>& q, bool active, const T* __restrict__ r,
-                                       int count, T* s, T* cmp, T* in) {
-    T p0 = T(0), p1 = T(0), p2 = T(0), i0 = T(0), i1 = T(0), i2 = T(0);
-    int j = 0;
-    for (; j + kUnroll <= count; j += kUnroll) {
-#pragma unroll
-        for (int u = 0; u < kUnroll; u++)
-            iterm<T, OP, CONT, NEAR>(q, r + (int64_t)(j + u) * kRec, p0, p1, p2, i0, i1, i2);
+__device__ __forceinline__ void itile(const IQ<T>& q, const IQ2<T>& q2, bool active,
+                                      const T* __restrict__ b, int nb, bool sf, bool sl, T* s,
+                                      T* cmp, T* in) {
+    P2<T> p0 = pk(T(0), T(0)), p1 = p0, p2 = p0;
+    T i0 = T(0), i1 = T(0), i2 = T(0);
+    int j0 = 0, j1 = nb;
+    if (sf) {
+        pterm<T, OP, CONT, NEAR, true>(q, q2, b, (nb == 1 && sl) ? 0u : 2u, p0, p1, p2, i0, i1, i2);
+        j0 = 1;
     }
-    for (; j < count; j++) iterm<T, OP, CONT, NEAR>(q, r + (int64_t)j * kRec, p0, p1, p2, i0, i1, i2);
+    const bool last_masked = sl && nb - 1 >= j0;
+    if (last_masked) j1 = nb - 1;
+    int j = j0;
+    for (; j + kUnrollB <= j1; j += kUnrollB) {
+#pragma unroll
+        for (int u = 0; u < kUnrollB; u++)
+            pterm<T, OP, CONT, NEAR, false>(q, q2, b + (int64_t)(j + u) * kBlk, 3u, p0, p1, p2, i0,
+                                            i1, i2);
+    }
+    for (; j < j1; j++)
+        pterm<T, OP, CONT, NEAR, false>(q, q2, b + (int64_t)j * kBlk, 3u, p0, p1, p2, i0, i1, i2);
+    if (last_masked)
+        pterm<T, OP, CONT, NEAR, true>(q, q2, b + (int64_t)(nb - 1) * kBlk, 1u, p0, p1, p2, i0, i1,
+                                       i2);
     if (!active) return;
     if constexpr (OP == kOpCount) {
-        s[0] += p0;
+        s[0] += p0.x + p0.y;
     } else {
-        kahan(s[0], cmp[0], p0);
-        kahan(s[1], cmp[1], p1);
-        kahan(s[2], cmp[2], p2);
+        kahan(s[0], cmp[0], p0.x + p0.y);
+        kahan(s[1], cmp[1], p1.x + p1.y);
+        kahan(s[2], cmp[2], p2.x + p2.y);
         if constexpr (NEAR && CONT) {
             in[0] += i0;
             in[1] += i1;
@@ -707,9 +833,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
     return false;
 }
 
+// blocks (record pairs) per tile: 38 in float, 19 in double
 template <typename T>
-constexpr int tile_records() {
-    return kTileBytes / (kRec * (int)sizeof(T));
+constexpr int tile_blocks() {
+    return kTileBytes / (kBlk * (int)sizeof(T));
 }
 
 template <typename T>
@@ -729,11 +856,14 @@ __global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
         mbar_init_fence();
     }
     __syncwarp();
-    constexpr int kTR = tile_records<T>();
+    constexpr int kTB = tile_blocks<T>();
+    static_assert(kTB < 64 && kSlots <= 6, "tile fields: 6-bit block count, 10 bits per slot");
     // warp-uniform pipeline state: next slot to consume, tiles in flight, the
-    // parity of each slot's next completion, and each slot's tile (count | near << 7)
+    // parity of each slot's next completion, and each slot's tile in 10 bits:
+    // blocks | near << 6 | skip the first record << 7 | skip the last << 8
     int head = 0, inflight = 0;
-    uint32_t phase = 0, tinfo = 0;
+    uint32_t phase = 0;
+    uint64_t tinfo = 0;
     const int M = (int)p.M;
     const int64_t ngroups = (p.nq + 31) / 32;
     for (;;) {
@@ -759,6 +889,13 @@ __global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
         } else {
             q.ex0 = q.ex1 = q.ex2 = T(1);
         }
+        IQ2<T> q2;
+        q2.x = pk(q.x, q.x);
+        q2.y = pk(q.y, q.y);
+        q2.z = pk(q.z, q.z);
+        q2.ex0 = pk(q.ex0, q.ex0);
+        q2.ex1 = pk(q.ex1, q.ex1);
+        q2.ex2 = pk(q.ex2, q.ex2);
         int bits;
         const Batch<T> mine = lane_batch(q, valid, w, &bits);
         T s[3] = {T(0), T(0), T(0)}, cmp[3] = {T(0), T(0), T(0)}, in[3] = {T(0), T(0), T(0)};
@@ -774,9 +911,14 @@ __global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
             const T bcx = __shfl_sync(kAll, mine.cx, g), bcy = __shfl_sync(kAll, mine.cy, g),
                     bcz = __shfl_sync(kAll, mine.cz, g), br = __shfl_sync(kAll, mine.r, g),
                     wm = __shfl_sync(kAll, mine.w, g);
-            // producer: the walk, one interaction (a run of records) at a time
-            int n = 0, left = 0, near = 0;
-            const T* src = nullptr;
+            // producer: the walk, one interaction (a run of records) at a time,
+            // as a run of blocks with its first / last half skipped when the run
+            // starts / ends inside a block
+            int n = 0;
+            int64_t blk = 0;       // next block of the current interaction
+            int left = 0;          // its blocks still to issue
+            int near = 0, skip_first = 0, skip_last = 0;
+            const T* base = nullptr;
             bool more = true;
             for (;;) {
                 while (more && inflight < kSlots) {
@@ -792,39 +934,51 @@ __global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
                         const T a = bx.w + p.theta * br;
                         const bool far = a * a < (p.theta * p.theta) * R2 && R2 >= sw * sw;
                         const int np = node_npts(mt);
+                        int64_t r0 = -1, cnt = 0;
                         if (far) {
                             const int ii = __ldg(p.iidx + n);
                             if (ii >= 0) {
-                                src = p.prox + (int64_t)ii * p.P3 * kRec;
-                                left = p.P3;
+                                base = p.prox;
+                                r0 = (int64_t)ii * p.P3e;
+                                cnt = p.P3;
                             } else {
-                                src = p.pts + (int64_t)mt.y * kRec;
-                                left = np;
+                                base = p.pts;
+                                r0 = mt.y;
+                                cnt = np;
                             }
                             near = 0;
                             n = mt.x;
                         } else if (node_leaf(mt) || np <= p.direct_max) {
-                            src = p.pts + (int64_t)mt.y * kRec;
-                            left = np;
+                            base = p.pts;
+                            r0 = mt.y;
+                            cnt = np;
                             near = 1;
                             n = mt.x;
                         } else {
                             n = n + 1;
+                        }
+                        if (r0 >= 0) {
+                            blk = r0 >> 1;
+                            left = (int)(((r0 + cnt + 1) >> 1) - blk);
+                            skip_first = (int)(r0 & 1);
+                            skip_last = (int)((r0 + cnt) & 1);
                         }
                     }
                     if (left == 0) {
                         more = false;
                         break;
                     }
-                    const int cnt = min(left, kTR);
+                    const int nb = min(left, kTB);
                     const int slot = (head + inflight) % kSlots;
                     if (lane == 0)
-                        tma_load_1d(tiles + (size_t)slot * kTileBytes, src,
-                                    (uint32_t)(cnt * kRec * sizeof(T)), bars + slot);
-                    tinfo = (tinfo & ~(0xffu << (8 * slot))) |
-                            ((uint32_t)(cnt | (near << 7)) << (8 * slot));
-                    src += (int64_t)cnt * kRec;
-                    left -= cnt;
+                        tma_load_1d(tiles + (size_t)slot * kTileBytes, base + blk * kBlk,
+                                    (uint32_t)(nb * kBlk * sizeof(T)), bars + slot);
+                    const uint64_t f = (uint64_t)(nb | (near << 6) | (skip_first << 7) |
+                                                  ((nb == left ? skip_last : 0) << 8));
+                    tinfo = (tinfo & ~(0x3ffull << (10 * slot))) | (f << (10 * slot));
+                    skip_first = 0;
+                    blk += nb;
+                    left -= nb;
                     inflight++;
                 }
                 if (inflight == 0) break;
@@ -839,12 +993,14 @@ __global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
                     return;
                 }
                 phase ^= 1u << head;
-                const uint32_t inf = (tinfo >> (8 * head)) & 0xffu;
+                const uint32_t inf = (uint32_t)(tinfo >> (10 * head)) & 0x3ffu;
                 const T* r = reinterpret_cast<const T*>(tiles + (size_t)head * kTileBytes);
-                if (inf >> 7)
-                    irange<T, OP, CONT, true>(q, active, r, (int)(inf & 0x7fu), s, cmp, in);
+                const int nbt = (int)(inf & 0x3fu);
+                const bool sf = (inf >> 7) & 1u, slast = (inf >> 8) & 1u;
+                if ((inf >> 6) & 1u)
+                    itile<T, OP, CONT, true>(q, q2, active, r, nbt, sf, slast, s, cmp, in);
                 else
-                    irange<T, OP, CONT, false>(q, active, r, (int)(inf & 0x7fu), s, cmp, in);
+                    itile<T, OP, CONT, false>(q, q2, active, r, nbt, sf, slast, s, cmp, in);
                 __syncwarp();  // every lane has read the slot before it is refilled
                 head = (head + 1) % kSlots;
                 inflight--;
@@ -1010,6 +1166,7 @@ ChargeParams<T> charge_params(const Interp* I) {
     ChargeParams<T> p;
     p.P = I->P;
     p.P3 = I->P3;
+    p.P3e = I->P3 + (I->P3 & 1);
     for (int k = 0; k < kPMax; k++) {
         p.cheb[k] = (T)I->cheb[k];
         p.omega[k] = (T)I->omega[k];
@@ -1020,12 +1177,14 @@ ChargeParams<T> charge_params(const Interp* I) {
 template <typename T>
 int scatter_impl(Tree* t, Interp* I, int slot, const void* attrs, int dim, cudaStream_t s) {
     const int64_t N = t->n;
-    if (!I->pts[slot]) {
-        if (int rc = pool_alloc(&I->pts[slot], sizeof(T) * kRec * N, s)) return rc;
+    const int P3e = I->P3 + (I->P3 & 1);
+    if (!I->pts[slot]) {  // record pairs: ceil(N / 2) blocks
+        if (int rc = pool_alloc(&I->pts[slot], sizeof(T) * kBlk * (size_t)((N + 1) / 2), s))
+            return rc;
     }
     if (!I->prox[slot]) {
-        const size_t np = (size_t)(I->num_interp > 0 ? I->num_interp : 1) * I->P3;
-        if (int rc = pool_alloc(&I->prox[slot], sizeof(T) * kRec * np, s)) return rc;
+        const size_t np = (size_t)(I->num_interp > 0 ? I->num_interp : 1) * P3e;
+        if (int rc = pool_alloc(&I->prox[slot], sizeof(T) * kBlk * (np / 2), s)) return rc;
     }
     I->dim[slot] = 0;
     k_ipoints<T><<<blocks_for(N, 256), 256, 0, s>>>((const T*)t->spos, t->perm, N, (const T*)attrs,
@@ -1038,7 +1197,7 @@ int scatter_impl(Tree* t, Interp* I, int slot, const void* attrs, int dim, cudaS
         cp.pts = (const T*)I->pts[slot];
         cp.part = (T*)I->part;
         k_charges<T><<<(unsigned)I->num_chunks, kChargeThreads, 0, s>>>(cp);
-        k_charges_finish<T><<<blocks_for(I->num_interp * I->P3, 256), 256, 0, s>>>(
+        k_charges_finish<T><<<blocks_for(I->num_interp * P3e, 256), 256, 0, s>>>(
             I->chunk_first, I->num_interp, I->chunks, (const T*)I->part, (const T*)I->box_c,
             (const T*)I->box_h, cp, (T*)I->prox[slot]);
     }
@@ -1074,6 +1233,7 @@ int traverse_impl(const Tree* t, Interp* I, const TraverseArgs& a, cudaStream_t 
     p.bc = (const T*)I->box_c;
     p.iidx = I->iidx;
     p.P3 = I->P3;
+    p.P3e = I->P3 + (I->P3 & 1);
     p.direct_max = I->direct_max;
     p.theta = (T)I->theta;
     p.spos = (const T*)t->spos;
