@@ -67,10 +67,10 @@ constexpr int kComp = 9;
 constexpr unsigned kAll = 0xffffffffu;
 // the pipelined walk's shape (see k_iwalk)
 #ifndef CAGR_IW_SLOTS
-#define CAGR_IW_SLOTS 3
+#define CAGR_IW_SLOTS 2
 #endif
 #ifndef CAGR_IW_TILE
-#define CAGR_IW_TILE 3072
+#define CAGR_IW_TILE 4096
 #endif
 #ifndef CAGR_IW_WARPS
 #define CAGR_IW_WARPS 4
@@ -79,10 +79,10 @@ constexpr unsigned kAll = 0xffffffffu;
 #define CAGR_IW_UNROLL 4
 #endif
 constexpr int kSlots = CAGR_IW_SLOTS;       // tiles in flight per warp
-constexpr int kTileBytes = CAGR_IW_TILE;    // per tile (3072: 64 float / 32 double records)
-// (measured at 1M points, A2_FUSED / A2T_SUM walk: 4 slots, unroll 2: 43.3 / 53.1 ms;
-// 3 slots: 40.2 / 46.0; unroll 4: 40.6 / 48.4; 2048-byte tiles: 42.6 / 51.6;
-// 3 slots and unroll 4: 38.0 / 45.8 ms)
+constexpr int kTileBytes = CAGR_IW_TILE;    // per tile (4096: 51 float / 25 double record pairs)
+// (measured at 1M points, A2_FUSED walk, record pairs with packed arithmetic:
+// 3 slots x 3072 B 25.8 ms, 4 x 3072 26.9, 3 x 4096 26.5, 2 x 4096 23.5,
+// 2 x 6144 23.8, 2 x 8192 26.2; 2-warp blocks the same as 4)
 constexpr int kPWarps = CAGR_IW_WARPS;      // warps per block
 constexpr int kUnroll = CAGR_IW_UNROLL;     // pair terms per inner-loop iteration
 constexpr int kUnrollB = kUnroll > 1 ? kUnroll / 2 : 1;  // blocks (two terms each) per iteration
@@ -857,10 +857,10 @@ __global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
     }
     __syncwarp();
     constexpr int kTB = tile_blocks<T>();
-    static_assert(kTB < 64 && kSlots <= 6, "tile fields: 6-bit block count, 10 bits per slot");
+    static_assert(kTB < 128 && kSlots <= 6, "tile fields: 7-bit block count, 10 bits per slot");
     // warp-uniform pipeline state: next slot to consume, tiles in flight, the
     // parity of each slot's next completion, and each slot's tile in 10 bits:
-    // blocks | near << 6 | skip the first record << 7 | skip the last << 8
+    // blocks | near << 7 | skip the first record << 8 | skip the last << 9
     int head = 0, inflight = 0;
     uint32_t phase = 0;
     uint64_t tinfo = 0;
@@ -973,8 +973,8 @@ __global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
                     if (lane == 0)
                         tma_load_1d(tiles + (size_t)slot * kTileBytes, base + blk * kBlk,
                                     (uint32_t)(nb * kBlk * sizeof(T)), bars + slot);
-                    const uint64_t f = (uint64_t)(nb | (near << 6) | (skip_first << 7) |
-                                                  ((nb == left ? skip_last : 0) << 8));
+                    const uint64_t f = (uint64_t)(nb | (near << 7) | (skip_first << 8) |
+                                                  ((nb == left ? skip_last : 0) << 9));
                     tinfo = (tinfo & ~(0x3ffull << (10 * slot))) | (f << (10 * slot));
                     skip_first = 0;
                     blk += nb;
@@ -995,9 +995,9 @@ __global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
                 phase ^= 1u << head;
                 const uint32_t inf = (uint32_t)(tinfo >> (10 * head)) & 0x3ffu;
                 const T* r = reinterpret_cast<const T*>(tiles + (size_t)head * kTileBytes);
-                const int nbt = (int)(inf & 0x3fu);
-                const bool sf = (inf >> 7) & 1u, slast = (inf >> 8) & 1u;
-                if ((inf >> 6) & 1u)
+                const int nbt = (int)(inf & 0x7fu);
+                const bool sf = (inf >> 8) & 1u, slast = (inf >> 9) & 1u;
+                if ((inf >> 7) & 1u)
                     itile<T, OP, CONT, true>(q, q2, active, r, nbt, sf, slast, s, cmp, in);
                 else
                     itile<T, OP, CONT, false>(q, q2, active, r, nbt, sf, slast, s, cmp, in);
