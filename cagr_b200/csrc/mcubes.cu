@@ -337,7 +337,8 @@ __global__ void __launch_bounds__(kChunk) k_mc_emit(const float* __restrict__ v,
                                                      const int64_t* __restrict__ vbase,
                                                      const int64_t* __restrict__ tbase,
                                                      float* __restrict__ verts,
-                                                     int32_t* __restrict__ faces) {
+                                                     int32_t* __restrict__ faces,
+                                                     int64_t max_verts, int64_t max_faces) {
     using ScanV = cub::BlockScan<unsigned long long, kChunk>;
     using ScanT = cub::BlockScan<int32_t, kChunk>;
     __shared__ typename ScanV::TempStorage tmp_v;
@@ -392,9 +393,11 @@ __global__ void __launch_bounds__(kChunk) k_mc_emit(const float* __restrict__ v,
                 if (!((own >> a) & 1)) continue;
                 const float tt = root_t(v[p], v[p + step[a]], g.iso);
                 const float d = __fmul_rn(tt, g.h);
-                verts[3 * o + 0] = a == 0 ? __fadd_rn(x, d) : x;
-                verts[3 * o + 1] = a == 1 ? __fadd_rn(y, d) : y;
-                verts[3 * o + 2] = a == 2 ? __fadd_rn(z, d) : z;
+                if (o < max_verts) {  // the host reports a mesh larger than the buffers
+                    verts[3 * o + 0] = a == 0 ? __fadd_rn(x, d) : x;
+                    verts[3 * o + 1] = a == 1 ? __fadd_rn(y, d) : y;
+                    verts[3 * o + 2] = a == 2 ? __fadd_rn(z, d) : z;
+                }
                 o++;
             }
         }
@@ -415,7 +418,7 @@ __global__ void __launch_bounds__(kChunk) k_mc_emit(const float* __restrict__ v,
                          __popc(s_mask[r][li] & below);
                 else
                     id = s_next[r] + __popc(s_mask[r][kChunk] & below);
-                faces[3 * (o + q) + s] = (int32_t)id;
+                if (o + q < max_faces) faces[3 * (o + q) + s] = (int32_t)id;
             }
         }
     }
@@ -486,6 +489,16 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
         rc = cub_scan([&](void* t, size_t& b) {
             return cub::DeviceScan::ExclusiveSum(t, b, tcnt, tbase, U + 1, s);
         }, s);
+    // with output buffers, the mesh is emitted right after the one count pass
+    // (writes beyond the buffers are skipped on the device) and the sizes are
+    // read back once: a mesh larger than the buffers is reported with its sizes,
+    // so the caller can call again with buffers of exactly those sizes
+    const bool emit = verts && faces && max_verts >= 0 && max_faces >= 0;
+    if (!rc && emit) {
+        k_mc_emit<<<grid_e, kChunk, 0, s>>>(values, g, vbase, tbase, verts, faces, max_verts,
+                                             max_faces);
+        if (cudaGetLastError() != cudaSuccess) rc = set_error(kErrCuda, "marching cubes launch");
+    }
     int64_t nv = 0, nf = 0;
     if (!rc) {
         cudaMemcpyAsync(&nv, vbase + U, 8, cudaMemcpyDeviceToHost, s);
@@ -496,14 +509,8 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
     if (!rc) {
         *nverts = nv;
         *nfaces = nf;
-        if (verts && faces) {
-            if (nv > max_verts || nf > max_faces) {
-                rc = set_error(kErrOverflow, "output buffers too small for the mesh");
-            } else {
-                k_mc_emit<<<grid_e, kChunk, 0, s>>>(values, g, vbase, tbase, verts, faces);
-                if (cudaGetLastError() != cudaSuccess) rc = set_error(kErrCuda, "marching cubes launch");
-            }
-        }
+        if (emit && (nv > max_verts || nf > max_faces))
+            rc = set_error(kErrOverflow, "output buffers too small for the mesh (sizes returned)");
     }
     cleanup();
     return rc;

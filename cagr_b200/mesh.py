@@ -46,7 +46,12 @@ def field_grid(wn: WindingNumberTreecode, dims, origin, spacing: float, width,
 
 def marching_cubes(values: torch.Tensor, origin, spacing: float, iso: float):
     """Iso-surface {values = iso} of a [nz, ny, nx] float32 CUDA grid: (vertices
-    [V,3] float32, faces [F,3] int32), outward = toward values below iso."""
+    [V,3] float32, faces [F,3] int32), outward = toward values below iso.
+
+    One pass over the grid: the mesh goes straight into buffers sized by an
+    estimate (a surface crossing the grid in every layer, 8 vertices per
+    cell column of the largest face); a larger mesh is reported with its sizes
+    and extracted again into buffers of exactly those sizes."""
     if not values.is_cuda or values.dtype != torch.float32 or values.dim() != 3:
         raise RuntimeError("values must be a float32 CUDA tensor [nz, ny, nx]")
     v = values.contiguous()
@@ -54,17 +59,21 @@ def marching_cubes(values: torch.Tensor, origin, spacing: float, iso: float):
     org = (ctypes.c_double * 3)(*[float(o) for o in origin])
     L = _lib.lib()
     nv, nf = ctypes.c_int64(), ctypes.c_int64()
+    est_v = 8 * max(nx * ny, ny * nz, nz * nx)
+    cap = (est_v, 2 * est_v + 1024)
     with torch.cuda.device(v.device):
         s = _stream(v.device)
-        check(L.cagr_marching_cubes(_ptr(v), nx, ny, nz, org, float(spacing), float(iso), None, 0,
-                                    None, 0, ctypes.byref(nv), ctypes.byref(nf), s),
-              "cagr_marching_cubes")
-        verts = torch.empty(max(nv.value, 1), 3, dtype=torch.float32, device=v.device)
-        faces = torch.empty(max(nf.value, 1), 3, dtype=torch.int32, device=v.device)
-        check(L.cagr_marching_cubes(_ptr(v), nx, ny, nz, org, float(spacing), float(iso),
-                                    _ptr(verts), verts.shape[0], _ptr(faces), faces.shape[0],
-                                    ctypes.byref(nv), ctypes.byref(nf), s),
-              "cagr_marching_cubes")
+        for _ in range(2):
+            verts = torch.empty(max(cap[0], 1), 3, dtype=torch.float32, device=v.device)
+            faces = torch.empty(max(cap[1], 1), 3, dtype=torch.int32, device=v.device)
+            rc = L.cagr_marching_cubes(_ptr(v), nx, ny, nz, org, float(spacing), float(iso),
+                                       _ptr(verts), cap[0], _ptr(faces), cap[1],
+                                       ctypes.byref(nv), ctypes.byref(nf), s)
+            if rc == 4 and (nv.value > cap[0] or nf.value > cap[1]):   # CAGR_ERR_OVERFLOW
+                cap = (nv.value, nf.value)
+                continue
+            check(rc, "cagr_marching_cubes")
+            break
     return verts[:nv.value], faces[:nf.value]
 
 

@@ -202,8 +202,11 @@ int cagr_field_grid(const cagr_tree* tree, int op, int nx, int ny, int nz, const
  * the surface value = iso, corners with value > iso inside, triangles wound
  * outward (toward decreasing values).  Writes *num_vertices / *num_faces; when
  * vertices_dev and faces_dev are non-NULL also the mesh (vertices [V,3]
- * float32, faces [F,3] int32 indices, vertices shared between cells), or
- * CAGR_ERR_OVERFLOW if V or F exceed the given maxima.  Synchronises `stream`.
+ * float32, faces [F,3] int32 indices, vertices shared between cells) in the
+ * same pass over the grid; if V or F exceed the given maxima, nothing beyond
+ * them is written, the sizes are still set and the call returns
+ * CAGR_ERR_OVERFLOW (call again with buffers of those sizes).  With NULL
+ * buffers only the sizes are computed.  Synchronises `stream`.
  * The reference extracts the surface with PoissonRecon's adaptive octree MC
  * (gaussrecon_src/Octree.cpp:852-1090, tables MarchingCubes.cpp:32-324); this
  * uniform-grid MC uses its own generated case table (cagr_mc_table). */

@@ -108,3 +108,34 @@ def test_reconstruct_sphere(cuda_lib):
     a, b, c = (v[f[:, k]].astype(np.float64) for k in range(3))
     vol = np.einsum("ij,ij->i", a, np.cross(b, c)).sum() / 6
     assert vol > 0
+
+
+def test_small_buffers_report_the_sizes_and_nothing_beyond_them(cuda_lib):
+    """With buffers smaller than the mesh the call writes nothing beyond them,
+    returns CAGR_ERR_OVERFLOW and the sizes; buffers of those sizes then give
+    the mesh the Python wrapper returns."""
+    import ctypes
+
+    import torch
+    from cagr_b200 import _lib
+    from cagr_b200.mesh import marching_cubes
+    g = 48
+    ax = np.linspace(-1, 1, g)
+    X, Y, Z = np.meshgrid(ax, ax, ax, indexing="ij")
+    vals = np.ascontiguousarray((1.0 - (X ** 2 + Y ** 2 + Z ** 2)).transpose(2, 1, 0), np.float32)
+    V = torch.from_numpy(vals).cuda()
+    h = 2.0 / (g - 1)
+    v_ref, f_ref = marching_cubes(V, (-1, -1, -1), h, 0.5)
+    org = (ctypes.c_double * 3)(-1.0, -1.0, -1.0)
+    nv, nf = ctypes.c_int64(), ctypes.c_int64()
+    cap_v, cap_f = 100, 100
+    verts = torch.full((cap_v + 8, 3), 7.0, device="cuda")
+    faces = torch.full((cap_f + 8, 3), -7, dtype=torch.int32, device="cuda")
+    rc = _lib.lib().cagr_marching_cubes(ctypes.c_void_p(V.data_ptr()), g, g, g, org, h, 0.5,
+                                        ctypes.c_void_p(verts.data_ptr()), cap_v,
+                                        ctypes.c_void_p(faces.data_ptr()), cap_f,
+                                        ctypes.byref(nv), ctypes.byref(nf), None)
+    torch.cuda.synchronize()
+    assert rc == 4 and nv.value == v_ref.shape[0] and nf.value == f_ref.shape[0]
+    assert (verts[cap_v:] == 7.0).all() and (faces[cap_f:] == -7).all()
+    assert torch.equal(verts[:cap_v], v_ref[:cap_v])
