@@ -74,8 +74,13 @@ struct TravParams {
     int out_stride = 1;
     int accumulate = 0;  // bit 0: add into `out` instead of overwriting it; bit 1: write -op
     const T* g = nullptr;  // adjoint: d loss / d out per query [nq, 3], original order
-    T* accn = nullptr;     // adjoint: per-node accumulators [M, 3]
-    T* accp = nullptr;     // adjoint: per-point accumulators [N, 3], Morton order
+    // adjoint: fixed-point accumulators (integers: their sums do not depend on
+    // the order of the atomic adds), the per-node [M, 3] and per-point [N, 3]
+    // (Morton order) sums of round(v * scale)
+    unsigned long long* accn = nullptr;
+    unsigned long long* accp = nullptr;
+    unsigned long long* vmax = nullptr;  // pass 1: the largest |v| (as double bits)
+    const double* scale = nullptr;       // pass 2: 2^e from vmax
 };
 
 template <typename T>
@@ -836,10 +841,16 @@ int dispatch(const Tree* t, const TraverseArgs& a, cudaStream_t s) {
 // term at a visit use the same node or point: one warp sum, one atomic add per
 // component); k_adj_push adds the leaf-to-root node sums to each point's own.
 
-// Adds (a, b, c) of the lanes with `take` into dst[0..2] (the same dst for all
-// of them); called by the whole warp.
-template <typename T>
-__device__ __forceinline__ void warp_red3(bool take, T a, T b, T c, T* dst) {
+// The warp sum of (a, b, c) over the lanes with `take` (all of them use the
+// same node or point).  PASS 1 records its largest magnitude in *vmax (the
+// bits of a non-negative double order as its value; NaN above infinity);
+// pass 2 adds round(sum * scale) to the integer accumulators dst[0..2].  The
+// warp sum has a fixed shuffle order and integer addition is associative, so
+// the accumulated gradient is the same bits on every run (float atomics would
+// add in the order the warps arrive).
+template <bool PASS1, typename T>
+__device__ __forceinline__ void warp_red3(bool take, T a, T b, T c, unsigned long long* dst,
+                                          unsigned long long* vmax, const double* scale) {
     const unsigned m = __ballot_sync(kFull, take);
     if (m == 0u) return;
     if (!take) a = b = c = T(0);
@@ -852,10 +863,36 @@ __device__ __forceinline__ void warp_red3(bool take, T a, T b, T c, T* dst) {
         }
     }
     if ((int)(threadIdx.x & 31) == __ffs(m) - 1) {
-        atomicAdd(dst, a);
-        atomicAdd(dst + 1, b);
-        atomicAdd(dst + 2, c);
+        if constexpr (PASS1) {
+            const double mx = fmax(fabs((double)a), fmax(fabs((double)b), fabs((double)c)));
+            const bool bad = !(mx <= 1.0e300);  // NaN or infinite
+            atomicMax(vmax, (unsigned long long)__double_as_longlong(bad ? (double)INFINITY : mx));
+        } else {
+            const double sc = *scale;
+            atomicAdd(dst, (unsigned long long)llrint((double)a * sc));
+            atomicAdd(dst + 1, (unsigned long long)llrint((double)b * sc));
+            atomicAdd(dst + 2, (unsigned long long)llrint((double)c * sc));
+        }
     }
+}
+
+// The fixed-point scale from the largest warp sum: a power of two with
+// vmax * scale * bound < 2^62, bound = the most terms one accumulator can
+// receive and the push can add (one per warp, times the levels of a path).
+// 0 when a sum is not finite (the push then writes NaN).
+__global__ void k_adj_scale(const unsigned long long* vmax, double bound, double* scale) {
+    const double v = __longlong_as_double((long long)*vmax);
+    if (!(v < (double)INFINITY)) {
+        *scale = 0.0;
+        return;
+    }
+    if (v == 0.0) {
+        *scale = 1.0;
+        return;
+    }
+    int e;
+    frexp(v * bound, &e);  // v * bound < 2^e
+    *scale = ldexp(1.0, 62 - e);
 }
 
 // d loss / d m of one term; G_k = g_k ex_k(x) (query side), gs_k = g_k, ew = e^w
@@ -882,7 +919,7 @@ __device__ __forceinline__ void adj_term(const Lane<T>& L, const T* src, T dx, T
     }
 }
 
-template <typename T, bool CONT>
+template <typename T, bool CONT, bool PASS1>
 __global__ void __launch_bounds__(kWarps * 32) k_adjoint_a2(const TravParams<T> p) {
     const int lane = threadIdx.x & 31;
     const int64_t qi = ((int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5)) * 32 + lane;
@@ -931,15 +968,18 @@ __global__ void __launch_bounds__(kWarps * 32) k_adjoint_a2(const TravParams<T> 
             }
             T v[3];
             adj_term<T, CONT>(L, src, dx, dy, dz, d2, G, gs, ew, v);
-            warp_red3(active && !use_pt, v[0], v[1], v[2], p.accn + (int64_t)n * 3);
-            warp_red3(active && use_pt, v[0], v[1], v[2], p.accp + (int64_t)mt.y * 3);
+            warp_red3<PASS1>(active && !use_pt, v[0], v[1], v[2], p.accn + (int64_t)n * 3, p.vmax,
+                             p.scale);
+            warp_red3<PASS1>(active && use_pt, v[0], v[1], v[2], p.accp + (int64_t)mt.y * 3, p.vmax,
+                             p.scale);
             n = mt.x;
             continue;
         }
         {
             T v[3];
             adj_term<T, CONT>(L, r, dx, dy, dz, d2, G, gs, ew, v);
-            warp_red3(active && far, v[0], v[1], v[2], p.accn + (int64_t)n * 3);
+            warp_red3<PASS1>(active && far, v[0], v[1], v[2], p.accn + (int64_t)n * 3, p.vmax,
+                             p.scale);
         }
         if (leaf) {
             const int np = -mt.z;
@@ -952,7 +992,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_adjoint_a2(const TravParams<T> 
                     const T ez = sub_rn(L.q2, s0.z);
                     T v[3];
                     adj_term<T, CONT>(L, pr, ex, ey, ez, dist2_exact(ex, ey, ez), G, gs, ew, v);
-                    warp_red3(open, v[0], v[1], v[2], p.accp + ((int64_t)mt.y + j) * 3);
+                    warp_red3<PASS1>(open, v[0], v[1], v[2], p.accp + ((int64_t)mt.y + j) * 3,
+                                     p.vmax, p.scale);
                 }
             }
             n = mt.x;
@@ -963,16 +1004,21 @@ __global__ void __launch_bounds__(kWarps * 32) k_adjoint_a2(const TravParams<T> 
 }
 
 // per leaf: the sum of its and its ancestors' node vectors, added to each of
-// its points' own vector; written in original point order
+// its points' own vector (all in the fixed point, exactly), converted once and
+// written in original point order
 template <typename T>
 __global__ void k_adj_push(const int32_t* __restrict__ leaf_ids, int64_t num_leaves,
                            const int4* __restrict__ meta, const int32_t* __restrict__ parent,
-                           const int32_t* __restrict__ perm, const T* __restrict__ accn,
-                           const T* __restrict__ accp, T* __restrict__ grad) {
+                           const int32_t* __restrict__ perm,
+                           const unsigned long long* __restrict__ accn,
+                           const unsigned long long* __restrict__ accp,
+                           const double* __restrict__ scale, T* __restrict__ grad) {
     const int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (li >= num_leaves) return;
+    const double sc = *scale;
+    const double inv = sc > 0.0 ? 1.0 / sc : (double)NAN;  // a power of two: exact
     const int leafn = leaf_ids[li];
-    T s0 = T(0), s1 = T(0), s2 = T(0);
+    unsigned long long s0 = 0, s1 = 0, s2 = 0;
     for (int n = leafn; n >= 0; n = parent[n]) {
         s0 += accn[(int64_t)n * 3];
         s1 += accn[(int64_t)n * 3 + 1];
@@ -983,9 +1029,9 @@ __global__ void k_adj_push(const int32_t* __restrict__ leaf_ids, int64_t num_lea
     for (int j = 0; j < np; j++) {
         const int64_t s = (int64_t)lm.y + j;
         const int64_t pt = perm[s];
-        grad[pt * 3] = accp[s * 3] + s0;
-        grad[pt * 3 + 1] = accp[s * 3 + 1] + s1;
-        grad[pt * 3 + 2] = accp[s * 3 + 2] + s2;
+        grad[pt * 3] = (T)((double)(long long)(accp[s * 3] + s0) * inv);
+        grad[pt * 3 + 1] = (T)((double)(long long)(accp[s * 3 + 1] + s1) * inv);
+        grad[pt * 3 + 2] = (T)((double)(long long)(accp[s * 3 + 2] + s2) * inv);
     }
 }
 
@@ -1005,26 +1051,42 @@ int adjoint_impl(const Tree* t, const TraverseArgs& a, const void* grad, void* g
     for (int k = 0; k < 3; k++) p.rec[k] = (const T*)t->rec[0];
     p.g = (const T*)grad;
     if (p.nq == 0) return kOk;
-    void *accn = nullptr, *accp = nullptr;
-    int rc = pool_alloc(&accn, sizeof(T) * 3 * (size_t)t->m, s);
-    if (!rc) rc = pool_alloc(&accp, sizeof(T) * 3 * (size_t)t->n, s);
+    const size_t bn = sizeof(unsigned long long) * 3 * (size_t)t->m;
+    const size_t bp = sizeof(unsigned long long) * 3 * (size_t)t->n;
+    void *accn = nullptr, *accp = nullptr, *aux = nullptr;
+    int rc = pool_alloc(&accn, bn, s);
+    if (!rc) rc = pool_alloc(&accp, bp, s);
+    if (!rc) rc = pool_alloc(&aux, 16, s);  // vmax bits, scale
     if (!rc) {
-        p.accn = (T*)accn;
-        p.accp = (T*)accp;
-        cudaMemsetAsync(accn, 0, sizeof(T) * 3 * (size_t)t->m, s);
-        cudaMemsetAsync(accp, 0, sizeof(T) * 3 * (size_t)t->n, s);
-        const int64_t blocks = ((p.nq + 31) / 32 + kWarps - 1) / kWarps;
-        if (a.continuous)
-            k_adjoint_a2<T, true><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
-        else
-            k_adjoint_a2<T, false><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
+        p.accn = (unsigned long long*)accn;
+        p.accp = (unsigned long long*)accp;
+        p.vmax = (unsigned long long*)aux;
+        p.scale = (const double*)((char*)aux + 8);
+        cudaMemsetAsync(accn, 0, bn, s);
+        cudaMemsetAsync(accp, 0, bp, s);
+        cudaMemsetAsync(aux, 0, 16, s);
+        const int64_t nwarps = (p.nq + 31) / 32;
+        const int64_t blocks = (nwarps + kWarps - 1) / kWarps;
+        // an accumulator gets at most one sum per warp; a point adds its own and
+        // its ancestors' (at most CAGR_MAX_DEPTH + 2 accumulators)
+        const double bound = (double)nwarps * (CAGR_MAX_DEPTH + 2);
+        if (a.continuous) {
+            k_adjoint_a2<T, true, true><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
+            k_adj_scale<<<1, 1, 0, s>>>(p.vmax, bound, (double*)p.scale);
+            k_adjoint_a2<T, true, false><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
+        } else {
+            k_adjoint_a2<T, false, true><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
+            k_adj_scale<<<1, 1, 0, s>>>(p.vmax, bound, (double*)p.scale);
+            k_adjoint_a2<T, false, false><<<(unsigned)blocks, kWarps * 32, 0, s>>>(p);
+        }
         k_adj_push<T><<<(unsigned)((t->num_leaves + 255) / 256), 256, 0, s>>>(
-            t->leaf_ids, t->num_leaves, t->meta, t->parent, t->perm, p.accn, p.accp,
+            t->leaf_ids, t->num_leaves, t->meta, t->parent, t->perm, p.accn, p.accp, p.scale,
             (T*)grad_attrs);
         if (cudaGetLastError() != cudaSuccess) rc = set_error(kErrCuda, "adjoint launch");
     }
     pool_free(accn, s);
     pool_free(accp, s);
+    pool_free(aux, s);
     return rc;
 }
 
