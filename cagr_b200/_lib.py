@@ -64,6 +64,9 @@ _SIGNATURES = {
     "cagr_marching_cubes": (_i32, [_p, _i32, _i32, _i32, ctypes.POINTER(ctypes.c_double),
                                    ctypes.c_double, ctypes.c_double, _p, _i64, _p, _i64, _pi64,
                                    _pi64, _p]),
+    "cagr_marching_cubes_table": (_i32, [_p, _i32, _i32, _i32, ctypes.POINTER(ctypes.c_double),
+                                         ctypes.c_double, ctypes.c_double, _p, _p, _i64, _p,
+                                         _i64, _pi64, _pi64, _p]),
     "cagr_mc_table": (_i32, [_p, _p]),
     "cagr_scatter_noalloc": (_i32, [_p] * 6 + [_i64, _i32, _p, _p, _p, _i32, _p, _p, _p, _p]),
     "cagr_pool_trim": (_i32, [_i64]),

@@ -269,9 +269,21 @@ int cagr_marching_cubes(const float* values_dev, int nx, int ny, int nz, const d
                         int32_t* faces_dev, int64_t max_faces, int64_t* num_vertices,
                         int64_t* num_faces, void* stream) {
     if (!origin) return set_error(CAGR_ERR_INVALID, "origin is null");
-    return cagr::marching_cubes(values_dev, nx, ny, nz, origin, spacing, iso, vertices_dev,
-                                max_vertices, faces_dev, max_faces, num_vertices, num_faces,
-                                as_stream(stream));
+    return cagr::marching_cubes(values_dev, nx, ny, nz, origin, spacing, iso, nullptr,
+                                vertices_dev, max_vertices, faces_dev, max_faces, num_vertices,
+                                num_faces, as_stream(stream));
+}
+
+int cagr_marching_cubes_table(const float* values_dev, int nx, int ny, int nz,
+                              const double* origin, double spacing, double iso,
+                              const int8_t* triangles, float* vertices_dev, int64_t max_vertices,
+                              int32_t* faces_dev, int64_t max_faces, int64_t* num_vertices,
+                              int64_t* num_faces, void* stream) {
+    if (!origin) return set_error(CAGR_ERR_INVALID, "origin is null");
+    if (!triangles) return set_error(CAGR_ERR_INVALID, "triangles is null");
+    return cagr::marching_cubes(values_dev, nx, ny, nz, origin, spacing, iso, triangles,
+                                vertices_dev, max_vertices, faces_dev, max_faces, num_vertices,
+                                num_faces, as_stream(stream));
 }
 
 int cagr_forward(cagr_tree* tree, int op, const void* values_dev, const void* widths_dev,

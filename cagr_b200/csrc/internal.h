@@ -174,8 +174,11 @@ int query_groups(const Tree* t, int32_t* order, cudaStream_t stream);
 // Marching cubes (mcubes.cu).  The case table: tri[256][36] edge ids (12
 // triangles at most) and ntri[256].
 int mc_table(int8_t* tri, uint8_t* ntri);
+// ref_table: null (the generated table, inside = value > iso) or triangles[256][16]
+// in the reference's layout (inside = value < iso).
 int marching_cubes(const float* values, int nx, int ny, int nz, const double* origin,
-                   double spacing, double iso, float* verts, int64_t max_verts, int32_t* faces,
-                   int64_t max_faces, int64_t* nverts, int64_t* nfaces, cudaStream_t s);
+                   double spacing, double iso, const int8_t* ref_table, float* verts,
+                   int64_t max_verts, int32_t* faces, int64_t max_faces, int64_t* nverts,
+                   int64_t* nfaces, cudaStream_t s);
 
 }  // namespace cagr

@@ -20,11 +20,20 @@
 //     its edges' inside-to-outside directions (outward), then fan-triangulated.
 // A corner is inside when value > iso (NaN is outside).
 //
+// Caller-supplied tables (cagr_marching_cubes_table): the reference's layout
+// (gaussrecon_src/MarchingCubes.cpp:32-324, 333-345): a case index whose bit k
+// is set when corner cornerMap[k] = {0, 1, 3, 2, 4, 5, 7, 6}[k] has value < iso,
+// and per case up to 5 triangles of edge ids in this file's numbering (the
+// reference's Cube::EdgeIndex, Cube.cpp:86-108, is the same), -1 terminated.
+// It is re-indexed on the host into the layout above with "inside" meaning
+// value < iso; the device code is the same, with that predicate.
+//
 // Device pipeline over units of 128 consecutive grid points of one x-row:
 //   count:  per unit, its points' crossed +x/+y/+z edges and its cells' triangles
 //   scan:   per-unit counts -> each unit's first vertex and first triangle
-//   emit:   per unit, one vertex per crossed edge (the linear root along it) and
-//           each cell's triangles as vertex indices (shared edges share vertices)
+//   emit:   per unit that has any, one vertex per crossed edge (the linear root
+//           along it) and each cell's triangles as vertex indices (shared edges
+//           share vertices); blocks skip the empty units from the scanned counts
 // Output order is grid-point order for vertices (edges +x, +y, +z of a point)
 // and cell order for triangles, with no per-point scratch.
 #include <cub/cub.cuh>
@@ -43,7 +52,8 @@ namespace cagr {
 namespace {
 
 constexpr int kMaxTri = 12;  // the generator checks the bound
-constexpr int kChunk = 128;  // grid points per unit (one block)
+constexpr int kChunk = 128;  // grid points per unit
+constexpr int kEmitUnits = 256;  // units an emit block scans
 
 struct McTable {
     int8_t tri[256][3 * kMaxTri];
@@ -218,37 +228,79 @@ int upload_table() {
     return kOk;
 }
 
+// A caller's table in the reference's layout (triangles[256][16], edge ids, -1
+// terminated; case bit k = corner kCornerMap[k] below iso) re-indexed into an
+// McTable whose case bit c = corner c below iso.  Rejects entries that are not
+// edge ids, more than 5 triangles, and triangles on edges the case does not cross.
+constexpr int kCornerMap[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+
+bool table_from_reference_layout(const int8_t* tri16, McTable& T, std::string& err) {
+    std::memset(&T, 0, sizeof(T));
+    for (int cs = 0; cs < 256; cs++) {
+        int ci = 0;
+        for (int k = 0; k < 8; k++) ci |= ((cs >> kCornerMap[k]) & 1) << k;
+        const int8_t* row = tri16 + 16 * ci;
+        int len = 0;
+        while (len < 16 && row[len] != -1) len++;
+        if (len == 16 || len % 3 != 0 || len / 3 > 5) {
+            err = "case " + std::to_string(ci) + ": not a -1 terminated list of at most 5 triangles";
+            return false;
+        }
+        for (int q = 0; q < len; q++) {
+            const int e = row[q];
+            int c0 = 0, c1 = 0;
+            if (e >= 0 && e < 12) edge_corners(e, c0, c1);
+            if (e < 0 || e >= 12 || ((cs >> c0) & 1) == ((cs >> c1) & 1)) {
+                err = "case " + std::to_string(ci) + ": entry " + std::to_string(e) +
+                      " is not an edge the case crosses";
+                return false;
+            }
+            T.tri[cs][q] = (int8_t)e;
+        }
+        T.ntri[cs] = (uint8_t)(len / 3);
+    }
+    return true;
+}
+
 struct Grid {
     int nx, ny, nz, nchunks;
     int64_t units;
     float ox, oy, oz, h, iso;
 };
 
-__device__ __forceinline__ bool inside(float v, float iso) { return v > iso; }
+// the inside test: value > iso (this module's table) or value < iso (a table in
+// the reference's layout); NaN is outside in both
+template <bool BELOW>
+__device__ __forceinline__ bool inside(float v, float iso) {
+    if constexpr (BELOW) return v < iso;
+    return v > iso;
+}
 
 __device__ __forceinline__ int64_t gid(const Grid& g, int i, int j, int k) {
     return ((int64_t)k * g.ny + j) * g.nx + i;
 }
 
 // crossed edges owned by grid point (i, j, k): bit a = the edge toward +axis a
+template <bool BELOW>
 __device__ __forceinline__ uint32_t point_mask(const float* __restrict__ v, const Grid& g, int i,
                                                int j, int k) {
     const int64_t p = gid(g, i, j, k);
-    const bool a = inside(v[p], g.iso);
+    const bool a = inside<BELOW>(v[p], g.iso);
     uint32_t m = 0;
-    if (i + 1 < g.nx && inside(v[p + 1], g.iso) != a) m |= 1;
-    if (j + 1 < g.ny && inside(v[p + g.nx], g.iso) != a) m |= 2;
-    if (k + 1 < g.nz && inside(v[p + (int64_t)g.nx * g.ny], g.iso) != a) m |= 4;
+    if (i + 1 < g.nx && inside<BELOW>(v[p + 1], g.iso) != a) m |= 1;
+    if (j + 1 < g.ny && inside<BELOW>(v[p + g.nx], g.iso) != a) m |= 2;
+    if (k + 1 < g.nz && inside<BELOW>(v[p + (int64_t)g.nx * g.ny], g.iso) != a) m |= 4;
     return m;
 }
 
+template <bool BELOW>
 __device__ __forceinline__ int cell_case(const float* __restrict__ v, const Grid& g, int64_t p) {
     const int64_t sx = 1, sy = g.nx, sz = (int64_t)g.nx * g.ny;
     int c = 0;
 #pragma unroll
     for (int q = 0; q < 8; q++) {
         const int64_t o = (q & 1) * sx + ((q >> 1) & 1) * sy + (q >> 2) * sz;
-        c |= inside(v[p + o], g.iso) ? (1 << q) : 0;
+        c |= inside<BELOW>(v[p + o], g.iso) ? (1 << q) : 0;
     }
     return c;
 }
@@ -265,66 +317,105 @@ struct Unit {
     int i0, j, k, chunk;
 };
 
-// the block's unit: blocks are laid out (chunk, j, k), so no index division
-__device__ __forceinline__ Unit block_unit() {
-    Unit r;
-    r.chunk = (int)blockIdx.x;
-    r.j = (int)blockIdx.y;
-    r.k = (int)blockIdx.z;
-    r.i0 = r.chunk * kChunk;
-    return r;
+// per unit: vertices (crossed edges owned by its points), triangles (its cells).
+// A warp takes kCountZ units stacked along z at one (chunk, j), kCountWarps
+// warps per block at consecutive j.  A unit needs the point rows (j, k),
+// (j+1, k), (j, k+1), (j+1, k+1); walking up in k, the k+1 rows of one unit are
+// the k rows of the next, so each unit reads two new rows, and the rows of the
+// unit after next are loaded before this one is counted (their latency overlaps
+// the bit work).  Lane l holds the points x = i0 + l + 32 q (q < 4, coalesced);
+// ballots turn them into inside-bit words w[q] held by every lane (w[4] bit 0:
+// the next unit's first point).  A funnel shift of (w[q+1] : w[q]) by l gives
+// the inside bits of x and x + 1, so a point's crossings and cell case are a
+// few bit operations.
+constexpr int kCountWarps = 4;
+constexpr int kCountZ = 8;
+
+struct RowVals {
+    float v[5];  // x = i0 + lane + 32 q, and (lane 0) x = i0 + kChunk
+};
+
+__device__ __forceinline__ void load_row(const float* __restrict__ row, bool ok, int i0, int nx,
+                                         int lane, RowVals& r) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int x = i0 + lane + 32 * q;
+        r.v[q] = (ok && x < nx) ? row[x] : 0.0f;
+    }
+    const int x = i0 + kChunk;
+    r.v[4] = (ok && lane == 0 && x < nx) ? row[x] : 0.0f;
 }
 
-// per unit: vertices (crossed edges owned by its points), triangles (its cells).
-// Each thread reads its x in the 4 point rows r = dy + 2 dz around the unit's
-// row once; warp ballots turn them into inside-bit rows in shared memory (bit x
-// of row r, x = 0 .. kChunk, the last one being the next unit's first point),
-// from which edge crossings and cell cases (corner dx + 2 r) are bit lookups.
-__global__ void __launch_bounds__(kChunk) k_mc_count(const float* __restrict__ v, Grid g,
-                                                      int32_t* __restrict__ vcnt,
-                                                      int32_t* __restrict__ tcnt) {
-    using Reduce = cub::BlockReduce<int32_t, kChunk>;
-    constexpr int kWords = kChunk / 32;
-    __shared__ typename Reduce::TempStorage tmp;
-    __shared__ uint32_t s_bits[4][kWords + 1];
-    {
-        const Unit U = block_unit();
-        const int64_t u = ((int64_t)U.k * g.ny + U.j) * g.nchunks + U.chunk;
-        const int t = (int)threadIdx.x, lane = t & 31;
-        const int i = U.i0 + t;
-        const bool has_y = U.j + 1 < g.ny, has_z = U.k + 1 < g.nz;
+template <bool BELOW>
+__device__ __forceinline__ void row_bits(const RowVals& r, bool ok, int i0, int nx, int lane,
+                                         float iso, uint32_t (&w)[5]) {
 #pragma unroll
-        for (int r = 0; r < 4; r++) {
-            const bool ok = i < g.nx && (!(r & 1) || has_y) && (!(r & 2) || has_z);
-            const bool in = ok && inside(v[gid(g, i, U.j + (r & 1), U.k + (r >> 1))], g.iso);
-            const uint32_t b = __ballot_sync(0xffffffffu, in);
-            if (lane == 0) s_bits[r][t >> 5] = b;
+    for (int q = 0; q < 4; q++) {
+        const int x = i0 + lane + 32 * q;
+        w[q] = __ballot_sync(0xffffffffu, ok && x < nx && inside<BELOW>(r.v[q], iso));
+    }
+    const int x = i0 + kChunk;
+    w[4] = __ballot_sync(0xffffffffu, ok && lane == 0 && x < nx && inside<BELOW>(r.v[4], iso));
+}
+
+template <bool BELOW>
+__global__ void __launch_bounds__(32 * kCountWarps) k_mc_count(const float* __restrict__ v, Grid g,
+                                                                const uint8_t* __restrict__ ntri,
+                                                                int32_t* __restrict__ vcnt,
+                                                                int32_t* __restrict__ tcnt) {
+    const int lane = (int)threadIdx.x & 31;
+    const int j = (int)blockIdx.y * kCountWarps + ((int)threadIdx.x >> 5);
+    if (j >= g.ny) return;  // whole warps; no block barrier in this kernel
+    const int i0 = (int)blockIdx.x * kChunk;
+    const int k0 = (int)blockIdx.z * kCountZ, k1 = min(k0 + kCountZ, g.nz);
+    const bool has_y = j + 1 < g.ny;
+    // row (j + dy, k) starts at v + (k ny + j + dy) nx; a missing row is not read
+    auto row = [&](int dy, int k) {
+        return v + ((int64_t)min(k, g.nz - 1) * g.ny + min(j + dy, g.ny - 1)) * g.nx;
+    };
+    RowVals a0, a1, b0, b1;  // raw rows k+1 (a) and k+2 (b) in flight
+    uint32_t c0[5], c1[5], n0[5], n1[5];  // bits of rows k (c) and k+1 (n)
+    load_row(row(0, k0), true, i0, g.nx, lane, a0);
+    load_row(row(1, k0), has_y, i0, g.nx, lane, a1);
+    load_row(row(0, k0 + 1), k0 + 1 < g.nz, i0, g.nx, lane, b0);
+    load_row(row(1, k0 + 1), has_y && k0 + 1 < g.nz, i0, g.nx, lane, b1);
+    row_bits<BELOW>(a0, true, i0, g.nx, lane, g.iso, c0);
+    row_bits<BELOW>(a1, has_y, i0, g.nx, lane, g.iso, c1);
+    for (int k = k0; k < k1; k++) {
+        const bool has_z = k + 1 < g.nz;
+        row_bits<BELOW>(b0, has_z, i0, g.nx, lane, g.iso, n0);
+        row_bits<BELOW>(b1, has_y && has_z, i0, g.nx, lane, g.iso, n1);
+        if (k + 1 < k1) {  // the rows of the next unit's k + 1
+            load_row(row(0, k + 2), k + 2 < g.nz, i0, g.nx, lane, b0);
+            load_row(row(1, k + 2), has_y && k + 2 < g.nz, i0, g.nx, lane, b1);
         }
-        if (t < 4) {
-            const int x = U.i0 + kChunk;
-            const bool ok = x < g.nx && (!(t & 1) || has_y) && (!(t & 2) || has_z);
-            s_bits[t][kWords] =
-                (ok && inside(v[gid(g, x, U.j + (t & 1), U.k + (t >> 1))], g.iso)) ? 1u : 0u;
-        }
-        __syncthreads();
-        auto bit = [&](int r, int x) { return (int)((s_bits[r][x >> 5] >> (x & 31)) & 1u); };
-        int32_t packed = 0;  // vertices + 2^16 * triangles (<= 3 * kChunk and kMaxTri * kChunk)
-        if (i < g.nx) {
-            const int a = bit(0, t);
-            const bool has_x = i + 1 < g.nx;
-            packed = (has_x && bit(0, t + 1) != a) + (has_y && bit(1, t) != a) +
-                     (has_z && bit(2, t) != a);
-            if (has_x && has_y && has_z) {
-                int cs = 0;
+        uint32_t packed = 0;  // vertices + 2^16 * triangles of this lane's 4 points
 #pragma unroll
-                for (int r = 0; r < 4; r++) cs |= (bit(r, t) | (bit(r, t + 1) << 1)) << (2 * r);
-                packed += (int32_t)__ldg(&g_ntri[cs]) << 16;
-            }
+        for (int q = 0; q < 4; q++) {
+            const int x = i0 + lane + 32 * q;
+            // bit 0: inside at x, bit 1: inside at x + 1, in rows (dy, dz) = r
+            const uint32_t p0 = __funnelshift_r(c0[q], c0[q + 1], lane) & 3u;
+            const uint32_t p1 = __funnelshift_r(c1[q], c1[q + 1], lane) & 3u;
+            const uint32_t p2 = __funnelshift_r(n0[q], n0[q + 1], lane) & 3u;
+            const uint32_t p3 = __funnelshift_r(n1[q], n1[q + 1], lane) & 3u;
+            const bool has_x = x + 1 < g.nx;
+            // crossings owned by x (bits past the grid and of missing rows are 0,
+            // so only the +x edge of the last point and the missing rows need masks)
+            packed += (has_x ? ((p0 ^ (p0 >> 1)) & 1u) : 0u) + (has_y ? ((p0 ^ p1) & 1u) : 0u) +
+                      (has_z ? ((p0 ^ p2) & 1u) : 0u);
+            if (has_x && has_y && has_z)
+                packed += (uint32_t)__ldg(&ntri[p0 | (p1 << 2) | (p2 << 4) | (p3 << 6)]) << 16;
         }
-        const int32_t sum = Reduce(tmp).Sum(packed);
-        if (t == 0) {
-            vcnt[u] = sum & 0xffff;
-            tcnt[u] = sum >> 16;
+        const uint32_t sum = __reduce_add_sync(0xffffffffu, packed);
+        if (lane == 0) {
+            const int64_t u = ((int64_t)k * g.ny + j) * g.nchunks + blockIdx.x;
+            vcnt[u] = (int32_t)(sum & 0xffffu);
+            tcnt[u] = (int32_t)(sum >> 16);
+        }
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            c0[q] = n0[q];
+            c1[q] = n1[q];
         }
     }
 }
@@ -333,7 +424,10 @@ __global__ void __launch_bounds__(kChunk) k_mc_count(const float* __restrict__ v
 // edges are owned by points in 4 point rows (dy, dz in {0, 1}) at x = i or i + 1;
 // each row's in-unit vertex prefix comes from one block scan of 4 packed 16-bit
 // counts, and x = i0 + kChunk (the next unit's first point) from that unit's base.
+template <bool BELOW>
 __global__ void __launch_bounds__(kChunk) k_mc_emit(const float* __restrict__ v, Grid g,
+                                                     const int8_t* __restrict__ tri,
+                                                     const uint8_t* __restrict__ ntri,
                                                      const int64_t* __restrict__ vbase,
                                                      const int64_t* __restrict__ tbase,
                                                      float* __restrict__ verts,
@@ -346,12 +440,30 @@ __global__ void __launch_bounds__(kChunk) k_mc_emit(const float* __restrict__ v,
     __shared__ uint8_t s_mask[4][kChunk + 1];
     __shared__ unsigned long long s_pre[kChunk];
     __shared__ int64_t s_base[4], s_next[4];
-    {
-        const Unit U = block_unit();
-        const int64_t u = ((int64_t)U.k * g.ny + U.j) * g.nchunks + U.chunk;
-        // a unit with neither vertices nor triangles (most of the grid) has nothing
-        // to emit; the test is the same for the whole block
-        if (vbase[u + 1] == vbase[u] && tbase[u + 1] == tbase[u]) return;
+    __shared__ int32_t s_list[kEmitUnits];
+    __shared__ int s_count;
+    // the block's kEmitUnits consecutive units: the ones with vertices or
+    // triangles (a small part of the grid) are listed, then emitted one by one
+    // (outputs go to the scanned positions, so the list order does not matter)
+    const int64_t u0 = (int64_t)blockIdx.x * kEmitUnits;
+    if (threadIdx.x == 0) s_count = 0;
+    __syncthreads();
+    for (int a = (int)threadIdx.x; a < kEmitUnits; a += kChunk) {
+        const int64_t u = u0 + a;
+        if (u < g.units && (vbase[u + 1] != vbase[u] || tbase[u + 1] != tbase[u]))
+            s_list[atomicAdd(&s_count, 1)] = a;
+    }
+    __syncthreads();
+    const int count = s_count;
+    for (int a = 0; a < count; a++) {
+        if (a > 0) __syncthreads();  // the previous unit is done with the shared arrays
+        const int64_t u = u0 + s_list[a];
+        Unit U;
+        U.chunk = (int)(u % g.nchunks);
+        const int64_t row = u / g.nchunks;
+        U.j = (int)(row % g.ny);
+        U.k = (int)(row / g.ny);
+        U.i0 = U.chunk * kChunk;
         const int t = (int)threadIdx.x;
         const int i = U.i0 + t;
         const bool cell_row = U.j + 1 < g.ny && U.k + 1 < g.nz;
@@ -359,15 +471,16 @@ __global__ void __launch_bounds__(kChunk) k_mc_emit(const float* __restrict__ v,
         unsigned long long c = 0;
         uint32_t own = 0;
         for (int r = 0; r < rows; r++) {
-            const uint32_t m = i < g.nx ? point_mask(v, g, i, U.j + (r & 1), U.k + (r >> 1)) : 0u;
+            const uint32_t m =
+                i < g.nx ? point_mask<BELOW>(v, g, i, U.j + (r & 1), U.k + (r >> 1)) : 0u;
             if (r == 0) own = m;
             s_mask[r][t] = (uint8_t)m;
             c |= (unsigned long long)__popc(m) << (16 * r);
         }
         int cs = 0, nt = 0;
         if (cell_row && i + 1 < g.nx) {
-            cs = cell_case(v, g, gid(g, i, U.j, U.k));
-            nt = __ldg(&g_ntri[cs]);
+            cs = cell_case<BELOW>(v, g, gid(g, i, U.j, U.k));
+            nt = __ldg(&ntri[cs]);
         }
         unsigned long long cpre;
         int32_t tpre;
@@ -379,7 +492,8 @@ __global__ void __launch_bounds__(kChunk) k_mc_emit(const float* __restrict__ v,
             s_base[t] = vbase[row * g.nchunks + U.chunk];
             if (U.chunk + 1 < g.nchunks) {
                 s_next[t] = vbase[row * g.nchunks + U.chunk + 1];
-                s_mask[t][kChunk] = (uint8_t)point_mask(v, g, U.i0 + kChunk, U.j + (t & 1), U.k + (t >> 1));
+                s_mask[t][kChunk] = (uint8_t)point_mask<BELOW>(v, g, U.i0 + kChunk, U.j + (t & 1),
+                                                               U.k + (t >> 1));
             }
         }
         __syncthreads();
@@ -404,7 +518,7 @@ __global__ void __launch_bounds__(kChunk) k_mc_emit(const float* __restrict__ v,
         const int64_t o = tbase[u] + tpre;
         for (int q = 0; q < nt; q++) {
             for (int s = 0; s < 3; s++) {
-                const int e = __ldg(&g_tri[cs][3 * q + s]);
+                const int e = __ldg(&tri[cs * 3 * kMaxTri + 3 * q + s]);
                 const int a = e >> 2, u = e & 1, w = (e >> 1) & 1;
                 // the point owning edge e of this cell, as (dx, row r = dy + 2 dz)
                 const int dx = a == 0 ? 0 : u;
@@ -448,40 +562,77 @@ int mc_table(int8_t* tri, uint8_t* ntri) {
 }
 
 int marching_cubes(const float* values, int nx, int ny, int nz, const double* origin,
-                   double spacing, double iso, float* verts, int64_t max_verts, int32_t* faces,
-                   int64_t max_faces, int64_t* nverts, int64_t* nfaces, cudaStream_t s) {
+                   double spacing, double iso, const int8_t* ref_table, float* verts,
+                   int64_t max_verts, int32_t* faces, int64_t max_faces, int64_t* nverts,
+                   int64_t* nfaces, cudaStream_t s) {
     if (!values || nx < 2 || ny < 2 || nz < 2 || !nverts || !nfaces)
         return set_error(kErrInvalid, "marching cubes needs values on a grid of at least 2^3");
     if ((int64_t)nx * ny * nz >= (int64_t(1) << 31))
         return set_error(kErrOverflow, "grid too large for 32-bit vertex indices");
-    if (int rc = upload_table()) return rc;
+    // the case table: this module's (uploaded once per device) or the caller's,
+    // re-indexed and copied to the device for this call
+    McTable user;
+    if (ref_table) {
+        std::string err;
+        if (!table_from_reference_layout(ref_table, user, err))
+            return set_error(kErrInvalid, "marching-cubes table: " + err);
+    } else if (int rc = upload_table()) {
+        return rc;
+    }
     const int nchunks = (nx + kChunk - 1) / kChunk;
     const int64_t U = (int64_t)nchunks * ny * nz;
     Grid g{nx, ny, nz, nchunks, U, (float)origin[0], (float)origin[1], (float)origin[2],
            (float)spacing, (float)iso};
-    // one block per unit, blocks laid out (chunk, j, k)
+    // count: a warp per kCountZ units stacked in z, blocks (chunk, j / kCountWarps,
+    // k / kCountZ); emit: a block per kEmitUnits consecutive units
     if (ny > 65535 || nz > 65535)
         return set_error(kErrInvalid, "marching cubes needs ny, nz <= 65535");
-    const dim3 grid_c((unsigned)nchunks, (unsigned)ny, (unsigned)nz), grid_e = grid_c;
+    const dim3 grid_c((unsigned)nchunks, (unsigned)((ny + kCountWarps - 1) / kCountWarps),
+                      (unsigned)((nz + kCountZ - 1) / kCountZ)),
+        grid_e((unsigned)((U + kEmitUnits - 1) / kEmitUnits));
     int32_t *vcnt = nullptr, *tcnt = nullptr;
     int64_t *vbase = nullptr, *tbase = nullptr;
+    McTable* dtable = nullptr;  // the caller's table on the device
     auto cleanup = [&] {
         pool_free(vcnt, s);
         pool_free(tcnt, s);
         pool_free(vbase, s);
         pool_free(tbase, s);
+        pool_free(dtable, s);
     };
     int rc = pool_alloc((void**)&vcnt, 4 * (U + 1), s);
     if (!rc) rc = pool_alloc((void**)&tcnt, 4 * (U + 1), s);
     if (!rc) rc = pool_alloc((void**)&vbase, 8 * (U + 1), s);
     if (!rc) rc = pool_alloc((void**)&tbase, 8 * (U + 1), s);
+    if (!rc && ref_table) rc = pool_alloc((void**)&dtable, sizeof(McTable), s);
+    const int8_t* tri = nullptr;
+    const uint8_t* ntri = nullptr;
+    if (!rc && ref_table) {
+        // `user` outlives the copy: the stream is synchronised below
+        if (cudaMemcpyAsync(dtable, &user, sizeof(McTable), cudaMemcpyHostToDevice, s) !=
+            cudaSuccess)
+            rc = set_error(kErrCuda, "marching-cubes table copy");
+        tri = &dtable->tri[0][0];
+        ntri = dtable->ntri;
+    } else if (!rc) {
+        void *pt = nullptr, *pn = nullptr;
+        if (cudaGetSymbolAddress(&pt, g_tri) != cudaSuccess ||
+            cudaGetSymbolAddress(&pn, g_ntri) != cudaSuccess)
+            rc = set_error(kErrCuda, "marching-cubes table address");
+        tri = (const int8_t*)pt;
+        ntri = (const uint8_t*)pn;
+    }
     if (rc) {
         cleanup();
         return rc;
     }
+    const bool below = ref_table != nullptr;
     cudaMemsetAsync(vcnt + U, 0, 4, s);
     cudaMemsetAsync(tcnt + U, 0, 4, s);
-    k_mc_count<<<grid_c, kChunk, 0, s>>>(values, g, vcnt, tcnt);
+    if (below)
+        k_mc_count<true><<<grid_c, 32 * kCountWarps, 0, s>>>(values, g, ntri, vcnt, tcnt);
+    else
+        k_mc_count<false><<<grid_c, 32 * kCountWarps, 0, s>>>(values, g, ntri, vcnt, tcnt);
     rc = cub_scan([&](void* t, size_t& b) {
         return cub::DeviceScan::ExclusiveSum(t, b, vcnt, vbase, U + 1, s);
     }, s);
@@ -495,8 +646,12 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
     // so the caller can call again with buffers of exactly those sizes
     const bool emit = verts && faces && max_verts >= 0 && max_faces >= 0;
     if (!rc && emit) {
-        k_mc_emit<<<grid_e, kChunk, 0, s>>>(values, g, vbase, tbase, verts, faces, max_verts,
-                                             max_faces);
+        if (below)
+            k_mc_emit<true><<<grid_e, kChunk, 0, s>>>(values, g, tri, ntri, vbase, tbase, verts,
+                                                      faces, max_verts, max_faces);
+        else
+            k_mc_emit<false><<<grid_e, kChunk, 0, s>>>(values, g, tri, ntri, vbase, tbase, verts,
+                                                       faces, max_verts, max_faces);
         if (cudaGetLastError() != cudaSuccess) rc = set_error(kErrCuda, "marching cubes launch");
     }
     int64_t nv = 0, nf = 0;

@@ -44,9 +44,17 @@ def field_grid(wn: WindingNumberTreecode, dims, origin, spacing: float, width,
     return out
 
 
-def marching_cubes(values: torch.Tensor, origin, spacing: float, iso: float):
+def marching_cubes(values: torch.Tensor, origin, spacing: float, iso: float,
+                   table: np.ndarray | None = None):
     """Iso-surface {values = iso} of a [nz, ny, nx] float32 CUDA grid: (vertices
     [V,3] float32, faces [F,3] int32), outward = toward values below iso.
+
+    table: None (the library's generated case table, inside = values > iso) or
+    a [256, 16] case table in the reference's layout (PoissonRecon's
+    MarchingCubes::triangles: case bit k = corner {0,1,3,2,4,5,7,6}[k] below
+    iso, edge ids 4a + u + 2v, -1 terminated), used as given: inside = values
+    < iso, each cell's triangles in the table's order and winding
+    (cagr_marching_cubes_table).
 
     One pass over the grid: the mesh goes straight into buffers sized by an
     estimate (a surface crossing the grid in every layer, 8 vertices per
@@ -58,6 +66,17 @@ def marching_cubes(values: torch.Tensor, origin, spacing: float, iso: float):
     nz, ny, nx = v.shape
     org = (ctypes.c_double * 3)(*[float(o) for o in origin])
     L = _lib.lib()
+    if table is not None:
+        tab = np.ascontiguousarray(table, np.int8)
+        if tab.shape != (256, 16):
+            raise RuntimeError("table must be [256, 16] int8")
+
+        def run(*a):
+            return L.cagr_marching_cubes_table(*a[:7], tab.ctypes.data_as(ctypes.c_void_p),
+                                               *a[7:])
+        name = "cagr_marching_cubes_table"
+    else:
+        run, name = L.cagr_marching_cubes, "cagr_marching_cubes"
     nv, nf = ctypes.c_int64(), ctypes.c_int64()
     est_v = 8 * max(nx * ny, ny * nz, nz * nx)
     cap = (est_v, 2 * est_v + 1024)
@@ -66,13 +85,12 @@ def marching_cubes(values: torch.Tensor, origin, spacing: float, iso: float):
         for _ in range(2):
             verts = torch.empty(max(cap[0], 1), 3, dtype=torch.float32, device=v.device)
             faces = torch.empty(max(cap[1], 1), 3, dtype=torch.int32, device=v.device)
-            rc = L.cagr_marching_cubes(_ptr(v), nx, ny, nz, org, float(spacing), float(iso),
-                                       _ptr(verts), cap[0], _ptr(faces), cap[1],
-                                       ctypes.byref(nv), ctypes.byref(nf), s)
+            rc = run(_ptr(v), nx, ny, nz, org, float(spacing), float(iso), _ptr(verts), cap[0],
+                     _ptr(faces), cap[1], ctypes.byref(nv), ctypes.byref(nf), s)
             if rc == 4 and (nv.value > cap[0] or nf.value > cap[1]):   # CAGR_ERR_OVERFLOW
                 cap = (nv.value, nf.value)
                 continue
-            check(rc, "cagr_marching_cubes")
+            check(rc, name)
             break
     return verts[:nv.value], faces[:nf.value]
 

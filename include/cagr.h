@@ -209,11 +209,32 @@ int cagr_field_grid(const cagr_tree* tree, int op, int nx, int ny, int nz, const
  * buffers only the sizes are computed.  Synchronises `stream`.
  * The reference extracts the surface with PoissonRecon's adaptive octree MC
  * (gaussrecon_src/Octree.cpp:852-1090, tables MarchingCubes.cpp:32-324); this
- * uniform-grid MC uses its own generated case table (cagr_mc_table). */
+ * uniform-grid MC uses its own generated case table (cagr_mc_table), or the
+ * reference's table through cagr_marching_cubes_table. */
 int cagr_marching_cubes(const float* values_dev, int nx, int ny, int nz, const double* origin,
                         double spacing, double iso, float* vertices_dev, int64_t max_vertices,
                         int32_t* faces_dev, int64_t max_faces, int64_t* num_vertices,
                         int64_t* num_faces, void* stream);
+
+/* cagr_marching_cubes with a caller-supplied case table in the reference's
+ * layout (gaussrecon_src/MarchingCubes.cpp:32-324 triangles[256][16] with
+ * GetIndex at :333-345), replacing PoissonRecon's per-cube table lookup
+ * (MarchingCubes::AddTriangleIndices, :573-584) on a regular grid.
+ * triangles (host memory, 256 * 16 int8): row = case index whose bit k is set
+ * when corner {0, 1, 3, 2, 4, 5, 7, 6}[k] (corner c = x + 2y + 4z) has
+ * value < iso; entries = edge ids 4a + u + 2v as in cagr_mc_table, three per
+ * triangle, -1 after the last (at most 5 triangles).  Corners with value < iso
+ * are inside; vertices (one per crossed grid edge, in the same order and at
+ * the same positions as cagr_marching_cubes) are shared between cells, and the
+ * triangles of each cell are the table's, in its order and winding, cells in
+ * index order.  Returns CAGR_ERR_INVALID for a table with other entries or
+ * with a triangle on an edge its case does not cross; otherwise as
+ * cagr_marching_cubes. */
+int cagr_marching_cubes_table(const float* values_dev, int nx, int ny, int nz,
+                              const double* origin, double spacing, double iso,
+                              const int8_t* triangles, float* vertices_dev, int64_t max_vertices,
+                              int32_t* faces_dev, int64_t max_faces, int64_t* num_vertices,
+                              int64_t* num_faces, void* stream);
 
 /* The marching-cubes case table (host memory): tri[256 * 36] edge ids, three
  * per triangle, and ntri[256] triangle counts.  Corner c = x + 2y + 4z; edge

@@ -811,3 +811,98 @@ int oracle_interp_f64(int op, int cont, const double* q, const double* qw, const
     free(pchg);
     return 0;
 }
+
+/* Marching cubes with a case table in the reference's layout, restating its
+ * per-cube lookup: MarchingCubes::GetIndex (gaussrecon_src/MarchingCubes.cpp:
+ * 333-345; bit k set when the k-th corner of (0,0,0), (1,0,0), (1,1,0), (0,1,0),
+ * (0,0,1), (1,0,1), (1,1,1), (0,1,1) has value < iso), AddTriangleIndices
+ * (:573-584; the case's row of triangles[256][16] until -1) and
+ * Cube::EdgeCorners / FactorEdgeIndex (Cube.cpp:86-108; edge e runs along axis
+ * e >> 2 from corner (.., e & 1, (e >> 1) & 1) in the other two axes' order).
+ * Inside = value < iso.  Vertices: one per crossed grid edge, numbered and
+ * placed as in oracle_marching_cubes; faces: cells in index order, each case's
+ * triangles in the table's order.  Returns -2 for an entry that is not an
+ * edge the case crosses. */
+int oracle_marching_cubes_reftable(const float* v, int nx, int ny, int nz, double ox, double oy,
+                                   double oz, double h, float iso, const signed char* tri16,
+                                   float* verts, idx_t maxv, int* faces, idx_t maxf,
+                                   idx_t* nv_out, idx_t* nf_out) {
+    static const int corner_xyz[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                         {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    const idx_t P = (idx_t)nx * ny * nz, sx = 1, sy = nx, sz = (idx_t)nx * ny;
+    unsigned char* mask = calloc(P, 1);
+    idx_t* vbase = malloc(sizeof(idx_t) * (P + 1));
+    if (!mask || !vbase) {
+        free(mask);
+        free(vbase);
+        return -1;
+    }
+    const float fh = (float)h, fo[3] = {(float)ox, (float)oy, (float)oz};
+    idx_t nv = 0;
+    for (idx_t p = 0; p < P; p++) {
+        const int c[3] = {(int)(p % nx), (int)((p / nx) % ny), (int)(p / sz)};
+        const int n[3] = {nx, ny, nz};
+        const idx_t step[3] = {sx, sy, sz};
+        const int below = v[p] < iso;
+        unsigned char m = 0;
+        for (int ax = 0; ax < 3; ax++)
+            if (c[ax] + 1 < n[ax] && (v[p + step[ax]] < iso) != below) m |= (unsigned char)(1 << ax);
+        mask[p] = m;
+        vbase[p] = nv;
+        for (int ax = 0; ax < 3; ax++) {
+            if (!((m >> ax) & 1)) continue;
+            if (verts && nv < maxv) {
+                const float t = (iso - v[p]) / (v[p + step[ax]] - v[p]);
+                for (int d = 0; d < 3; d++) {
+                    const float x = fmaf((float)c[d], fh, fo[d]);
+                    verts[3 * nv + d] = d == ax ? x + t * fh : x;
+                }
+            }
+            nv++;
+        }
+    }
+    vbase[P] = nv;
+    idx_t nf = 0;
+    int rc = 0;
+    for (int k = 0; k + 1 < nz && !rc; k++) {
+        for (int j = 0; j + 1 < ny && !rc; j++) {
+            for (int i = 0; i + 1 < nx && !rc; i++) {
+                const idx_t p = (idx_t)k * sz + (idx_t)j * sy + i;
+                int idx = 0;
+                for (int q = 0; q < 8; q++) {
+                    const int* o = corner_xyz[q];
+                    if (v[p + o[0] * sx + o[1] * sy + o[2] * sz] < iso) idx |= 1 << q;
+                }
+                const signed char* row = tri16 + 16 * idx;
+                for (int q = 0; q < 15 && row[q] != -1; q += 3, nf++) {
+                    for (int s = 0; s < 3; s++) {
+                        const int e = row[q + s];
+                        if (e < 0 || e > 11) {
+                            rc = -2;
+                            break;
+                        }
+                        const int ax = e >> 2, a = e & 1, b = (e >> 1) & 1;
+                        int off[3];
+                        off[ax] = 0;
+                        off[ax == 0 ? 1 : 0] = a;
+                        off[ax == 2 ? 1 : 2] = b;
+                        const idx_t g = p + off[0] * sx + off[1] * sy + off[2] * sz;
+                        if (!((mask[g] >> ax) & 1)) {
+                            rc = -2;
+                            break;
+                        }
+                        int rank = 0;
+                        for (int t = 0; t < ax; t++) rank += (mask[g] >> t) & 1;
+                        if (faces && nf < maxf) faces[3 * nf + s] = (int)(vbase[g] + rank);
+                    }
+                    if (rc) break;
+                }
+            }
+        }
+    }
+    *nv_out = nv;
+    *nf_out = nf;
+    free(mask);
+    free(vbase);
+    return rc;
+}

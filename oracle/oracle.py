@@ -275,6 +275,35 @@ class Oracle:
             raise MemoryError("oracle marching cubes")
         return verts, faces
 
+    def marching_cubes_reftable(self, values: np.ndarray, origin, spacing: float, iso: float,
+                                triangles: np.ndarray):
+        """Regular-grid marching cubes with a case table in the reference's
+        layout (triangles [256, 16], MarchingCubes.cpp's GetIndex and
+        AddTriangleIndices restated; the checker of cagr_marching_cubes_table).
+        values: [nz, ny, nx] float32."""
+        v = np.ascontiguousarray(values, np.float32)
+        nz, ny, nx = v.shape
+        tri = np.ascontiguousarray(triangles, np.int8).reshape(-1)
+        assert tri.size == 256 * 16
+        f = self.lib.oracle_marching_cubes_reftable
+        f.restype = ctypes.c_int
+        f.argtypes = [_p, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 4 + \
+            [ctypes.c_float, _p, _p, _i64, _p, _i64, _p, _p]
+        nv, nf = ctypes.c_int64(), ctypes.c_int64()
+        args = [_ptr(v), nx, ny, nz, float(origin[0]), float(origin[1]), float(origin[2]),
+                float(spacing), float(iso), _ptr(tri)]
+        for _ in range(2):
+            verts = np.zeros((max(nv.value, 0), 3), np.float32)
+            faces = np.zeros((max(nf.value, 0), 3), np.int32)
+            rc = f(*args, _ptr(verts) if verts.size else None, nv.value,
+                   _ptr(faces) if faces.size else None, nf.value, ctypes.byref(nv),
+                   ctypes.byref(nf))
+            if rc == -1:
+                raise MemoryError("oracle marching cubes")
+            if rc == -2:
+                raise ValueError("table entry is not an edge the case crosses")
+        return verts, faces
+
     # -- the reference's per-call composition ----------------------------------
     def forward(self, op: str, tree: Tree, points: np.ndarray, values: np.ndarray,
                 widths: np.ndarray, queries: np.ndarray | None = None,

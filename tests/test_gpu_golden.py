@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-               if not os.path.basename(p).startswith("bunny"))
+               if not os.path.basename(p).startswith(("bunny", "mc_")))
 OPS = ["A", "AT", "A3", "A21", "A22", "A23", "A2T1", "A2T2", "A2T3", "G"]
 TREE_KEYS = ["parent", "children", "is_leaf", "half_w", "npts", "n2p", "n2p_start"]
 
