@@ -19,6 +19,10 @@
 // ((2^d + 1)^3 nodes over the unit cube), evaluated and contoured on the GPU
 // (cagr_field_grid, cagr_marching_cubes); -m (PGR's minimum depth) has no
 // meaning for a regular grid and is accepted for compatibility.
+// --op A selects the operator of the reference's CPU driver
+// (main_GaussRecon_cpu.cpp:280-318: multiply_by_A, continuous kernel) instead
+// of the CUDA driver's A3.  The run prints its phases: input parsing, device
+// set-up (context and uploads), the device work, output.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,12 +40,13 @@ namespace {
 
 const char* kUsage =
     "usage: main_GaussReconCUDA -i <input.xyz> -o <output.ply> [-w width=0.01] [-m minDepth=1] "
-    "[-d maxDepth=10]\n";
+    "[-d maxDepth=10] [--op A3|A]\n";
 
 struct Args {
     std::string in, out;
     float width = 0.01f;
     int min_depth = 1, max_depth = 10;
+    int op = CAGR_OP_A3;
 };
 
 bool parse(int argc, char** argv, Args* a) {
@@ -55,6 +60,8 @@ bool parse(int argc, char** argv, Args* a) {
         else if (k == "-w") a->width = std::strtof(v, &end);
         else if (k == "-m") a->min_depth = (int)std::strtol(v, &end, 10);
         else if (k == "-d") a->max_depth = (int)std::strtol(v, &end, 10);
+        else if (k == "--op" && std::strcmp(v, "A3") == 0) a->op = CAGR_OP_A3;
+        else if (k == "--op" && std::strcmp(v, "A") == 0) a->op = CAGR_OP_A;
         else return false;
         if (end && *end) return false;
     }
@@ -91,6 +98,34 @@ struct TreeGuard {
         if (t) cagr_tree_destroy(t);
     }
 };
+
+// Whole-file read of "x y z nx ny nz" records (whitespace separated; a
+// trailing incomplete record is ignored, as fscanf's loop would).
+bool read_xyz(const std::string& path, std::vector<float>& xyz, std::vector<float>& nml) {
+    FILE* fp = std::fopen(path.c_str(), "rb");
+    if (!fp) return false;
+    std::vector<char> buf;
+    char chunk[1 << 16];
+    size_t got;
+    while ((got = std::fread(chunk, 1, sizeof(chunk), fp)) > 0) buf.insert(buf.end(), chunk, chunk + got);
+    std::fclose(fp);
+    buf.push_back('\0');
+    const char* p = buf.data();
+    float r[6];
+    for (;;) {
+        int k = 0;
+        for (; k < 6; k++) {
+            char* end = nullptr;
+            r[k] = std::strtof(p, &end);
+            if (end == p) break;
+            p = end;
+        }
+        if (k < 6) break;
+        xyz.insert(xyz.end(), r, r + 3);
+        nml.insert(nml.end(), r + 3, r + 6);
+    }
+    return true;
+}
 
 bool write_ply(const std::string& path, const std::vector<float>& v, const std::vector<int32_t>& f) {
     FILE* fp = std::fopen(path.c_str(), "wb");
@@ -129,28 +164,23 @@ int main(int argc, char** argv) {
     const auto t_start = std::chrono::steady_clock::now();
 
     // ---- input: x y z nx ny nz per line (Octree.cpp:211-224) ----
-    FILE* fp = std::fopen(a.in.c_str(), "r");
-    if (!fp) {
+    std::vector<float> xyz, nml;
+    if (!read_xyz(a.in, xyz, nml)) {
         std::fprintf(stderr, "[main_GaussReconCUDA] cannot open %s\n", a.in.c_str());
         return 1;
     }
-    std::vector<float> xyz, nml;
-    float r[6];
-    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-    while (std::fscanf(fp, "%f %f %f %f %f %f", r, r + 1, r + 2, r + 3, r + 4, r + 5) == 6) {
-        for (int d = 0; d < 3; d++) {
-            if (xyz.empty() || r[d] > hi[d]) hi[d] = r[d];
-            if (xyz.empty() || r[d] < lo[d]) lo[d] = r[d];
-        }
-        xyz.insert(xyz.end(), r, r + 3);
-        nml.insert(nml.end(), r + 3, r + 6);
-    }
-    std::fclose(fp);
     const int64_t n = (int64_t)xyz.size() / 3;
     if (n == 0) {
         std::fprintf(stderr, "[main_GaussReconCUDA] no points in %s\n", a.in.c_str());
         return 1;
     }
+    float lo[3], hi[3];
+    for (int d = 0; d < 3; d++) lo[d] = hi[d] = xyz[d];
+    for (int64_t j = 1; j < n; j++)
+        for (int d = 0; d < 3; d++) {
+            hi[d] = std::max(hi[d], xyz[3 * j + d]);
+            lo[d] = std::min(lo[d], xyz[3 * j + d]);
+        }
     // ---- normalisation (Octree.cpp:244-261, main_GaussRecon_cuda.cu:270-288) ----
     const float scale = std::max(std::max(hi[0] - lo[0], hi[1] - lo[1]), hi[2] - lo[2]) * 1.1f;
     float corner[3];
@@ -165,12 +195,15 @@ int main(int argc, char** argv) {
         attrs[3 * j + 1] = ny / len * area;
         attrs[3 * j + 2] = nz / len * area;
     }
-    std::printf("[main_GaussReconCUDA] %lld points, grid depth %d, width %g\n", (long long)n,
-                a.max_depth, a.width);
+    std::printf("[main_GaussReconCUDA] %lld points, grid depth %d, width %g, operator %s\n",
+                (long long)n, a.max_depth, a.width, a.op == CAGR_OP_A ? "A" : "A3");
+    const double t_read = seconds_since(t_start);
 
     // ---- treecode field at the samples and at the grid nodes ----
+    const auto t_dev0 = std::chrono::steady_clock::now();
     cudaStream_t st = nullptr;
     cudaError_t ce;
+    if ((ce = cudaFree(nullptr))) return cuda_fail("CUDA context", ce);
     Dev d_pts, d_attrs, d_w, d_samples;
     if ((ce = d_pts.alloc(sizeof(float) * 3 * n)) || (ce = d_attrs.alloc(sizeof(float) * 3 * n)) ||
         (ce = d_w.alloc(sizeof(float) * n)) || (ce = d_samples.alloc(sizeof(float) * n)))
@@ -179,13 +212,16 @@ int main(int argc, char** argv) {
         (ce = cudaMemcpy(d_attrs.p, attrs.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice)) ||
         (ce = cudaMemcpy(d_w.p, weights.data(), sizeof(float) * n, cudaMemcpyHostToDevice)))
         return cuda_fail("cudaMemcpy", ce);
+    const double t_setup = seconds_since(t_dev0);
+    const auto t_gpu0 = std::chrono::steady_clock::now();
+    const char* opname = a.op == CAGR_OP_A ? "cagr_multiply(A)" : "cagr_multiply(A3)";
     TreeGuard tree;
     int rc = cagr_tree_build(d_pts.p, n, CAGR_F32, 15, 1, st, &tree.t);
     if (rc) return fail("cagr_tree_build", rc);
     if ((rc = cagr_scatter(tree.t, 0, d_attrs.p, 3, d_w.p, st))) return fail("cagr_scatter", rc);
-    if ((rc = cagr_multiply(tree.t, CAGR_OP_A3, nullptr, nullptr, n, nullptr, a.width,
+    if ((rc = cagr_multiply(tree.t, a.op, nullptr, nullptr, n, nullptr, a.width,
                             CAGR_FLAG_CONTINUOUS, d_samples.p, 0, st)))
-        return fail("cagr_multiply(A3)", rc);
+        return fail(opname, rc);
     std::vector<float> samples(n);
     if ((ce = cudaMemcpy(samples.data(), d_samples.p, sizeof(float) * n, cudaMemcpyDeviceToHost)))
         return cuda_fail("cudaMemcpy", ce);
@@ -198,25 +234,37 @@ int main(int argc, char** argv) {
     const size_t nodes = (size_t)g * g * g;
     Dev d_field;
     if ((ce = d_field.alloc(sizeof(float) * nodes))) return cuda_fail("cudaMalloc(field)", ce);
-    // grid value = -A3 (main_GaussRecon_cuda.cu:478)
-    if ((rc = cagr_field_grid(tree.t, CAGR_OP_A3, g, g, g, origin, spacing, nullptr, a.width,
+    // grid value = -A3 (main_GaussRecon_cuda.cu:478; -A in main_GaussRecon_cpu.cpp)
+    if ((rc = cagr_field_grid(tree.t, a.op, g, g, g, origin, spacing, nullptr, a.width,
                               CAGR_FLAG_CONTINUOUS | CAGR_FLAG_NEGATE, d_field.p, st)))
         return fail("cagr_field_grid", rc);
-    int64_t nv = 0, nf = 0;
-    if ((rc = cagr_marching_cubes((const float*)d_field.p, g, g, g, origin, spacing, iso, nullptr,
-                                  0, nullptr, 0, &nv, &nf, st)))
-        return fail("cagr_marching_cubes", rc);
+    // one pass over the grid into buffers of an estimated size (a surface
+    // crossing every layer: 8 vertices per cell column of a face), again with
+    // the exact sizes if the mesh is larger
+    int64_t nv = 8 * (int64_t)g * g, nf = 2 * nv + 1024;
     Dev d_v, d_f;
-    if ((ce = d_v.alloc(sizeof(float) * 3 * nv)) || (ce = d_f.alloc(sizeof(int32_t) * 3 * nf)))
-        return cuda_fail("cudaMalloc(mesh)", ce);
-    if ((rc = cagr_marching_cubes((const float*)d_field.p, g, g, g, origin, spacing, iso,
-                                  (float*)d_v.p, nv, (int32_t*)d_f.p, nf, &nv, &nf, st)))
-        return fail("cagr_marching_cubes", rc);
+    for (int attempt = 0;; attempt++) {
+        if ((ce = d_v.alloc(sizeof(float) * 3 * nv)) || (ce = d_f.alloc(sizeof(int32_t) * 3 * nf)))
+            return cuda_fail("cudaMalloc(mesh)", ce);
+        const int64_t cap_v = nv, cap_f = nf;
+        rc = cagr_marching_cubes((const float*)d_field.p, g, g, g, origin, spacing, iso,
+                                 (float*)d_v.p, cap_v, (int32_t*)d_f.p, cap_f, &nv, &nf, st);
+        if (rc == CAGR_ERR_OVERFLOW && attempt == 0 && (nv > cap_v || nf > cap_f)) {
+            cudaFree(d_v.p);
+            cudaFree(d_f.p);
+            d_v.p = d_f.p = nullptr;
+            continue;
+        }
+        if (rc) return fail("cagr_marching_cubes", rc);
+        break;
+    }
     std::vector<float> verts(3 * nv);
     std::vector<int32_t> faces(3 * nf);
     if ((ce = cudaMemcpy(verts.data(), d_v.p, sizeof(float) * 3 * nv, cudaMemcpyDeviceToHost)) ||
         (ce = cudaMemcpy(faces.data(), d_f.p, sizeof(int32_t) * 3 * nf, cudaMemcpyDeviceToHost)))
         return cuda_fail("cudaMemcpy", ce);
+    const double t_gpu = seconds_since(t_gpu0);
+    const auto t_out0 = std::chrono::steady_clock::now();
     // back to the input's coordinates (Octree.cpp:1262-1266, 1285-1287)
     for (int64_t i = 0; i < nv; i++)
         for (int d = 0; d < 3; d++)
@@ -227,5 +275,8 @@ int main(int argc, char** argv) {
     }
     std::printf("[main_GaussReconCUDA] iso-value %g, %lld vertices, %lld faces -> %s (%.3f s)\n",
                 iso, (long long)nv, (long long)nf, a.out.c_str(), seconds_since(t_start));
+    std::printf("[main_GaussReconCUDA] phases: input %.3f s, device set-up %.3f s, device work "
+                "(tree, moments, field, marching cubes, mesh copy) %.3f s, output %.3f s\n",
+                t_read, t_setup, t_gpu, seconds_since(t_out0));
     return 0;
 }
