@@ -26,6 +26,7 @@
 //     root-to-leaf walk, then a stable radix sort by node id.
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -195,13 +196,26 @@ __global__ void k_chain(const int8_t* __restrict__ lcp, int64_t n, int D, int s,
     isleafpos[i] = exists ? 1 : 0;
 }
 
-// sparse table level k from level k-1: st[k][j] = min(lcp[j .. j + 2^k - 1])
-__global__ void k_sparse_level(const int8_t* __restrict__ prev, int8_t* __restrict__ cur,
-                               int64_t n, int64_t half) {
-    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// sparse table: st[k][j] = min(lcp[j .. min(j + 2^k, n) - 1]).  One launch
+// writes levels k0 .. k0 + m - 1 (m <= kLevelsPerLaunch) from level k0 - 1:
+// level k0 - 1 + i at j is the min of prev[j + t h] over t < 2^i (h = 2^(k0-1),
+// positions past n skipped), the union of those windows being [j, j + 2^i h).
+// The strided reads of neighbouring threads are coalesced and come from L2.
+constexpr int kLevelsPerLaunch = 4;
+
+__global__ void k_sparse_levels(const int8_t* __restrict__ prev, int8_t* __restrict__ out,
+                                int64_t n, int64_t h, int m) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
-    int8_t a = prev[j];
-    cur[j] = (j + half < n) ? (int8_t)min((int)a, (int)prev[j + half]) : a;
+    int cur = prev[j];
+    int t = 1;
+    for (int i = 1; i <= m; i++) {
+        for (; t < (1 << i); t++) {
+            const int64_t x = j + (int64_t)t * h;
+            if (x < n) cur = min(cur, (int)prev[x]);
+        }
+        out[(int64_t)(i - 1) * n + j] = (int8_t)cur;
+    }
 }
 
 // first j > i with lcp[j] < d, or n
@@ -416,9 +430,10 @@ int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) 
     k_lcp<<<gN, kBlock, 0, st>>>(sk, n, D, lcp);
     k_chain<<<gN, kBlock, 0, st>>>(lcp, n, D, s, (int32_t*)nn.p, (int8_t*)d0a.p, (int8_t*)dla.p,
                                    (int32_t*)isleafpos.p);
-    for (int k = 1; k < K; k++)
-        k_sparse_level<<<gN, kBlock, 0, st>>>(lcp + (int64_t)(k - 1) * n, lcp + (int64_t)k * n, n,
-                                              int64_t(1) << (k - 1));
+    for (int k0 = 1; k0 < K; k0 += kLevelsPerLaunch)
+        k_sparse_levels<<<gN, kBlock, 0, st>>>(lcp + (int64_t)(k0 - 1) * n, lcp + (int64_t)k0 * n,
+                                               n, int64_t(1) << (k0 - 1),
+                                               std::min(kLevelsPerLaunch, K - k0));
     CAGR_CUDA(cudaGetLastError());
     if (int rc = cub_call(
             [&](void* tp, size_t& b) {
