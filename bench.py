@@ -40,6 +40,12 @@ UNIT = "ms"
 # + d.mu (5) + d.mu r^-3 (1) + r^-1/2 (1), then per direction 2 FMA (4):
 FLOPS_A2_FUSED = 29      # three directions
 FLOPS_A2T = 22           # d (3) + |d|^2 (5) + r^-3 (2) + e s r^-3 (2) + 3 FMA (6) + e s r^-1/2 (3) + add (1)
+# The interpolated A2T sum evaluates all three directions of a (query, source)
+# pair at once (cagr_b200/csrc/interp.cu, pterm, A2T sum): d (3) + |d|^2 (5)
+# + r^-3 (2) + g_k = exp(x_k/2) (exp(-y_k/2) s_k) (3) + sum g (2) + (sum g) r^-3 (1)
+# + r/2 (1) + per direction d_k c + g_k r/2 as 2 FMA (12); rsqrt not counted,
+# as in the counts above.  (Per-direction terms of the reference mode: 22 each.)
+FLOPS_IA2T_SUM = 29
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the two
 # traversals on this workload, taken from one ncu capture of these kernels with
@@ -547,10 +553,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     peak_tflops = gf.value / 1e3
 
     if interp is not None:
-        # FP32 work of the interpolated walks (the same flops per pair term as the
-        # reference-mode walks; a proxy term is a point term)
+        # FP32 work of the interpolated walks per (query, source) pair term, a proxy
+        # term counting as a point term: A2_FUSED as in the reference mode, the A2T
+        # sum with its three directions together
         ta = interp["pair_terms_A2"] * FLOPS_A2_FUSED / (interp["A2_FUSED_walk_ms"] * 1e-3) / 1e12
-        tt = interp["pair_terms_A2"] * FLOPS_A2T / (interp["A2T_SUM_walk_ms"] * 1e-3) / 1e12
+        tt = interp["pair_terms_A2"] * FLOPS_IA2T_SUM / (interp["A2T_SUM_walk_ms"] * 1e-3) / 1e12
+        interp["flops_per_pair_term"] = {"A2_FUSED": FLOPS_A2_FUSED, "A2T_SUM": FLOPS_IA2T_SUM}
         interp["A2_FUSED_tflops"], interp["A2_FUSED_fp32_frac"] = round(ta, 3), round(ta / peak_tflops, 4)
         interp["A2T_SUM_tflops"], interp["A2T_SUM_fp32_frac"] = round(tt, 3), round(tt / peak_tflops, 4)
     T, E = max_over_ranks([float(np.mean(step_ms)), float(np.mean(e2e_ms))], world, dev)

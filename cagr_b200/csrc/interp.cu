@@ -244,6 +244,20 @@ __global__ void k_ipoints(const T* __restrict__ spos, const int32_t* __restrict_
     write_rec(out, s, n, spos[3 * s], spos[3 * s + 1], spos[3 * s + 2], a0, a1, a2);
 }
 
+// The records of the three-column slot (sum_k A2Tk) in their walk form: the
+// exp factor e_k = exp(-y_k/2) replaced by its product with the column's
+// charge, e_k s_k, which is all the A2T sum reads of a source (the walk
+// multiplied the same two numbers for every pair; now once per record).
+template <typename T>
+__global__ void k_es_form(T* __restrict__ rec, int64_t nblocks) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 2 * nblocks) return;
+    T* b = rec + (i >> 1) * kBlk + (i & 1);
+    constexpr int kCharge[3] = {3, 7, 8};
+#pragma unroll
+    for (int k = 0; k < 3; k++) b[2 * (4 + k)] = b[2 * (4 + k)] * b[2 * kCharge[k]];
+}
+
 template <typename T>
 struct ChargeParams {
     const int4* chunks = nullptr;
@@ -592,13 +606,18 @@ __device__ __forceinline__ void pterm(const IQ<T>& q, const IQ2<T>& q2, const T*
             if constexpr (K == 1) p1 = fma2(half, gr, p1);
             if constexpr (K == 2) p2 = fma2(half, gr, p2);
         } else if constexpr (IOp<OP>::a2tsum) {
-            // sum_k exp(x_k/2) exp(-y_k/2) s_k (d / r^3 + e_k / (2r))
-            const P2<T> sa = k.c[3];
-            const P2<T> sb = OP == kIOpA2TSum ? k.c[7] : k.c[3];
-            const P2<T> sc = OP == kIOpA2TSum ? k.c[8] : k.c[3];
-            const P2<T> g0 = mul2(q2.ex0, mul2(k.c[4], sa));
-            const P2<T> g1 = mul2(q2.ex1, mul2(k.c[5], sb));
-            const P2<T> g2 = mul2(q2.ex2, mul2(k.c[6], sc));
+            // sum_k exp(x_k/2) exp(-y_k/2) s_k (d / r^3 + e_k / (2r)); the three-column
+            // slot's records hold exp(-y_k/2) s_k (k_es_form), the shared one e_k and s
+            P2<T> g0, g1, g2;
+            if constexpr (OP == kIOpA2TSum) {
+                g0 = mul2(q2.ex0, k.c[4]);
+                g1 = mul2(q2.ex1, k.c[5]);
+                g2 = mul2(q2.ex2, k.c[6]);
+            } else {
+                g0 = mul2(q2.ex0, mul2(k.c[4], k.c[3]));
+                g1 = mul2(q2.ex1, mul2(k.c[5], k.c[3]));
+                g2 = mul2(q2.ex2, mul2(k.c[6], k.c[3]));
+            }
             const P2<T> c = mul2(add2(add2(g0, g1), g2), r3);
             const P2<T> hr = mul2(half, r);
             p0 = fma2(dx, c, fma2(g0, hr, p0));
@@ -1200,6 +1219,11 @@ int scatter_impl(Tree* t, Interp* I, int slot, const void* attrs, int dim, cudaS
         k_charges_finish<T><<<blocks_for(I->num_interp * P3e, 256), 256, 0, s>>>(
             I->chunk_first, I->num_interp, I->chunks, (const T*)I->part, (const T*)I->box_c,
             (const T*)I->box_h, cp, (T*)I->prox[slot]);
+    }
+    if (slot == 3) {  // the A2T sum's slot: e_k s_k in place of e_k
+        const int64_t pb = (N + 1) / 2, xb = I->num_interp * P3e / 2;
+        k_es_form<T><<<blocks_for(2 * pb, 256), 256, 0, s>>>((T*)I->pts[slot], pb);
+        if (xb > 0) k_es_form<T><<<blocks_for(2 * xb, 256), 256, 0, s>>>((T*)I->prox[slot], xb);
     }
     CAGR_CUDA(cudaGetLastError());
     I->dim[slot] = dim;
