@@ -842,15 +842,16 @@ int dispatch(const Tree* t, const TraverseArgs& a, cudaStream_t s) {
 // component); k_adj_push adds the leaf-to-root node sums to each point's own.
 
 // The warp sum of (a, b, c) over the lanes with `take` (all of them use the
-// same node or point).  PASS 1 records its largest magnitude in *vmax (the
-// bits of a non-negative double order as its value; NaN above infinity);
-// pass 2 adds round(sum * scale) to the integer accumulators dst[0..2].  The
+// same node or point).  PASS 1 keeps its largest magnitude in the leader
+// lane's running maximum vm (non-finite sums as infinity; each warp publishes
+// its maximum once, at the end of its walk); pass 2 adds round(sum * sc) to
+// the integer accumulators dst[0..2].  The
 // warp sum has a fixed shuffle order and integer addition is associative, so
 // the accumulated gradient is the same bits on every run (float atomics would
 // add in the order the warps arrive).
 template <bool PASS1, typename T>
 __device__ __forceinline__ void warp_red3(bool take, T a, T b, T c, unsigned long long* dst,
-                                          unsigned long long* vmax, const double* scale) {
+                                          double& vm, double sc) {
     const unsigned m = __ballot_sync(kFull, take);
     if (m == 0u) return;
     if (!take) a = b = c = T(0);
@@ -866,9 +867,8 @@ __device__ __forceinline__ void warp_red3(bool take, T a, T b, T c, unsigned lon
         if constexpr (PASS1) {
             const double mx = fmax(fabs((double)a), fmax(fabs((double)b), fabs((double)c)));
             const bool bad = !(mx <= 1.0e300);  // NaN or infinite
-            atomicMax(vmax, (unsigned long long)__double_as_longlong(bad ? (double)INFINITY : mx));
+            vm = fmax(vm, bad ? (double)INFINITY : mx);
         } else {
-            const double sc = *scale;
             atomicAdd(dst, (unsigned long long)llrint((double)a * sc));
             atomicAdd(dst + 1, (unsigned long long)llrint((double)b * sc));
             atomicAdd(dst + 2, (unsigned long long)llrint((double)c * sc));
@@ -934,6 +934,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_adjoint_a2(const TravParams<T> 
     const T G[3] = {gs[0] * exp_t(L.q0 * T(0.5)), gs[1] * exp_t(L.q1 * T(0.5)),
                     gs[2] * exp_t(L.q2 * T(0.5))};
     const T ew = CONT ? exp_t(w) : T(0);
+    double vm = 0.0;                          // pass 1: this lane's largest warp sum
+    const double sc = PASS1 ? 0.0 : *p.scale;  // pass 2: the fixed-point scale
 
     const int M = (int)p.M;
     const T* __restrict__ rec = p.rec[0];
@@ -968,18 +970,15 @@ __global__ void __launch_bounds__(kWarps * 32) k_adjoint_a2(const TravParams<T> 
             }
             T v[3];
             adj_term<T, CONT>(L, src, dx, dy, dz, d2, G, gs, ew, v);
-            warp_red3<PASS1>(active && !use_pt, v[0], v[1], v[2], p.accn + (int64_t)n * 3, p.vmax,
-                             p.scale);
-            warp_red3<PASS1>(active && use_pt, v[0], v[1], v[2], p.accp + (int64_t)mt.y * 3, p.vmax,
-                             p.scale);
+            warp_red3<PASS1>(active && !use_pt, v[0], v[1], v[2], p.accn + (int64_t)n * 3, vm, sc);
+            warp_red3<PASS1>(active && use_pt, v[0], v[1], v[2], p.accp + (int64_t)mt.y * 3, vm, sc);
             n = mt.x;
             continue;
         }
         {
             T v[3];
             adj_term<T, CONT>(L, r, dx, dy, dz, d2, G, gs, ew, v);
-            warp_red3<PASS1>(active && far, v[0], v[1], v[2], p.accn + (int64_t)n * 3, p.vmax,
-                             p.scale);
+            warp_red3<PASS1>(active && far, v[0], v[1], v[2], p.accn + (int64_t)n * 3, vm, sc);
         }
         if (leaf) {
             const int np = -mt.z;
@@ -992,14 +991,20 @@ __global__ void __launch_bounds__(kWarps * 32) k_adjoint_a2(const TravParams<T> 
                     const T ez = sub_rn(L.q2, s0.z);
                     T v[3];
                     adj_term<T, CONT>(L, pr, ex, ey, ez, dist2_exact(ex, ey, ez), G, gs, ew, v);
-                    warp_red3<PASS1>(open, v[0], v[1], v[2], p.accp + ((int64_t)mt.y + j) * 3,
-                                     p.vmax, p.scale);
+                    warp_red3<PASS1>(open, v[0], v[1], v[2], p.accp + ((int64_t)mt.y + j) * 3, vm,
+                                     sc);
                 }
             }
             n = mt.x;
         } else {
             n = any_open ? n + 1 : mt.x;
         }
+    }
+    if constexpr (PASS1) {
+        // one atomic per warp (the bits of a non-negative double order as its value)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vm = fmax(vm, __shfl_xor_sync(kFull, vm, o));
+        if (lane == 0) atomicMax(p.vmax, (unsigned long long)__double_as_longlong(vm));
     }
 }
 
