@@ -53,7 +53,6 @@ namespace {
 
 constexpr int kMaxTri = 12;  // the generator checks the bound
 constexpr int kChunk = 128;  // grid points per unit
-constexpr int kEmitUnits = 256;  // units an emit block scans
 
 struct McTable {
     int8_t tri[256][3 * kMaxTri];
@@ -276,35 +275,6 @@ __device__ __forceinline__ bool inside(float v, float iso) {
     return v > iso;
 }
 
-__device__ __forceinline__ int64_t gid(const Grid& g, int i, int j, int k) {
-    return ((int64_t)k * g.ny + j) * g.nx + i;
-}
-
-// crossed edges owned by grid point (i, j, k): bit a = the edge toward +axis a
-template <bool BELOW>
-__device__ __forceinline__ uint32_t point_mask(const float* __restrict__ v, const Grid& g, int i,
-                                               int j, int k) {
-    const int64_t p = gid(g, i, j, k);
-    const bool a = inside<BELOW>(v[p], g.iso);
-    uint32_t m = 0;
-    if (i + 1 < g.nx && inside<BELOW>(v[p + 1], g.iso) != a) m |= 1;
-    if (j + 1 < g.ny && inside<BELOW>(v[p + g.nx], g.iso) != a) m |= 2;
-    if (k + 1 < g.nz && inside<BELOW>(v[p + (int64_t)g.nx * g.ny], g.iso) != a) m |= 4;
-    return m;
-}
-
-template <bool BELOW>
-__device__ __forceinline__ int cell_case(const float* __restrict__ v, const Grid& g, int64_t p) {
-    const int64_t sx = 1, sy = g.nx, sz = (int64_t)g.nx * g.ny;
-    int c = 0;
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-        const int64_t o = (q & 1) * sx + ((q >> 1) & 1) * sy + (q >> 2) * sz;
-        c |= inside<BELOW>(v[p + o], g.iso) ? (1 << q) : 0;
-    }
-    return c;
-}
-
 // root position on a crossed edge: t = (iso - v0) / (v1 - v0), reference rounding
 __device__ __forceinline__ float root_t(float v0, float v1, float iso) {
     return __fdiv_rn(__fsub_rn(iso, v0), __fsub_rn(v1, v0));
@@ -313,9 +283,6 @@ __device__ __forceinline__ float root_t(float v0, float v1, float iso) {
 // A unit is kChunk consecutive grid points of one x-row (and the cells whose
 // lowest corner they are).  Units in (row, chunk) order are in grid-point order,
 // so per-unit counts scanned give each unit's first vertex and triangle.
-struct Unit {
-    int i0, j, k, chunk;
-};
 
 // per unit: vertices (crossed edges owned by its points), triangles (its cells).
 // A warp takes kCountZ units stacked along z at one (chunk, j), kCountWarps
@@ -323,27 +290,54 @@ struct Unit {
 // (j+1, k), (j, k+1), (j+1, k+1); walking up in k, the k+1 rows of one unit are
 // the k rows of the next, so each unit reads two new rows, and the rows of the
 // unit after next are loaded before this one is counted (their latency overlaps
-// the bit work).  Lane l holds the points x = i0 + l + 32 q (q < 4, coalesced);
-// ballots turn them into inside-bit words w[q] held by every lane (w[4] bit 0:
-// the next unit's first point).  A funnel shift of (w[q+1] : w[q]) by l gives
-// the inside bits of x and x + 1, so a point's crossings and cell case are a
-// few bit operations.
+// the work).  Lane l holds the points x = i0 + l + 32 q (q < 4, coalesced) and
+// lane 0 also x = i0 + kChunk (the next unit's first point).
+//
+// Most units lie away from the surface: every point of their 4 rows is on the
+// same side.  Each row keeps, per lane, the minimum and maximum of its points
+// (a point outside the grid or in a missing row loads as NaN, which fmin and
+// fmax ignore; a NaN value of the field, which is outside, loads as -inf, or
+// +inf when inside means below the iso-value); two warp votes on the 4 rows'
+// extremes then settle such a unit with no bit work.  The others are counted
+// from ballots:
+// inside-bit words w[q] held by every lane, where a funnel shift of
+// (w[q+1] : w[q]) by l gives the inside bits of x and x + 1, so a point's
+// crossings and cell case are a few bit operations.
 constexpr int kCountWarps = 4;
 constexpr int kCountZ = 8;
 
 struct RowVals {
     float v[5];  // x = i0 + lane + 32 q, and (lane 0) x = i0 + kChunk
+    float lo, hi;  // their minimum and maximum (points that do not exist ignored)
 };
 
-__device__ __forceinline__ void load_row(const float* __restrict__ row, bool ok, int i0, int nx,
-                                         int lane, RowVals& r) {
+// The field value as the early-out compares it: NaN (outside) as the side
+// that is never inside.
+template <bool BELOW>
+__device__ __forceinline__ float sided(float x) {
+    return x == x ? x : (BELOW ? INFINITY : -INFINITY);
+}
+
+// The row's values at this lane's points (the row's pointer is only formed
+// for rows inside the grid); a point that does not exist (ok = false: a
+// missing row) loads as NaN.
+template <bool BELOW>
+__device__ __forceinline__ void load_row(const float* __restrict__ v, const Grid& g, int j, int k,
+                                         bool ok, int i0, int lane, RowVals& r) {
+    const float* row = v + ((int64_t)min(k, g.nz - 1) * g.ny + min(j, g.ny - 1)) * g.nx;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         const int x = i0 + lane + 32 * q;
-        r.v[q] = (ok && x < nx) ? row[x] : 0.0f;
+        r.v[q] = (ok && x < g.nx) ? sided<BELOW>(row[x]) : NAN;
     }
     const int x = i0 + kChunk;
-    r.v[4] = (ok && lane == 0 && x < nx) ? row[x] : 0.0f;
+    r.v[4] = (ok && lane == 0 && x < g.nx) ? sided<BELOW>(row[x]) : NAN;
+}
+
+template <bool BELOW>
+__device__ __forceinline__ void row_flags(const Grid&, bool, int, int, RowVals& r) {
+    r.lo = fminf(fminf(fminf(r.v[0], r.v[1]), fminf(r.v[2], r.v[3])), r.v[4]);
+    r.hi = fmaxf(fmaxf(fmaxf(r.v[0], r.v[1]), fmaxf(r.v[2], r.v[3])), r.v[4]);
 }
 
 template <bool BELOW>
@@ -362,179 +356,274 @@ template <bool BELOW>
 __global__ void __launch_bounds__(32 * kCountWarps) k_mc_count(const float* __restrict__ v, Grid g,
                                                                 const uint8_t* __restrict__ ntri,
                                                                 int32_t* __restrict__ vcnt,
-                                                                int32_t* __restrict__ tcnt) {
+                                                                int32_t* __restrict__ tcnt,
+                                                                int32_t* __restrict__ active,
+                                                                uint32_t* __restrict__ nactive) {
     const int lane = (int)threadIdx.x & 31;
     const int j = (int)blockIdx.y * kCountWarps + ((int)threadIdx.x >> 5);
     if (j >= g.ny) return;  // whole warps; no block barrier in this kernel
     const int i0 = (int)blockIdx.x * kChunk;
     const int k0 = (int)blockIdx.z * kCountZ, k1 = min(k0 + kCountZ, g.nz);
     const bool has_y = j + 1 < g.ny;
-    // row (j + dy, k) starts at v + (k ny + j + dy) nx; a missing row is not read
-    auto row = [&](int dy, int k) {
-        return v + ((int64_t)min(k, g.nz - 1) * g.ny + min(j + dy, g.ny - 1)) * g.nx;
-    };
-    RowVals a0, a1, b0, b1;  // raw rows k+1 (a) and k+2 (b) in flight
-    uint32_t c0[5], c1[5], n0[5], n1[5];  // bits of rows k (c) and k+1 (n)
-    load_row(row(0, k0), true, i0, g.nx, lane, a0);
-    load_row(row(1, k0), has_y, i0, g.nx, lane, a1);
-    load_row(row(0, k0 + 1), k0 + 1 < g.nz, i0, g.nx, lane, b0);
-    load_row(row(1, k0 + 1), has_y && k0 + 1 < g.nz, i0, g.nx, lane, b1);
-    row_bits<BELOW>(a0, true, i0, g.nx, lane, g.iso, c0);
-    row_bits<BELOW>(a1, has_y, i0, g.nx, lane, g.iso, c1);
-    for (int k = k0; k < k1; k++) {
-        const bool has_z = k + 1 < g.nz;
-        row_bits<BELOW>(b0, has_z, i0, g.nx, lane, g.iso, n0);
-        row_bits<BELOW>(b1, has_y && has_z, i0, g.nx, lane, g.iso, n1);
-        if (k + 1 < k1) {  // the rows of the next unit's k + 1
-            load_row(row(0, k + 2), k + 2 < g.nz, i0, g.nx, lane, b0);
-            load_row(row(1, k + 2), has_y && k + 2 < g.nz, i0, g.nx, lane, b1);
-        }
-        uint32_t packed = 0;  // vertices + 2^16 * triangles of this lane's 4 points
+    // rows (j, k) and (j+1, k) in slot (k - k0) % 3: the unit's k, its k + 1,
+    // and k + 2 in flight (the loop is unrolled, so slots are registers)
+    RowVals ra[3], rb[3];
+    load_row<BELOW>(v, g, j, k0, true, i0, lane, ra[0]);
+    load_row<BELOW>(v, g, j + 1, k0, has_y, i0, lane, rb[0]);
+    load_row<BELOW>(v, g, j, k0 + 1, k0 + 1 < g.nz, i0, lane, ra[1]);
+    load_row<BELOW>(v, g, j + 1, k0 + 1, has_y && k0 + 1 < g.nz, i0, lane, rb[1]);
+    row_flags<BELOW>(g, true, i0, lane, ra[0]);
+    row_flags<BELOW>(g, has_y, i0, lane, rb[0]);
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int x = i0 + lane + 32 * q;
-            // bit 0: inside at x, bit 1: inside at x + 1, in rows (dy, dz) = r
-            const uint32_t p0 = __funnelshift_r(c0[q], c0[q + 1], lane) & 3u;
-            const uint32_t p1 = __funnelshift_r(c1[q], c1[q + 1], lane) & 3u;
-            const uint32_t p2 = __funnelshift_r(n0[q], n0[q + 1], lane) & 3u;
-            const uint32_t p3 = __funnelshift_r(n1[q], n1[q + 1], lane) & 3u;
-            const bool has_x = x + 1 < g.nx;
-            // crossings owned by x (bits past the grid and of missing rows are 0,
-            // so only the +x edge of the last point and the missing rows need masks)
-            packed += (has_x ? ((p0 ^ (p0 >> 1)) & 1u) : 0u) + (has_y ? ((p0 ^ p1) & 1u) : 0u) +
-                      (has_z ? ((p0 ^ p2) & 1u) : 0u);
-            if (has_x && has_y && has_z)
-                packed += (uint32_t)__ldg(&ntri[p0 | (p1 << 2) | (p2 << 4) | (p3 << 6)]) << 16;
+    for (int kk = 0; kk < kCountZ; kk++) {
+        const int k = k0 + kk;
+        if (k >= k1) break;
+        const int s0 = kk % 3, s1 = (kk + 1) % 3, s2 = (kk + 2) % 3;
+        const bool has_z = k + 1 < g.nz;
+        if (kk + 1 < kCountZ && k + 1 < k1) {  // the rows of the next unit's k + 1
+            load_row<BELOW>(v, g, j, k + 2, k + 2 < g.nz, i0, lane, ra[s2]);
+            load_row<BELOW>(v, g, j + 1, k + 2, has_y && k + 2 < g.nz, i0, lane, rb[s2]);
         }
-        const uint32_t sum = __reduce_add_sync(0xffffffffu, packed);
+        row_flags<BELOW>(g, has_z, i0, lane, ra[s1]);
+        row_flags<BELOW>(g, has_y && has_z, i0, lane, rb[s1]);
+        // (every lane: NaN extremes, no point, compare false and vote neither way)
+        const float lo = fminf(fminf(ra[s0].lo, rb[s0].lo), fminf(ra[s1].lo, rb[s1].lo));
+        const float hi = fmaxf(fmaxf(ra[s0].hi, rb[s0].hi), fmaxf(ra[s1].hi, rb[s1].hi));
+        const bool lane_all = BELOW ? !(hi >= g.iso) : !(lo <= g.iso);  // every point inside
+        const bool lane_any = BELOW ? lo < g.iso : hi > g.iso;           // some point inside
+        const bool all_in = __all_sync(0xffffffffu, lane_all);
+        const bool any_in = __any_sync(0xffffffffu, lane_any);
+        uint32_t sum = 0;  // vertices + 2^16 * triangles of the unit
+        if (any_in && !all_in) {
+            uint32_t w0[5], w1[5], w2[5], w3[5];
+            row_bits<BELOW>(ra[s0], true, i0, g.nx, lane, g.iso, w0);
+            row_bits<BELOW>(rb[s0], has_y, i0, g.nx, lane, g.iso, w1);
+            row_bits<BELOW>(ra[s1], has_z, i0, g.nx, lane, g.iso, w2);
+            row_bits<BELOW>(rb[s1], has_y && has_z, i0, g.nx, lane, g.iso, w3);
+            uint32_t packed = 0;  // this lane's 4 points
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int x = i0 + lane + 32 * q;
+                // bit 0: inside at x, bit 1: inside at x + 1, in rows (dy, dz)
+                const uint32_t b0 = __funnelshift_r(w0[q], w0[q + 1], lane) & 3u;
+                const uint32_t b1 = __funnelshift_r(w1[q], w1[q + 1], lane) & 3u;
+                const uint32_t b2 = __funnelshift_r(w2[q], w2[q + 1], lane) & 3u;
+                const uint32_t b3 = __funnelshift_r(w3[q], w3[q + 1], lane) & 3u;
+                const bool has_x = x + 1 < g.nx;
+                // crossings owned by x (bits past the grid and of missing rows are 0,
+                // so only the +x edge of the last point and the missing rows need masks)
+                packed += (has_x ? ((b0 ^ (b0 >> 1)) & 1u) : 0u) +
+                          (has_y ? ((b0 ^ b1) & 1u) : 0u) + (has_z ? ((b0 ^ b2) & 1u) : 0u);
+                if (has_x && has_y && has_z)
+                    packed += (uint32_t)__ldg(&ntri[b0 | (b1 << 2) | (b2 << 4) | (b3 << 6)]) << 16;
+            }
+            sum = __reduce_add_sync(0xffffffffu, packed);
+        }
         if (lane == 0) {
             const int64_t u = ((int64_t)k * g.ny + j) * g.nchunks + blockIdx.x;
             vcnt[u] = (int32_t)(sum & 0xffffu);
             tcnt[u] = (int32_t)(sum >> 16);
-        }
-#pragma unroll
-        for (int q = 0; q < 5; q++) {
-            c0[q] = n0[q];
-            c1[q] = n1[q];
+            if (sum != 0u) active[atomicAdd(nactive, 1u)] = (int32_t)u;  // order is free
         }
     }
 }
 
-// per unit: its vertices, and its cells' triangles as vertex indices.  A cell's
-// edges are owned by points in 4 point rows (dy, dz in {0, 1}) at x = i or i + 1;
-// each row's in-unit vertex prefix comes from one block scan of 4 packed 16-bit
-// counts, and x = i0 + kChunk (the next unit's first point) from that unit's base.
+// per unit with output: its vertices, and its cells' triangles as vertex
+// indices.  One warp per listed unit (grid-stride over the count kernel's
+// list; the outputs go to the scanned positions, so the list order does not
+// matter).  A cell's edges are owned by points of the 4 point rows R = dy +
+// 2 dz (dy, dz in {0, 1}) at x or x + 1; a point's crossed edges need its +y
+// and +z neighbour rows too, so the warp reads 8 rows: (j + dy, k + dz) for
+// the 4 point rows and (j + 2, k), (j + 2, k + 1), (j, k + 2), (j + 1, k + 2);
+// lanes 0 and 1 also read x = i0 + 128 and i0 + 129.
+// From the rows' inside-bit words (ballots) every lane forms, per point row,
+// the crossed-edge words and their prefix counts, and writes each of its
+// points' edge mask and in-unit vertex prefix to per-warp shared memory; a
+// triangle's vertex is then that point's unit base + prefix + the edge's rank
+// among the point's crossed edges (the next unit's base for x = i0 + 128).
+constexpr int kEmitWarps = 4;
+
 template <bool BELOW>
-__global__ void __launch_bounds__(kChunk) k_mc_emit(const float* __restrict__ v, Grid g,
-                                                     const int8_t* __restrict__ tri,
-                                                     const uint8_t* __restrict__ ntri,
-                                                     const int64_t* __restrict__ vbase,
-                                                     const int64_t* __restrict__ tbase,
-                                                     float* __restrict__ verts,
-                                                     int32_t* __restrict__ faces,
-                                                     int64_t max_verts, int64_t max_faces) {
-    using ScanV = cub::BlockScan<unsigned long long, kChunk>;
-    using ScanT = cub::BlockScan<int32_t, kChunk>;
-    __shared__ typename ScanV::TempStorage tmp_v;
-    __shared__ typename ScanT::TempStorage tmp_t;
-    __shared__ uint8_t s_mask[4][kChunk + 1];
-    __shared__ unsigned long long s_pre[kChunk];
-    __shared__ int64_t s_base[4], s_next[4];
-    __shared__ int32_t s_list[kEmitUnits];
-    __shared__ int s_count;
-    // the block's kEmitUnits consecutive units: the ones with vertices or
-    // triangles (a small part of the grid) are listed, then emitted one by one
-    // (outputs go to the scanned positions, so the list order does not matter)
-    const int64_t u0 = (int64_t)blockIdx.x * kEmitUnits;
-    if (threadIdx.x == 0) s_count = 0;
-    __syncthreads();
-    for (int a = (int)threadIdx.x; a < kEmitUnits; a += kChunk) {
-        const int64_t u = u0 + a;
-        if (u < g.units && (vbase[u + 1] != vbase[u] || tbase[u + 1] != tbase[u]))
-            s_list[atomicAdd(&s_count, 1)] = a;
-    }
-    __syncthreads();
-    const int count = s_count;
-    for (int a = 0; a < count; a++) {
-        if (a > 0) __syncthreads();  // the previous unit is done with the shared arrays
-        const int64_t u = u0 + s_list[a];
-        Unit U;
-        U.chunk = (int)(u % g.nchunks);
-        const int64_t row = u / g.nchunks;
-        U.j = (int)(row % g.ny);
-        U.k = (int)(row / g.ny);
-        U.i0 = U.chunk * kChunk;
-        const int t = (int)threadIdx.x;
-        const int i = U.i0 + t;
-        const bool cell_row = U.j + 1 < g.ny && U.k + 1 < g.nz;
-        const int rows = cell_row ? 4 : 1;
-        unsigned long long c = 0;
-        uint32_t own = 0;
-        for (int r = 0; r < rows; r++) {
-            const uint32_t m =
-                i < g.nx ? point_mask<BELOW>(v, g, i, U.j + (r & 1), U.k + (r >> 1)) : 0u;
-            if (r == 0) own = m;
-            s_mask[r][t] = (uint8_t)m;
-            c |= (unsigned long long)__popc(m) << (16 * r);
+__global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __restrict__ v, Grid g,
+                                                              const int8_t* __restrict__ tri,
+                                                              const uint8_t* __restrict__ ntri,
+                                                              const int64_t* __restrict__ vbase,
+                                                              const int64_t* __restrict__ tbase,
+                                                              const int32_t* __restrict__ active,
+                                                              const uint32_t* __restrict__ nactive,
+                                                              float* __restrict__ verts,
+                                                              int32_t* __restrict__ faces,
+                                                              int64_t max_verts, int64_t max_faces) {
+    __shared__ uint8_t s_m[kEmitWarps][4][kChunk + 1];     // crossed edges (bit a: +axis a)
+    __shared__ uint16_t s_pre[kEmitWarps][4][kChunk];      // in-unit vertex prefix
+    __shared__ int64_t s_base[kEmitWarps][8];              // R: unit base; 4 + R: next unit's
+    const int lane = (int)threadIdx.x & 31, wid = (int)threadIdx.x >> 5;
+    const uint32_t n_act = *nactive;
+    for (uint32_t a = blockIdx.x * kEmitWarps + wid; a < n_act; a += gridDim.x * kEmitWarps) {
+        const int64_t u = active[a];
+        const int chunk = (int)(u % g.nchunks);
+        const int64_t rowid = u / g.nchunks;
+        const int j = (int)(rowid % g.ny), k = (int)(rowid / g.ny);
+        const int i0 = chunk * kChunk;
+        // the unit bases, issued with the rows' loads: lane R < 4 the unit of point
+        // row R, lane 4 + R the next unit of that row, lane 8 this unit's triangles
+        int64_t base = 0;
+        {
+            const int R = lane & 3, dy = R & 1, dz = R >> 1;
+            const int64_t uR = ((int64_t)(k + dz) * g.ny + (j + dy)) * g.nchunks + chunk;
+            const bool rok = j + dy < g.ny && k + dz < g.nz;
+            if (lane < 4 && rok) base = vbase[uR];
+            else if (lane < 8 && rok && chunk + 1 < g.nchunks) base = vbase[uR + 1];
+            else if (lane == 8) base = tbase[u];
         }
-        int cs = 0, nt = 0;
-        if (cell_row && i + 1 < g.nx) {
-            cs = cell_case<BELOW>(v, g, gid(g, i, U.j, U.k));
-            nt = __ldg(&ntri[cs]);
+        // rows: 0..3 = point rows (dy, dz) = (R & 1, R >> 1); 4, 5 = (2, 0), (2, 1);
+        // 6, 7 = (0, 2), (1, 2)
+        constexpr int kDy[8] = {0, 1, 0, 1, 2, 2, 0, 1}, kDz[8] = {0, 0, 1, 1, 0, 1, 2, 2};
+        uint32_t w[8][5];
+        float val[3][5];  // raw values of point rows 0, 1, 2 (the vertex roots)
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+            const int jj = j + kDy[r], kz = k + kDz[r];
+            const bool ok = jj < g.ny && kz < g.nz;
+            const float* row = v + ((int64_t)min(kz, g.nz - 1) * g.ny + min(jj, g.ny - 1)) * g.nx;
+            float x5[5];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int x = i0 + lane + 32 * q;
+                x5[q] = (ok && x < g.nx) ? row[x] : 0.0f;
+            }
+            const int xe = i0 + kChunk + lane;  // lanes 0, 1: x = i0 + 128, i0 + 129
+            x5[4] = (ok && lane < 2 && xe < g.nx) ? row[xe] : 0.0f;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int x = i0 + lane + 32 * q;
+                w[r][q] = __ballot_sync(0xffffffffu, ok && x < g.nx && inside<BELOW>(x5[q], g.iso));
+            }
+            w[r][4] = __ballot_sync(0xffffffffu,
+                                    ok && lane < 2 && xe < g.nx && inside<BELOW>(x5[4], g.iso));
+            if (r < 3)
+#pragma unroll
+                for (int q = 0; q < 5; q++) val[r][q] = x5[q];
         }
-        unsigned long long cpre;
-        int32_t tpre;
-        ScanV(tmp_v).ExclusiveSum(c, cpre);
-        ScanT(tmp_t).ExclusiveSum(nt, tpre);
-        s_pre[t] = cpre;
-        if (t < rows) {
-            const int64_t row = (int64_t)(U.k + (t >> 1)) * g.ny + (U.j + (t & 1));
-            s_base[t] = vbase[row * g.nchunks + U.chunk];
-            if (U.chunk + 1 < g.nchunks) {
-                s_next[t] = vbase[row * g.nchunks + U.chunk + 1];
-                s_mask[t][kChunk] = (uint8_t)point_mask<BELOW>(v, g, U.i0 + kChunk, U.j + (t & 1),
-                                                               U.k + (t >> 1));
+        // per point row: crossed-edge words, each lane's points' masks and prefixes
+        const bool row_ok[4] = {true, j + 1 < g.ny, k + 1 < g.nz, j + 1 < g.ny && k + 1 < g.nz};
+        const int ny_of[4] = {1, 4, 3, 5};  // the row one step +y of point row R
+        const int nz_of[4] = {2, 3, 6, 7};  // the row one step +z of point row R
+        uint32_t m0[4];  // this lane's points' crossed edges in row 0
+#pragma unroll
+        for (int R = 0; R < 4; R++) {
+            const int dy = R & 1, dz = R >> 1;
+            const bool yok = row_ok[R] && j + dy + 1 < g.ny;
+            const bool zok = row_ok[R] && k + dz + 1 < g.nz;
+            uint32_t cum = 0;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int xl = g.nx - 1 - (i0 + 32 * q);  // bits whose point has x + 1 < nx
+                const uint32_t X = (w[R][q] ^ __funnelshift_r(w[R][q], w[R][q + 1], 1)) &
+                                   (xl >= 32 ? 0xffffffffu : (xl <= 0 ? 0u : (1u << xl) - 1u));
+                const uint32_t Y = yok ? (w[R][q] ^ w[ny_of[R]][q]) : 0u;
+                const uint32_t Z = zok ? (w[R][q] ^ w[nz_of[R]][q]) : 0u;
+                const uint32_t lo = (1u << lane) - 1u;
+                const uint32_t m = ((X >> lane) & 1u) | (((Y >> lane) & 1u) << 1) |
+                                   (((Z >> lane) & 1u) << 2);
+                if (R == 0) m0[q] = m;
+                // (a word without crossings owns no vertex: no triangle reads its entries)
+                if ((X | Y | Z) != 0u) {
+                    s_m[wid][R][lane + 32 * q] = (uint8_t)m;
+                    s_pre[wid][R][lane + 32 * q] =
+                        (uint16_t)(cum + __popc(X & lo) + __popc(Y & lo) + __popc(Z & lo));
+                    cum += __popc(X) + __popc(Y) + __popc(Z);
+                }
+            }
+            if (lane == R) {  // the next unit's first point, x = i0 + 128, in this row
+                const int x = i0 + kChunk;
+                uint32_t m = 0;
+                if (x < g.nx) {
+                    const uint32_t b = w[R][4];
+                    if (x + 1 < g.nx) m |= (b ^ (b >> 1)) & 1u;
+                    if (yok) m |= ((b ^ w[ny_of[R]][4]) & 1u) << 1;
+                    if (zok) m |= ((b ^ w[nz_of[R]][4]) & 1u) << 2;
+                }
+                s_m[wid][R][kChunk] = (uint8_t)m;
             }
         }
-        __syncthreads();
-        if (own) {
-            const float x = __fmaf_rn(float(i), g.h, g.ox), y = __fmaf_rn(float(U.j), g.h, g.oy),
-                        z = __fmaf_rn(float(U.k), g.h, g.oz);
-            const int64_t p = gid(g, i, U.j, U.k);
-            const int64_t step[3] = {1, g.nx, (int64_t)g.nx * g.ny};
-            int64_t o = s_base[0] + (int64_t)(cpre & 0xffffu);
-            for (int a = 0; a < 3; a++) {
-                if (!((own >> a) & 1)) continue;
-                const float tt = root_t(v[p], v[p + step[a]], g.iso);
-                const float d = __fmul_rn(tt, g.h);
+        if (lane < 8) s_base[wid][lane] = base;
+        const int64_t tb = __shfl_sync(0xffffffffu, base, 8);
+        __syncwarp();
+        // vertices of this unit's points (row 0)
+        const int64_t vb = s_base[wid][0];
+        float vx1[4];  // the +x neighbours: the next lane's value (lane 31: lane 0's of
+                       // the next word, or the next unit's first point)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const float wrap = __shfl_sync(0xffffffffu, q < 3 ? val[0][q + 1] : val[0][4], 0);
+            const float down = __shfl_down_sync(0xffffffffu, val[0][q], 1);
+            vx1[q] = lane == 31 ? wrap : down;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const uint32_t m = m0[q];
+            if (!m) continue;
+            const int i = i0 + lane + 32 * q;
+            const float x = __fmaf_rn(float(i), g.h, g.ox), y = __fmaf_rn(float(j), g.h, g.oy),
+                        z = __fmaf_rn(float(k), g.h, g.oz);
+            const float v0 = val[0][q];
+            const float nbr[3] = {vx1[q], val[1][q], val[2][q]};
+            int64_t o = vb + s_pre[wid][0][lane + 32 * q];
+#pragma unroll
+            for (int ax = 0; ax < 3; ax++) {
+                if (!((m >> ax) & 1u)) continue;
+                const float d = __fmul_rn(root_t(v0, nbr[ax], g.iso), g.h);
                 if (o < max_verts) {  // the host reports a mesh larger than the buffers
-                    verts[3 * o + 0] = a == 0 ? __fadd_rn(x, d) : x;
-                    verts[3 * o + 1] = a == 1 ? __fadd_rn(y, d) : y;
-                    verts[3 * o + 2] = a == 2 ? __fadd_rn(z, d) : z;
+                    verts[3 * o + 0] = ax == 0 ? __fadd_rn(x, d) : x;
+                    verts[3 * o + 1] = ax == 1 ? __fadd_rn(y, d) : y;
+                    verts[3 * o + 2] = ax == 2 ? __fadd_rn(z, d) : z;
                 }
                 o++;
             }
         }
-        const int64_t o = tbase[u] + tpre;
-        for (int q = 0; q < nt; q++) {
-            for (int s = 0; s < 3; s++) {
-                const int e = __ldg(&tri[cs * 3 * kMaxTri + 3 * q + s]);
-                const int a = e >> 2, u = e & 1, w = (e >> 1) & 1;
-                // the point owning edge e of this cell, as (dx, row r = dy + 2 dz)
-                const int dx = a == 0 ? 0 : u;
-                const int dy = a == 0 ? u : (a == 1 ? 0 : w);
-                const int dz = a == 2 ? 0 : w;
-                const int r = dy + 2 * dz, li = t + dx;
-                const uint32_t below = (1u << a) - 1u;
-                int64_t id;
-                if (li < kChunk)
-                    id = s_base[r] + (int64_t)((s_pre[li] >> (16 * r)) & 0xffffu) +
-                         __popc(s_mask[r][li] & below);
-                else
-                    id = s_next[r] + __popc(s_mask[r][kChunk] & below);
-                if (o + q < max_faces) faces[3 * (o + q) + s] = (int32_t)id;
+        // triangles of this unit's cells, in x order
+        if (j + 1 < g.ny && k + 1 < g.nz) {
+            int64_t fo = tb;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int x = i0 + lane + 32 * q;
+                int cs = 0, nt = 0;
+                if (x + 1 < g.nx) {
+#pragma unroll
+                    for (int R = 0; R < 4; R++)
+                        cs |= (int)((__funnelshift_r(w[R][q], w[R][q + 1], lane) & 3u) << (2 * R));
+                    nt = __ldg(&ntri[cs]);
+                }
+                int incl = nt;  // warp inclusive scan of the triangle counts
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                const int64_t first = fo + (incl - nt);
+                for (int t3 = 0; t3 < nt; t3++) {
+#pragma unroll
+                    for (int sv = 0; sv < 3; sv++) {
+                        const int e = __ldg(&tri[cs * 3 * kMaxTri + 3 * t3 + sv]);
+                        const int ax = e >> 2, eu = e & 1, ew = (e >> 1) & 1;
+                        // the point owning edge e of this cell: (dx, row R = dy + 2 dz)
+                        const int dx = ax == 0 ? 0 : eu;
+                        const int dy = ax == 0 ? eu : (ax == 1 ? 0 : ew);
+                        const int dz = ax == 2 ? 0 : ew;
+                        const int R = dy + 2 * dz, xi = lane + 32 * q + dx;
+                        const uint32_t below = (1u << ax) - 1u;
+                        const int64_t id =
+                            xi < kChunk ? s_base[wid][R] + s_pre[wid][R][xi] +
+                                              __popc(s_m[wid][R][xi] & below)
+                                        : s_base[wid][4 + R] + __popc(s_m[wid][R][kChunk] & below);
+                        if (first + t3 < max_faces) faces[3 * (first + t3) + sv] = (int32_t)id;
+                    }
+                }
+                fo += __shfl_sync(0xffffffffu, incl, 31);
             }
         }
+        __syncwarp();  // the shared rows are rewritten by the warp's next unit
     }
 }
 
@@ -584,13 +673,15 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
     Grid g{nx, ny, nz, nchunks, U, (float)origin[0], (float)origin[1], (float)origin[2],
            (float)spacing, (float)iso};
     // count: a warp per kCountZ units stacked in z, blocks (chunk, j / kCountWarps,
-    // k / kCountZ); emit: a block per kEmitUnits consecutive units
+    // k / kCountZ); emit: a persistent grid whose warps take the listed units
     if (ny > 65535 || nz > 65535)
         return set_error(kErrInvalid, "marching cubes needs ny, nz <= 65535");
     const dim3 grid_c((unsigned)nchunks, (unsigned)((ny + kCountWarps - 1) / kCountWarps),
                       (unsigned)((nz + kCountZ - 1) / kCountZ)),
-        grid_e((unsigned)((U + kEmitUnits - 1) / kEmitUnits));
-    int32_t *vcnt = nullptr, *tcnt = nullptr;
+        grid_e(148u * 5u);  // persistent (5 blocks per SM): warps stride over the
+                            // listed units
+    int32_t *vcnt = nullptr, *tcnt = nullptr, *act = nullptr;
+    uint32_t* nact = nullptr;
     int64_t *vbase = nullptr, *tbase = nullptr;
     McTable* dtable = nullptr;  // the caller's table on the device
     auto cleanup = [&] {
@@ -598,9 +689,13 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
         pool_free(tcnt, s);
         pool_free(vbase, s);
         pool_free(tbase, s);
+        pool_free(act, s);
+        pool_free(nact, s);
         pool_free(dtable, s);
     };
     int rc = pool_alloc((void**)&vcnt, 4 * (U + 1), s);
+    if (!rc) rc = pool_alloc((void**)&act, 4 * U, s);  // units with output, any order
+    if (!rc) rc = pool_alloc((void**)&nact, 4, s);
     if (!rc) rc = pool_alloc((void**)&tcnt, 4 * (U + 1), s);
     if (!rc) rc = pool_alloc((void**)&vbase, 8 * (U + 1), s);
     if (!rc) rc = pool_alloc((void**)&tbase, 8 * (U + 1), s);
@@ -629,10 +724,13 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
     const bool below = ref_table != nullptr;
     cudaMemsetAsync(vcnt + U, 0, 4, s);
     cudaMemsetAsync(tcnt + U, 0, 4, s);
+    cudaMemsetAsync(nact, 0, 4, s);
     if (below)
-        k_mc_count<true><<<grid_c, 32 * kCountWarps, 0, s>>>(values, g, ntri, vcnt, tcnt);
+        k_mc_count<true><<<grid_c, 32 * kCountWarps, 0, s>>>(values, g, ntri, vcnt, tcnt, act,
+                                                              nact);
     else
-        k_mc_count<false><<<grid_c, 32 * kCountWarps, 0, s>>>(values, g, ntri, vcnt, tcnt);
+        k_mc_count<false><<<grid_c, 32 * kCountWarps, 0, s>>>(values, g, ntri, vcnt, tcnt, act,
+                                                               nact);
     rc = cub_scan([&](void* t, size_t& b) {
         return cub::DeviceScan::ExclusiveSum(t, b, vcnt, vbase, U + 1, s);
     }, s);
@@ -647,11 +745,11 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
     const bool emit = verts && faces && max_verts >= 0 && max_faces >= 0;
     if (!rc && emit) {
         if (below)
-            k_mc_emit<true><<<grid_e, kChunk, 0, s>>>(values, g, tri, ntri, vbase, tbase, verts,
-                                                      faces, max_verts, max_faces);
+            k_mc_emit<true><<<grid_e, 32 * kEmitWarps, 0, s>>>(
+                values, g, tri, ntri, vbase, tbase, act, nact, verts, faces, max_verts, max_faces);
         else
-            k_mc_emit<false><<<grid_e, kChunk, 0, s>>>(values, g, tri, ntri, vbase, tbase, verts,
-                                                       faces, max_verts, max_faces);
+            k_mc_emit<false><<<grid_e, 32 * kEmitWarps, 0, s>>>(
+                values, g, tri, ntri, vbase, tbase, act, nact, verts, faces, max_verts, max_faces);
         if (cudaGetLastError() != cudaSuccess) rc = set_error(kErrCuda, "marching cubes launch");
     }
     int64_t nv = 0, nf = 0;

@@ -238,11 +238,16 @@ __device__ __forceinline__ void finish_node(const MomParams<T, DIM, NS>& p, int 
 }
 
 // Arrival at a parent: add 1 with release (this thread's records are visible to
-// whoever arrives later) and acquire (the last arrival sees every sibling's).
-__device__ __forceinline__ uint32_t arrive_acq_rel(uint32_t* counter) {
+// whoever arrives later).  Only the last arrival reads its siblings' records,
+// so only it orders its later loads after the atomic, with an acquire fence
+// (the release sequence of the counter's adds synchronises with it); the
+// others skip the acquire (and the L1 invalidation it implies).
+__device__ __forceinline__ bool arrive_last(uint32_t* counter, uint32_t need) {
     uint32_t old;
-    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(counter) : "memory");
-    return old;
+    asm volatile("atom.release.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(counter) : "memory");
+    if (old + 1u != need) return false;
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
+    return true;
 }
 
 // Each leaf thread climbs while it is the last child to arrive at the parent.
@@ -266,8 +271,7 @@ __global__ void __launch_bounds__(kClimbBlock) k_moments_climb(const MomParams<T
         const uint32_t need = p.nchild[par];
         const int4 c0 = reinterpret_cast<const int4*>(p.children)[2 * (int64_t)par];
         const int4 c1 = reinterpret_cast<const int4*>(p.children)[2 * (int64_t)par + 1];
-        const uint32_t arrived = arrive_acq_rel(&p.counters[par]);
-        if (arrived + 1u != need) return;
+        if (!arrive_last(&p.counters[par], need)) return;
         p.counters[par] = 0u;
         node = par;
         par = par == 0 ? 0 : p.parent[par];  // the next level's, in flight meanwhile
