@@ -534,8 +534,8 @@ struct IQ2 {
 // gets 1/r = 0, so its finite data contributes exactly zero.
 template <typename T, int OP, bool CONT, bool NEAR, bool MASKED>
 __device__ __forceinline__ void pterm(const IQ<T>& q, const IQ2<T>& q2, const T* __restrict__ b,
-                                      uint32_t mask, P2<T>& p0, P2<T>& p1, P2<T>& p2, T& i0,
-                                      T& i1, T& i2) {
+                                      uint32_t mask, P2<T>& p0, P2<T>& p1, P2<T>& p2, P2<T>& h0,
+                                      P2<T>& h1, P2<T>& h2, T& i0, T& i1, T& i2) {
     const bool ra = !MASKED || (mask & 1u), rb = !MASKED || (mask & 2u);  // in the range
     if constexpr (OP == kOpCount) {
         p0 = add2(p0, pk(ra ? T(1) : T(0), rb ? T(1) : T(0)));
@@ -618,11 +618,14 @@ __device__ __forceinline__ void pterm(const IQ<T>& q, const IQ2<T>& q2, const T*
                 g1 = mul2(q2.ex1, mul2(k.c[5], k.c[3]));
                 g2 = mul2(q2.ex2, mul2(k.c[6], k.c[3]));
             }
+            // d_k c into p_k and g_k r into h_k (the 1/2 applied once per tile)
             const P2<T> c = mul2(add2(add2(g0, g1), g2), r3);
-            const P2<T> hr = mul2(half, r);
-            p0 = fma2(dx, c, fma2(g0, hr, p0));
-            p1 = fma2(dy, c, fma2(g1, hr, p1));
-            p2 = fma2(dz, c, fma2(g2, hr, p2));
+            p0 = fma2(dx, c, p0);
+            p1 = fma2(dy, c, p1);
+            p2 = fma2(dz, c, p2);
+            h0 = fma2(g0, r, h0);
+            h1 = fma2(g1, r, h1);
+            h2 = fma2(g2, r, h2);
         }
     }
 }
@@ -634,11 +637,12 @@ template <typename T, int OP, bool CONT, bool NEAR>
 __device__ __forceinline__ void itile(const IQ<T>& q, const IQ2<T>& q2, bool active,
                                       const T* __restrict__ b, int nb, bool sf, bool sl, T* s,
                                       T* cmp, T* in) {
-    P2<T> p0 = pk(T(0), T(0)), p1 = p0, p2 = p0;
+    P2<T> p0 = pk(T(0), T(0)), p1 = p0, p2 = p0, h0 = p0, h1 = p0, h2 = p0;
     T i0 = T(0), i1 = T(0), i2 = T(0);
     int j0 = 0, j1 = nb;
     if (sf) {
-        pterm<T, OP, CONT, NEAR, true>(q, q2, b, (nb == 1 && sl) ? 0u : 2u, p0, p1, p2, i0, i1, i2);
+        pterm<T, OP, CONT, NEAR, true>(q, q2, b, (nb == 1 && sl) ? 0u : 2u, p0, p1, p2, h0, h1, h2,
+                                       i0, i1, i2);
         j0 = 1;
     }
     const bool last_masked = sl && nb - 1 >= j0;
@@ -647,17 +651,22 @@ __device__ __forceinline__ void itile(const IQ<T>& q, const IQ2<T>& q2, bool act
     for (; j + kUnrollB <= j1; j += kUnrollB) {
 #pragma unroll
         for (int u = 0; u < kUnrollB; u++)
-            pterm<T, OP, CONT, NEAR, false>(q, q2, b + (int64_t)(j + u) * kBlk, 3u, p0, p1, p2, i0,
-                                            i1, i2);
+            pterm<T, OP, CONT, NEAR, false>(q, q2, b + (int64_t)(j + u) * kBlk, 3u, p0, p1, p2, h0,
+                                            h1, h2, i0, i1, i2);
     }
     for (; j < j1; j++)
-        pterm<T, OP, CONT, NEAR, false>(q, q2, b + (int64_t)j * kBlk, 3u, p0, p1, p2, i0, i1, i2);
+        pterm<T, OP, CONT, NEAR, false>(q, q2, b + (int64_t)j * kBlk, 3u, p0, p1, p2, h0, h1, h2,
+                                        i0, i1, i2);
     if (last_masked)
-        pterm<T, OP, CONT, NEAR, true>(q, q2, b + (int64_t)(nb - 1) * kBlk, 1u, p0, p1, p2, i0, i1,
-                                       i2);
+        pterm<T, OP, CONT, NEAR, true>(q, q2, b + (int64_t)(nb - 1) * kBlk, 1u, p0, p1, p2, h0, h1,
+                                       h2, i0, i1, i2);
     if (!active) return;
     if constexpr (OP == kOpCount) {
         s[0] += p0.x + p0.y;
+    } else if constexpr (IOp<OP>::a2tsum) {
+        kahan(s[0], cmp[0], (p0.x + p0.y) + T(0.5) * (h0.x + h0.y));
+        kahan(s[1], cmp[1], (p1.x + p1.y) + T(0.5) * (h1.x + h1.y));
+        kahan(s[2], cmp[2], (p2.x + p2.y) + T(0.5) * (h2.x + h2.y));
     } else {
         kahan(s[0], cmp[0], p0.x + p0.y);
         kahan(s[1], cmp[1], p1.x + p1.y);
