@@ -47,14 +47,23 @@ FLOPS_A2T = 22           # d (3) + |d|^2 (5) + r^-3 (2) + e s r^-3 (2) + 3 FMA (
 # as in the counts above.  (Per-direction terms of the reference mode: 22 each.)
 FLOPS_IA2T_SUM = 29
 L2_FLUSH_BYTES = 256 << 20
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the two
-# traversals on this workload, taken from one ncu capture of these kernels with
-# the command below; ncu does not run inside the bench, so these are constants
-# of that capture, reported as such (roofline.traffic_source)
-TRAFFIC_BYTES = {"A2T_SUM": 165_164_800 + 7_062_784, "A2_FUSED": 136_392_704 + 5_499_904}
-TRAFFIC_SOURCE = ("ncu --set full --clock-control none -k regex:k_traverse -c 2 python bench.py "
-                  "--steps 1 --warmup 1 --no-cpu-baseline --no-fp64 --no-solve (one capture, "
-                  "not measured in this run)")
+# Counters of the two traversals on this workload from one ncu capture of the
+# warm-up step's launches (ncu does not run inside the bench; these are
+# constants of that capture, reported with the command that made it): DRAM
+# bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum), MUFU (XU
+# pipe) and issue-slot utilisation, FMA-pipe activity.
+TRAFFIC_BYTES = {"A2T_SUM": 163_672_832 + 7_347_968, "A2_FUSED": 136_197_888 + 4_479_488}
+KERNEL_COUNTERS = {
+    "A2T_SUM": {"mufu_frac": 0.1493, "issue_active": 0.8898, "fma_pipe_active": 0.3858},
+    "A2_FUSED": {"mufu_frac": 0.0962, "issue_active": 0.7988, "fma_pipe_active": 0.3437},
+}
+TRAFFIC_SOURCE = ("ncu --metrics smsp__issue_active.avg.pct_of_peak_sustained_active,"
+                  "sm__inst_executed_pipe_xu.avg.pct_of_peak_sustained_active,"
+                  "sm__pipe_fma_cycles_active.avg.pct_of_peak_sustained_active,"
+                  "dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum "
+                  "--clock-control none -k regex:k_traverse -s 5 -c 2 python bench.py --steps 1 "
+                  "--warmup 1 --no-fp64 --no-cpu-baseline --no-interp (one capture, not measured "
+                  "in this run)")
 
 
 def parse():
@@ -287,6 +296,8 @@ def interp_leg(args, P, W, MU, WV, p, widths, mu, dev, stream, flush, rank):
         step([ev() for _ in range(5)])
     torch.cuda.synchronize(dev)
     st, a2, a2t = [], [], []
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
     for _ in range(max(3, min(args.steps, 10))):
         flush.fill_(1.0)
         m = [ev() for _ in range(5)]
@@ -295,7 +306,8 @@ def interp_leg(args, P, W, MU, WV, p, widths, mu, dev, stream, flush, rank):
         st.append(m[0].elapsed_time(m[4]))
         a2.append(m[1].elapsed_time(m[2]))
         a2t.append(m[3].elapsed_time(m[4]))
-    leg = {"degree": args.interp_degree, "theta": 0.5,
+    leg_clocks = clocks.stop()
+    leg = {"degree": args.interp_degree, "theta": 0.5, "clocks": leg_clocks,
            "proxy_grids": wn.far_field_info()["proxy_grids"],
            "step_ms": round(float(np.mean(st)), 3),
            "A2_FUSED_walk_ms": round(float(np.mean(a2)), 3),
@@ -600,6 +612,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                      "frac": round(achieved / peak_tflops, 4), "traffic": traffic,
                      "traffic_unit": "bytes per launch",
                      "traffic_source": TRAFFIC_SOURCE if traffic is not None else None,
+                     "counters": (dict(KERNEL_COUNTERS[key], source=TRAFFIC_SOURCE)
+                                  if traffic is not None else None),
                      "peak_source": "measured FP32 FMA probe (cagr_probe_fp32_peak)",
                      "pair_terms_per_launch": round(terms_dom), "flops_per_term": fpt},
         "kernels_ms": {"moments_per_step": round(float(np.mean(mom_ms)), 4),

@@ -17,6 +17,7 @@ HEADER = os.path.join(ROOT, "include", "cagr.h")
 
 # status codes (include/cagr.h)
 CAGR_OK = 0
+CAGR_ERR_ALLOC = 3    # device allocation failed (include/cagr.h)
 # dtypes
 CAGR_F32, CAGR_F64 = 0, 1
 # operators
@@ -86,7 +87,11 @@ _lib = None
 
 
 class CagrError(RuntimeError):
-    """A cagr_* call returned a non-zero status."""
+    """A cagr_* call returned a non-zero status (`code`: the CAGR_ERR_* value)."""
+
+    def __init__(self, message: str, code: int = 0):
+        super().__init__(message)
+        self.code = code
 
 
 def header_symbols() -> list[str]:
@@ -118,4 +123,4 @@ def check(rc: int, what: str = "") -> None:
         L = lib()
         msg = L.cagr_last_error().decode(errors="replace")
         kind = L.cagr_status_string(rc).decode()
-        raise CagrError(f"{what}: {kind} ({rc}): {msg}")
+        raise CagrError(f"{what}: {kind} ({rc}): {msg}", rc)

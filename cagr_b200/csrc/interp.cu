@@ -76,13 +76,16 @@ constexpr unsigned kAll = 0xffffffffu;
 #define CAGR_IW_WARPS 4
 #endif
 #ifndef CAGR_IW_UNROLL
-#define CAGR_IW_UNROLL 4
+#define CAGR_IW_UNROLL 8
 #endif
 constexpr int kSlots = CAGR_IW_SLOTS;       // tiles in flight per warp
 constexpr int kTileBytes = CAGR_IW_TILE;    // per tile (4096: 51 float / 25 double record pairs)
 // (measured at 1M points, A2_FUSED walk, record pairs with packed arithmetic:
 // 3 slots x 3072 B 25.8 ms, 4 x 3072 26.9, 3 x 4096 26.5, 2 x 4096 23.5,
-// 2 x 6144 23.8, 2 x 8192 26.2; 2-warp blocks the same as 4)
+// 2 x 6144 23.8, 2 x 8192 26.2; 2-warp blocks the same as 4; later, with the
+// A2T-sum records in their walk form: unroll 8 / 4 / 2 terms 23.1 / 23.5 /
+// 24.8 ms (A2_FUSED) and 22.3 / 22.7 / 23.1 ms (A2T sum), 8-warp blocks 23.8 /
+// 24.6, 3 slots 26.6 / 23.4)
 constexpr int kPWarps = CAGR_IW_WARPS;      // warps per block
 constexpr int kUnroll = CAGR_IW_UNROLL;     // pair terms per inner-loop iteration
 constexpr int kUnrollB = kUnroll > 1 ? kUnroll / 2 : 1;  // blocks (two terms each) per iteration

@@ -25,6 +25,7 @@ import time
 import numpy as np
 import torch
 
+from ._lib import CAGR_ERR_ALLOC, CagrError
 from .wn_treecode import WindingNumberTreecode
 
 # b's window table (cagr_b_window_table) takes at most this many widths
@@ -138,7 +139,15 @@ def cagr_solve(points: torch.Tensor, wsmin: float, wsmax: float, iters: int = 40
         b_hi = wn.forward_A2T_shared(b, w_hi)
         wn.scatter(b, slot=1)   # b is constant: its moments serve every step
         if use_table:
-            b_table = wn.b_window_table(base, sc_t)
+            # an [S, N, 3] table: where the device has no room for it, each step
+            # adds b's window itself (the four-slot walk, no table)
+            try:
+                b_table = wn.b_window_table(base, sc_t)
+            except (torch.cuda.OutOfMemoryError, CagrError) as e:
+                if isinstance(e, CagrError) and e.code != CAGR_ERR_ALLOC:
+                    raise
+                use_table, b_table = False, None
+        if use_table:
             rk1 = b_hi + b_table[sd_scales.index(s_mid)]   # overwritten at i == n_sd
         else:
             rk1 = wn.forward_A2T_shared(b, base * sc_t[sd_scales.index(s_mid)])

@@ -256,7 +256,9 @@ int cagr_mc_table(int8_t* tri, uint8_t* ntri);
  * 2,097,152 nodes (8 MiB, held by every GPU that loads the library until
  * exit); larger trees return CAGR_ERR_INVALID.  All calls share that array:
  * calls that overlap on the GPU race, so order them on one stream.  The first
- * call on a device looks the array up; make it before any stream capture. */
+ * call on a device looks the array up; make it before any stream capture.
+ * Every buffer and the stream must belong to the CURRENT device (the scratch
+ * array is the current device's; a buffer of another device is not detected). */
 int cagr_scatter_noalloc(const int64_t* parent_dev, const int64_t* children_dev,
                          const uint8_t* is_leaf_dev, const int64_t* npts_dev,
                          const int64_t* n2p_dev, const int64_t* n2p_start_dev, int64_t num_nodes,

@@ -86,3 +86,32 @@ def test_width_table_and_its_fallback_give_the_same_solve(cuda_lib, monkeypatch)
     assert a.operator_calls == b.operator_calls
     assert _agree(mu_a, mu_b) >= 0.999
     assert np.linalg.norm(mu_a - mu_b) <= 1e-3 * np.linalg.norm(mu_a)
+
+
+def test_window_table_alloc_failure_falls_back(cuda_lib, monkeypatch):
+    """When the device has no room for b's window table (its allocation fails
+    with CAGR_ERR_ALLOC), the solve uses the table-free per-step walk and
+    gives the same result as the fallback chosen up front."""
+    from cagr_b200 import _lib, solver
+    from cagr_b200.wn_treecode import WindingNumberTreecode
+    _, pts = _bunny()
+    real = WindingNumberTreecode.b_window_table
+
+    def no_room(self, base, scales):
+        raise _lib.CagrError("cagr_b_window_table: device allocation failed", _lib.CAGR_ERR_ALLOC)
+
+    monkeypatch.setattr(WindingNumberTreecode, "b_window_table", no_room)
+    a = solver.cagr_solve(pts, 0.01, 0.04, iters=8, n_sd=5, wnnc_steps=0)
+    monkeypatch.setattr(WindingNumberTreecode, "b_window_table", real)
+    monkeypatch.setattr(solver, "MAX_TABLE_WIDTHS", 0)
+    b = solver.cagr_solve(pts, 0.01, 0.04, iters=8, n_sd=5, wnnc_steps=0)
+    assert a.operator_calls == b.operator_calls
+    assert np.array_equal(a.normals.cpu().numpy(), b.normals.cpu().numpy())
+
+    def broken(self, base, scales):
+        raise _lib.CagrError("cagr_b_window_table: invalid", 1)
+
+    monkeypatch.setattr(WindingNumberTreecode, "b_window_table", broken)
+    monkeypatch.setattr(solver, "MAX_TABLE_WIDTHS", 64)
+    with pytest.raises(_lib.CagrError):
+        solver.cagr_solve(pts, 0.01, 0.04, iters=8, n_sd=5, wnnc_steps=0)

@@ -67,6 +67,27 @@ def test_noalloc_matches_allocating_path_twice(cuda_lib):
             assert torch.equal(g, e), (dtype.__name__, name)
 
 
+def test_noalloc_with_caller_weights(cuda_lib):
+    """The caller-supplied point weights (some zero) give the allocating path's
+    moments with the same weights, bit for bit."""
+    import torch
+    from cagr_b200 import WindingNumberTreecode
+    for dtype, dim, seed in [(np.float32, 3, 33), (np.float64, 1, 34)]:
+        pts = _cloud(15000, seed, dtype)
+        rng = np.random.default_rng(seed)
+        wn = WindingNumberTreecode(torch.from_numpy(pts).cuda())
+        vals = torch.from_numpy(rng.normal(size=(len(pts), dim)).astype(dtype)).cuda()
+        wts = np.abs(rng.normal(size=len(pts))).astype(dtype)
+        wts[::7] = 0                                      # zero weights: centroid fallback
+        wts = torch.from_numpy(wts).cuda()
+        got = _noalloc(wn, vals, wts)
+        wn.scatter(vals, weights=wts)
+        ref = wn.scatter_export(0, dim)
+        torch.cuda.synchronize()
+        for g, e, name in zip(got, ref, ("node_attrs", "reppoints", "node_weights")):
+            assert torch.equal(g, e), (dtype.__name__, name)
+
+
 def test_noalloc_rejects_trees_beyond_its_capacity(cuda_lib):
     from cagr_b200 import _lib
     L = _lib.lib()
