@@ -294,40 +294,54 @@ __device__ __forceinline__ void lagrange(T u, int P, const T* t, const T* om, T*
     for (int k = 0; k < P; k++) L[k] *= inv;
 }
 
-constexpr int kTile = 64;
 constexpr int kChargeThreads = 256;
-constexpr int kMaxPer = (kPMax * kPMax * kPMax + kChargeThreads - 1) / kChargeThreads;
+// points staged per tile (shared memory: Lagrange values and charges; 64 in
+// double keeps the block under the 48 KB of static shared memory)
+template <typename T>
+constexpr int charge_tile() { return sizeof(T) == 4 ? 128 : 64; }
 
-// Partial proxy charges of one chunk: thread m accumulates
-// sum_j Lx_a(y_j) Ly_b(y_j) Lz_c(y_j) charges_j for its proxies m = (a, b, c).
+// Partial proxy charges of one chunk, q_abc = sum_j Lx_a(y_j) Ly_b(y_j) Lz_c(y_j)
+// charges_j, as a tensor-product contraction: thread (a, b) of a slice forms
+// Lx_a Ly_b charges_j once per point and adds it times every Lz_c (read from
+// shared memory by all threads alike), so a point costs a thread 2 + P shared
+// loads for P proxies; the kChargeThreads / P^2 slices take the tile's points
+// round robin and are summed in slice order at the end (deterministic).
 template <typename T>
 __global__ void __launch_bounds__(kChargeThreads) k_charges(const ChargeParams<T> p) {
+    constexpr int kTile = charge_tile<T>();
     __shared__ T sL[kTile][3][kPMax];
     __shared__ T sQ[kTile][4];
+    __shared__ T sRed[kPMax * kPMax * kPMax][3];
+    __shared__ T sCheb[kPMax], sOmega[kPMax];  // (indexed per k: not from the parameters)
+    if (threadIdx.x < kPMax) {
+        sCheb[threadIdx.x] = p.cheb[threadIdx.x];
+        sOmega[threadIdx.x] = p.omega[threadIdx.x];
+    }
+    __syncthreads();
     const int4 cd = p.chunks[blockIdx.x];  // {node, first sorted point, count, proxy block}
     const T* c = p.bc + 4 * (int64_t)cd.x;
     const T* h = p.bh + 4 * (int64_t)cd.x;
     const T cen[3] = {c[0], c[1], c[2]};
     const T ih[3] = {T(1) / h[0], T(1) / h[1], T(1) / h[2]};
-    const int P = p.P, P3 = p.P3;
-    T acc[kMaxPer][3];
-    int ma[kMaxPer], mb[kMaxPer], mc[kMaxPer];
+    const int P = p.P, P2 = P * P, P3 = p.P3;
+    const int slices = kChargeThreads / P2;  // >= 3 (P <= 9)
+    const int slice = (int)threadIdx.x / P2, pair = (int)threadIdx.x - slice * P2;
+    const bool on = slice < slices;
+    const int a = pair / P, b = pair - (pair / P) * P;
+    T acc[kPMax][3];
 #pragma unroll
-    for (int k = 0; k < kMaxPer; k++) {
-        const int m = threadIdx.x + k * kChargeThreads;
-        ma[k] = m / (P * P);
-        mb[k] = (m / P) % P;
-        mc[k] = m % P;
-        acc[k][0] = acc[k][1] = acc[k][2] = T(0);
-    }
+    for (int k = 0; k < kPMax; k++) acc[k][0] = acc[k][1] = acc[k][2] = T(0);
     for (int base = 0; base < cd.z; base += kTile) {
         const int cnt = min(kTile, cd.z - base);
         for (int t = threadIdx.x; t < cnt * 3; t += kChargeThreads) {
-            const int j = t / 3, a = t - 3 * j;
-            const T y = rec_comp(p.pts, (int64_t)cd.y + base + j, a);
-            T u = (y - cen[a]) * ih[a];
+            const int j = t / 3, ax = t - 3 * j;
+            const T y = rec_comp(p.pts, (int64_t)cd.y + base + j, ax);
+            // (selects, not a dynamic index into a register array)
+            const T cx = ax == 0 ? cen[0] : (ax == 1 ? cen[1] : cen[2]);
+            const T hx = ax == 0 ? ih[0] : (ax == 1 ? ih[1] : ih[2]);
+            T u = (y - cx) * hx;
             u = fmin(fmax(u, T(-1)), T(1));
-            lagrange(u, P, p.cheb, p.omega, &sL[j][a][0]);
+            lagrange(u, P, sCheb, sOmega, &sL[j][ax][0]);
         }
         for (int j = threadIdx.x; j < cnt; j += kChargeThreads) {
             const int64_t r = (int64_t)cd.y + base + j;
@@ -336,32 +350,50 @@ __global__ void __launch_bounds__(kChargeThreads) k_charges(const ChargeParams<T
             sQ[j][2] = rec_comp(p.pts, r, 8);
         }
         __syncthreads();
-        for (int j = 0; j < cnt; j++) {
-            const T q0 = sQ[j][0], q1 = sQ[j][1], q2 = sQ[j][2];
+        if (on) {
+            for (int j = slice; j < cnt; j += slices) {
+                const T lab = sL[j][0][a] * sL[j][1][b];
+                const T t0 = lab * sQ[j][0], t1 = lab * sQ[j][1], t2 = lab * sQ[j][2];
 #pragma unroll
-            for (int k = 0; k < kMaxPer; k++) {
-                if (threadIdx.x + k * kChargeThreads < P3) {
-                    const T w = sL[j][0][ma[k]] * sL[j][1][mb[k]] * sL[j][2][mc[k]];
-                    acc[k][0] += w * q0;
-                    acc[k][1] += w * q1;
-                    acc[k][2] += w * q2;
+                for (int k = 0; k < kPMax; k++) {
+                    if (k < P) {
+                        const T lz = sL[j][2][k];
+                        acc[k][0] += t0 * lz;
+                        acc[k][1] += t1 * lz;
+                        acc[k][2] += t2 * lz;
+                    }
                 }
             }
         }
         __syncthreads();
     }
+    // the slices' sums, added in slice order
+    for (int sl = 0; sl < slices; sl++) {
+        if (slice == sl) {
 #pragma unroll
-    for (int k = 0; k < kMaxPer; k++) {
-        const int m = threadIdx.x + k * kChargeThreads;
-        if (m < P3) {
-            T* o = p.part + ((int64_t)blockIdx.x * P3 + m) * 4;
-            st4<T>(o, make4(acc[k][0], acc[k][1], acc[k][2], T(0)));
+            for (int k = 0; k < kPMax; k++) {
+                if (k < P) {
+                    T* r = sRed[pair * P + k];
+                    r[0] = sl == 0 ? acc[k][0] : r[0] + acc[k][0];
+                    r[1] = sl == 0 ? acc[k][1] : r[1] + acc[k][1];
+                    r[2] = sl == 0 ? acc[k][2] : r[2] + acc[k][2];
+                }
+            }
         }
+        __syncthreads();
+    }
+    for (int m = threadIdx.x; m < P3; m += kChargeThreads) {
+        T* o = p.part + ((int64_t)blockIdx.x * P3 + m) * 4;
+        st4<T>(o, make4(sRed[m][0], sRed[m][1], sRed[m][2], T(0)));
     }
 }
 
 // Proxy records: charges = the node's chunk partials summed in chunk order
-// (in double), position = the Chebyshev grid point of the node's box.
+// (in double; the loads of 8 chunks are issued together, a node near the root
+// having hundreds of chunks), position = the Chebyshev grid point of the
+// node's box.
+constexpr int kFinishBatch = 8;
+
 template <typename T>
 __global__ void k_charges_finish(const int32_t* __restrict__ chunk_first, int64_t num_interp,
                                  const int4* __restrict__ chunks, const T* __restrict__ part,
@@ -379,11 +411,19 @@ __global__ void k_charges_finish(const int32_t* __restrict__ chunk_first, int64_
     }
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
     const int c0 = chunk_first[ii], c1 = chunk_first[ii + 1];
-    for (int ch = c0; ch < c1; ch++) {
-        const T* q = part + ((int64_t)ch * P3 + m) * 4;
-        s0 += (double)q[0];
-        s1 += (double)q[1];
-        s2 += (double)q[2];
+    for (int ch = c0; ch < c1; ch += kFinishBatch) {
+        Vec4<T> q[kFinishBatch];
+#pragma unroll
+        for (int u = 0; u < kFinishBatch; u++)
+            if (ch + u < c1) q[u] = ld4(part + ((int64_t)(ch + u) * P3 + m) * 4);
+#pragma unroll
+        for (int u = 0; u < kFinishBatch; u++) {
+            if (ch + u < c1) {
+                s0 += (double)q[u].x;
+                s1 += (double)q[u].y;
+                s2 += (double)q[u].z;
+            }
+        }
     }
     const int64_t node = chunks[c0].x;
     const T* c = bc + 4 * node;
