@@ -341,6 +341,41 @@ def interp_leg(args, P, W, MU, WV, p, widths, mu, dev, stream, flush, rank):
     return leg
 
 
+def reference_reconstruction(points: np.ndarray, normals: np.ndarray, verts: np.ndarray,
+                             faces: np.ndarray) -> dict:
+    """The reference's CPU reconstructor (build_GR_cpu.sh's sources, built by
+    `make -C oracle ref-gaussrecon`: its adaptive octree, host treecode with the
+    plain Gauss operator, octree marching cubes) on the oriented cloud of this
+    run's solve, timed as a whole program on the host cores (it sets 20 OpenMP
+    threads itself), and the distance between its mesh and this run's 512^3
+    reconstruction of the same oriented cloud.  A CPU-baseline leg: the reference
+    build is test infrastructure under oracle/."""
+    exe = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle", "_ref",
+                       "main_GaussRecon_cpu")
+    if not os.path.exists(exe):
+        return {"unavailable": "the reference reconstructor is not built "
+                               "(make -C oracle ref-gaussrecon needs the reference checkout)"}
+    from oracle.mesh_distance import hausdorff, read_ply
+    with tempfile.TemporaryDirectory() as d:
+        xyz, ply = os.path.join(d, "oriented.xyz"), os.path.join(d, "ref.ply")
+        np.hstack([points, normals]).astype(np.float32).tofile(xyz, sep=" ", format="%.7g")
+        t0 = time.perf_counter()
+        r = subprocess.run([exe, "-i", xyz, "-o", ply], cwd=d, capture_output=True, text=True,
+                           timeout=1200)
+        seconds = time.perf_counter() - t0
+        if r.returncode != 0 or not os.path.exists(ply):
+            return {"unavailable": f"the reference reconstructor failed (exit {r.returncode})"}
+        rv, rf = read_ply(ply)
+    diag = float(np.linalg.norm(rv.max(0) - rv.min(0)))
+    H, mean = hausdorff((verts.astype(np.float64), faces), (rv, rf), n=100_000)
+    return {"value": round(seconds, 3), "unit": "s", "cores": os.cpu_count(), "threads": 20,
+            "kind": "reference", "program": "main_GaussRecon_cpu (build_GR_cpu.sh sources)",
+            "input": f"this run's {len(points):,} points with their solved normals",
+            "mesh_vertices": int(rv.shape[0]), "mesh_faces": int(rf.shape[0]),
+            "hausdorff_over_diagonal_vs_ours": round(H / diag, 5),
+            "mean_distance_over_diagonal_vs_ours": round(mean / diag, 6)}
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import ctypes
 
@@ -503,7 +538,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     # end to end: the whole CAGR normal solve on this cloud (tree build + 40
     # iterations + 8 G steps, main_CAGR.py's schedule, preset l0)
-    solve = solve64 = None
+    solve = solve64 = our_mesh = None
     if not args.no_solve:
         from cagr_b200.mesh import reconstruct
         from cagr_b200.solver import PRESET_WIDTHS, cagr_solve
@@ -536,6 +571,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         del rec
         res, rec, t_solve, t_rec = pipeline(P)
         solve = record(res, rec, t_solve, t_rec, c_solve + c_rec)
+        our_mesh = (rec.vertices.cpu().numpy(), rec.faces.cpu().numpy(),
+                    res.normals.float().cpu().numpy())
         del rec
         if not args.no_fp64:
             # the same pipeline in float64 throughout (points, widths, moments, pair
@@ -588,7 +625,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         terms_dom, fpt = terms_a2, FLOPS_A2_FUSED
     traffic = TRAFFIC_BYTES[key] if args.n == 1_000_000 and args.workload == "union8" else None
     achieved = terms_dom * fpt / (dur * 1e-3) / 1e12
-    cpu = None
+    cpu = recon_ref = None
+    if not args.no_cpu_baseline and our_mesh is not None:
+        recon_ref = reference_reconstruction(p, our_mesh[2], our_mesh[0], our_mesh[1])
     if not args.no_cpu_baseline:
         import multiprocessing
         threads = multiprocessing.cpu_count()
@@ -631,6 +670,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if recon_ref is not None:
+        line["cpu_baseline_reconstruction"] = recon_ref
     print(json.dumps(line), flush=True)
 
 

@@ -50,7 +50,9 @@ struct Tree {
     int32_t* children = nullptr;   // [M*8], -1 = none
     int32_t* leaf_ids = nullptr;   // [num_leaves]
     int64_t* n2p_start = nullptr;  // [M]
-    int32_t* n2p = nullptr;        // [n2p_len] original indices
+    int32_t* n2p = nullptr;        // [n2p_len] original indices (built by the first export)
+    int32_t* lorder = nullptr;     // [N] leaves' points in original-index order, by sorted
+                                   // position (null: perm is that order, leaf size 1)
     void* spos = nullptr;          // [N*3] T, positions in sorted order
     int32_t* qgroup = nullptr;     // [N] self-query qi is the point at sorted position qgroup[qi]
                                    // (3-D Hilbert order: the traversals' warp grouping)
@@ -75,9 +77,8 @@ struct Tree {
 int tree_build(const void* points, int64_t n, int dtype, int max_depth, int leaf_size,
                cudaStream_t stream, Tree** out);
 void tree_free(Tree* t);
-int tree_export(const Tree* t, int64_t* parent, int64_t* children, uint8_t* is_leaf,
-                void* half_w, int64_t* npts, int64_t* n2p, int64_t* n2p_start,
-                cudaStream_t stream);
+int tree_export(Tree* t, int64_t* parent, int64_t* children, uint8_t* is_leaf, void* half_w,
+                int64_t* npts, int64_t* n2p, int64_t* n2p_start, cudaStream_t stream);
 
 // Bottom-up node moments into record slot `slot`.  attrs: [N, dim] in the
 // tree dtype (original point order); weights: [N] or null (then |attr|).

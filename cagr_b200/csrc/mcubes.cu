@@ -299,8 +299,7 @@ __device__ __forceinline__ float root_t(float v0, float v1, float iso) {
 // fmax ignore; a NaN value of the field, which is outside, loads as -inf, or
 // +inf when inside means below the iso-value); two warp votes on the 4 rows'
 // extremes then settle such a unit with no bit work.  The others are counted
-// from ballots:
-// inside-bit words w[q] held by every lane, where a funnel shift of
+// from ballots: inside-bit words w[q] held by every lane, where a funnel shift of
 // (w[q+1] : w[q]) by l gives the inside bits of x and x + 1, so a point's
 // crossings and cell case are a few bit operations.
 constexpr int kCountWarps = 4;
@@ -334,8 +333,7 @@ __device__ __forceinline__ void load_row(const float* __restrict__ v, const Grid
     r.v[4] = (ok && lane == 0 && x < g.nx) ? sided<BELOW>(row[x]) : NAN;
 }
 
-template <bool BELOW>
-__device__ __forceinline__ void row_flags(const Grid&, bool, int, int, RowVals& r) {
+__device__ __forceinline__ void row_flags(RowVals& r) {
     r.lo = fminf(fminf(fminf(r.v[0], r.v[1]), fminf(r.v[2], r.v[3])), r.v[4]);
     r.hi = fmaxf(fmaxf(fmaxf(r.v[0], r.v[1]), fmaxf(r.v[2], r.v[3])), r.v[4]);
 }
@@ -372,8 +370,8 @@ __global__ void __launch_bounds__(32 * kCountWarps) k_mc_count(const float* __re
     load_row<BELOW>(v, g, j + 1, k0, has_y, i0, lane, rb[0]);
     load_row<BELOW>(v, g, j, k0 + 1, k0 + 1 < g.nz, i0, lane, ra[1]);
     load_row<BELOW>(v, g, j + 1, k0 + 1, has_y && k0 + 1 < g.nz, i0, lane, rb[1]);
-    row_flags<BELOW>(g, true, i0, lane, ra[0]);
-    row_flags<BELOW>(g, has_y, i0, lane, rb[0]);
+    row_flags(ra[0]);
+    row_flags(rb[0]);
 #pragma unroll
     for (int kk = 0; kk < kCountZ; kk++) {
         const int k = k0 + kk;
@@ -384,8 +382,8 @@ __global__ void __launch_bounds__(32 * kCountWarps) k_mc_count(const float* __re
             load_row<BELOW>(v, g, j, k + 2, k + 2 < g.nz, i0, lane, ra[s2]);
             load_row<BELOW>(v, g, j + 1, k + 2, has_y && k + 2 < g.nz, i0, lane, rb[s2]);
         }
-        row_flags<BELOW>(g, has_z, i0, lane, ra[s1]);
-        row_flags<BELOW>(g, has_y && has_z, i0, lane, rb[s1]);
+        row_flags(ra[s1]);
+        row_flags(rb[s1]);
         // (every lane: NaN extremes, no point, compare false and vote neither way)
         const float lo = fminf(fminf(ra[s0].lo, rb[s0].lo), fminf(ra[s1].lo, rb[s1].lo));
         const float hi = fmaxf(fmaxf(ra[s0].hi, rb[s0].hi), fmaxf(ra[s1].hi, rb[s1].hi));

@@ -70,8 +70,7 @@ struct MomParams {
     const int32_t* children = nullptr;
     const int32_t* perm = nullptr;
     const int32_t* invperm = nullptr;
-    const int32_t* n2p = nullptr;
-    const int64_t* n2p_start = nullptr;
+    const int32_t* lorder = nullptr;  // leaves' points in original-index order (null: perm)
     const T* spos = nullptr;
     const T* attrs = nullptr;    // row stride astride; slot k reads columns [k*DIM, k*DIM+DIM)
     int astride = DIM;
@@ -126,10 +125,10 @@ __device__ __forceinline__ void leaf_pass(const MomParams<T, DIM, NS>& p, int no
         }
     }
     S.clear();
-    const int64_t base = p.n2p_start[node];
     for (int j = 0; j < np; j++) {
-        const int pt = (np == 1) ? p.perm[pstart] : p.n2p[base + j];
-        const int s = (np == 1) ? pstart : p.invperm[pt];
+        // the leaf's points in ascending original index (node2point order)
+        const int pt = p.lorder ? p.lorder[pstart + j] : p.perm[pstart + j];
+        const int s = p.lorder ? p.invperm[pt] : pstart + j;
         const T y[3] = {p.spos[3 * s], p.spos[3 * s + 1], p.spos[3 * s + 2]};
 #pragma unroll
         for (int k = 0; k < NS; k++) {
@@ -324,8 +323,7 @@ int run(Tree* t, MomParams<T, DIM, NS> p, cudaStream_t s) {
     p.children = t->children;
     p.perm = t->perm;
     p.invperm = t->invperm;
-    p.n2p = t->n2p;
-    p.n2p_start = t->n2p_start;
+    p.lorder = t->lorder;
     p.spos = (const T*)t->spos;
     p.counters = t->counters;
     const unsigned grid = (unsigned)((t->num_leaves + kClimbBlock - 1) / kClimbBlock);

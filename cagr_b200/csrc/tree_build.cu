@@ -22,8 +22,10 @@
 //  4. Preorder id of node (d, i) = (nodes at positions < i) + (d - d0): sorting
 //     nodes by (first point, depth) is preorder.  Subtree ends and parents come
 //     from a sparse-table search over lcp.
-//  5. Per-node point lists: (node, index) pairs emitted in index order by a
-//     root-to-leaf walk, then a stable radix sort by node id.
+//  5. Per-node point lists (needed only by the reference-layout export, so
+//     built on its first call): (node, index) pairs, a point's leaf and its
+//     ancestors, emitted in index order, then a stable radix sort by node id.
+//     The moments only need each leaf's own points in index order.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -313,30 +315,66 @@ __global__ void k_spos(const T* __restrict__ pts, const int32_t* __restrict__ pe
     spos[3 * s + 2] = pts[3 * p + 2];
 }
 
-// root-to-leaf walk for original point p: counts (WRITE=false) or emits pairs
+// ---- the per-node point lists (node2point_index), built on first export ----
+// Every point belongs to its leaf and the leaf's ancestors: per point (original
+// index p) its leaf's depth + 1 pairs (node, p), root first; a stable sort of
+// all pairs by node id then lists each node's points in ascending p.
+
+// leaf node of every sorted position
+__global__ void k_leaf_of_pos(const int32_t* __restrict__ leaf_ids, int64_t num_leaves,
+                              const int4* __restrict__ meta, int32_t* __restrict__ leaf_of) {
+    const int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= num_leaves) return;
+    const int leaf = leaf_ids[li];
+    const int4 m = meta[leaf];
+    for (int j = 0; j < node_npts(m); j++) leaf_of[(int64_t)m.y + j] = leaf;
+}
+
 template <bool WRITE>
-__global__ void k_walk(const int32_t* __restrict__ invperm, const uint64_t* __restrict__ sk,
-                       const int4* __restrict__ meta, const int32_t* __restrict__ children, int D,
-                       int64_t n, int32_t* __restrict__ cnt, const int64_t* __restrict__ off,
-                       int32_t* __restrict__ pair_node, int32_t* __restrict__ pair_pt) {
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_pairs(const int32_t* __restrict__ invperm, const int32_t* __restrict__ leaf_of,
+                        const int4* __restrict__ meta, const int32_t* __restrict__ parent,
+                        int64_t n, int32_t* __restrict__ cnt, const int64_t* __restrict__ off,
+                        int32_t* __restrict__ pair_node, int32_t* __restrict__ pair_pt) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
-    const uint64_t code = sk[invperm[p]];
-    int node = 0;
-    int64_t k = WRITE ? off[p] : 0;
-    int c = 0;
-    while (true) {
-        if (WRITE) {
-            pair_node[k + c] = node;
-            pair_pt[k + c] = (int32_t)p;
-        }
-        c++;
-        const int4 m = meta[node];
-        if (node_leaf(m) || c > CAGR_MAX_DEPTH + 1) break;
-        node = children[node * 8 + digit_at(code, D, node_depth(m))];
-        if (node < 0) break;  // unreachable for a consistent tree; never index with -1
+    int node = leaf_of[invperm[p]];
+    const int d = node_depth(meta[node]);
+    if (!WRITE) {
+        cnt[p] = d + 1;
+        return;
     }
-    if (!WRITE) cnt[p] = c;
+    const int64_t k = off[p];
+    for (int i = d; i >= 0 && node >= 0; i--) {  // the leaf at k + d, the root at k
+        pair_node[k + i] = node;
+        pair_pt[k + i] = (int32_t)p;
+        node = parent[node];
+    }
+}
+
+// Leaves of more than one point list them in ascending original index (the
+// reference's node2point order).  Morton-sorted positions already are in that
+// order where all the leaf's points share their code (the stable sort keeps
+// index order): every leaf of a leaf-size-1 tree, and any leaf of more than
+// leaf_size points (a cell at the maximum depth).  The other leaves of a tree
+// with larger leaves (at most leaf_size points) are sorted here.
+__global__ void k_leaf_order(const int32_t* __restrict__ leaf_ids, int64_t num_leaves,
+                             const int4* __restrict__ meta, const int32_t* __restrict__ perm,
+                             int leaf_size, int32_t* __restrict__ order) {
+    const int64_t li = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= num_leaves) return;
+    const int4 m = meta[leaf_ids[li]];
+    const int np = node_npts(m);
+    int32_t* o = order + m.y;
+    const bool sort = np <= leaf_size;
+    for (int j = 0; j < np; j++) {  // insertion sort of perm[m.y .. m.y + np), or a copy
+        const int32_t v = perm[(int64_t)m.y + j];
+        int i = j;
+        while (sort && i > 0 && o[i - 1] > v) {
+            o[i] = o[i - 1];
+            i--;
+        }
+        o[i] = v;
+    }
 }
 
 __global__ void k_fill_i32(int32_t* a, int64_t n, int32_t v) {
@@ -501,39 +539,16 @@ int build_impl(const T* pts, int64_t n, int D, int s, cudaStream_t st, Tree* t) 
     CAGR_CUDA(cudaMemcpyAsync(&L, t->n2p_start + M, 8, cudaMemcpyDeviceToHost, st));
     if (int rc = dev_alloc((void**)&t->invperm, sizeof(int32_t) * n, st)) return rc;
     k_inv<<<gN, kBlock, 0, st>>>(t->perm, n, t->invperm);
-    Tmp cnt, off;
-    if (int rc = tmp_alloc(cnt, sizeof(int32_t) * n, st)) return rc;
-    if (int rc = tmp_alloc(off, sizeof(int64_t) * n, st)) return rc;
-    k_walk<false><<<gN, kBlock, 0, st>>>(t->invperm, sk, t->meta, t->children, D, n,
-                                         (int32_t*)cnt.p, nullptr, nullptr, nullptr);
-    if (int rc = cub_call(
-            [&](void* tp, size_t& b) {
-                return cub::DeviceScan::ExclusiveSum(tp, b, (const int32_t*)cnt.p,
-                                                     (int64_t*)off.p, n + 0, st);
-            },
-            st))
-        return rc;
+    if (s > 1) {  // leaves of several codes: their points in original-index order
+        if (int rc = dev_alloc((void**)&t->lorder, sizeof(int32_t) * n, st)) return rc;
+        k_leaf_order<<<grid_for(NL), kBlock, 0, st>>>(t->leaf_ids, NL, t->meta, t->perm, s,
+                                                      t->lorder);
+    }
+    CAGR_CUDA(cudaGetLastError());
     CAGR_CUDA(cudaStreamSynchronize(st));
     if (L <= 0 || L >= (int64_t(1) << 31) - 2)
         return set_error(kErrOverflow, "point-list length out of range: " + std::to_string(L));
-    t->n2p_len = L;
-    Tmp pn, pp, pn2;
-    if (int rc = tmp_alloc(pn, sizeof(int32_t) * L, st)) return rc;
-    if (int rc = tmp_alloc(pp, sizeof(int32_t) * L, st)) return rc;
-    if (int rc = tmp_alloc(pn2, sizeof(int32_t) * L, st)) return rc;
-    if (int rc = dev_alloc((void**)&t->n2p, sizeof(int32_t) * L, st)) return rc;
-    k_walk<true><<<gN, kBlock, 0, st>>>(t->invperm, sk, t->meta, t->children, D, n, nullptr,
-                                        (const int64_t*)off.p, (int32_t*)pn.p, (int32_t*)pp.p);
-    CAGR_CUDA(cudaGetLastError());
-    const int node_bits = bit_width(M);
-    if (int rc = cub_call(
-            [&](void* tp, size_t& b) {
-                return cub::DeviceRadixSort::SortPairs(tp, b, (const uint32_t*)pn.p,
-                                                       (uint32_t*)pn2.p, (const int32_t*)pp.p,
-                                                       t->n2p, L, 0, node_bits, st);
-            },
-            st))
-        return rc;
+    t->n2p_len = L;  // the lists themselves are built by the first export (ensure_n2p)
 
     // sorted positions
     if (int rc = dev_alloc(&t->spos, sizeof(T) * 3 * n, st)) return rc;
@@ -587,7 +602,7 @@ void tree_free(Tree* t) {
     cudaSetDevice(t->device);
     cudaDeviceSynchronize();
     void* arrays[] = {t->perm,     t->invperm,  t->meta,      t->nchild, t->parent,
-                      t->children, t->leaf_ids, t->n2p_start, t->n2p,    t->spos,
+                      t->children, t->leaf_ids, t->n2p_start, t->n2p,    t->spos, t->lorder,
                       t->qgroup,   t->counters, t->rec[0],    t->rec[1], t->rec[2],
                       t->adj_nodes, t->adj_points, t->adj_sums};
     for (void* p : arrays) pool_free(p, nullptr);
@@ -625,10 +640,58 @@ int tree_build(const void* points, int64_t n, int dtype, int max_depth, int leaf
     return kOk;
 }
 
-int tree_export(const Tree* t, int64_t* parent, int64_t* children, uint8_t* is_leaf,
-                void* half_w, int64_t* npts, int64_t* n2p, int64_t* n2p_start,
-                cudaStream_t stream) {
+// The per-node point lists (node2point_index), built once, when first exported.
+int ensure_n2p(Tree* t, cudaStream_t st) {
+    if (t->n2p) return kOk;
+    const int64_t n = t->n, L = t->n2p_len;
+    const unsigned gN = grid_for(n);
+    Tmp leaf_of, cnt, off, pn, pn2, pp;
+    if (int rc = tmp_alloc(leaf_of, sizeof(int32_t) * n, st)) return rc;
+    if (int rc = tmp_alloc(cnt, sizeof(int32_t) * n, st)) return rc;
+    if (int rc = tmp_alloc(off, sizeof(int64_t) * n, st)) return rc;
+    if (int rc = tmp_alloc(pn, sizeof(int32_t) * L, st)) return rc;
+    if (int rc = tmp_alloc(pp, sizeof(int32_t) * L, st)) return rc;
+    if (int rc = tmp_alloc(pn2, sizeof(int32_t) * L, st)) return rc;
+    int32_t* lists = nullptr;
+    if (int rc = dev_alloc((void**)&lists, sizeof(int32_t) * L, st)) return rc;
+    k_leaf_of_pos<<<grid_for(t->num_leaves), kBlock, 0, st>>>(t->leaf_ids, t->num_leaves, t->meta,
+                                                             (int32_t*)leaf_of.p);
+    k_pairs<false><<<gN, kBlock, 0, st>>>(t->invperm, (const int32_t*)leaf_of.p, t->meta,
+                                          t->parent, n, (int32_t*)cnt.p, nullptr, nullptr,
+                                          nullptr);
+    int rc = cub_call(
+        [&](void* tp, size_t& b) {
+            return cub::DeviceScan::ExclusiveSum(tp, b, (const int32_t*)cnt.p, (int64_t*)off.p,
+                                                 n + 0, st);
+        },
+        st);
+    if (!rc) {
+        k_pairs<true><<<gN, kBlock, 0, st>>>(t->invperm, (const int32_t*)leaf_of.p, t->meta,
+                                             t->parent, n, nullptr, (const int64_t*)off.p,
+                                             (int32_t*)pn.p, (int32_t*)pp.p);
+        const int node_bits = bit_width(t->m);
+        rc = cub_call(
+            [&](void* tp, size_t& b) {
+                return cub::DeviceRadixSort::SortPairs(tp, b, (const uint32_t*)pn.p,
+                                                       (uint32_t*)pn2.p, (const int32_t*)pp.p,
+                                                       lists, L, 0, node_bits, st);
+            },
+            st);
+    }
+    if (!rc && cudaGetLastError() != cudaSuccess) rc = set_error(kErrCuda, "point lists launch");
+    if (rc) {
+        pool_free(lists, st);
+        return rc;
+    }
+    t->n2p = lists;
+    return kOk;
+}
+
+int tree_export(Tree* t, int64_t* parent, int64_t* children, uint8_t* is_leaf, void* half_w,
+                int64_t* npts, int64_t* n2p, int64_t* n2p_start, cudaStream_t stream) {
     const int64_t M = t->m;
+    if (n2p)
+        if (int rc = ensure_n2p(t, stream)) return rc;
     if (t->dtype == 0)
         k_export<float><<<grid_for(M), kBlock, 0, stream>>>(t->meta, t->parent, t->children,
                                                             t->n2p_start, M, parent, children,

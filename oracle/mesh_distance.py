@@ -1,4 +1,5 @@
-"""Mesh-to-mesh distances for the reconstruction comparisons (test helper).
+"""Mesh-to-mesh distances for the reconstruction comparisons.  TEST
+INFRASTRUCTURE (the tests and bench.py's CPU-baseline leg use it).
 
 read_ply reads the binary little-endian PLYs both reconstructors write (float
 x, y, z vertices; uchar-counted int faces).  hausdorff(A, B) samples each
@@ -80,7 +81,9 @@ def sample_surface(v, f, n, rng):
 def point_to_mesh(p, v, f, k=16):
     from scipy.spatial import cKDTree
     a, b, c = v[f[:, 0]], v[f[:, 1]], v[f[:, 2]]
+    k = min(k, len(f))
     _, nb = cKDTree((a + b + c) / 3).query(p, k=k, workers=-1)
+    nb = nb.reshape(len(p), k)
     best = np.full(len(p), np.inf)
     for j in range(k):
         t = nb[:, j]

@@ -68,6 +68,12 @@ def build_oracle(force: bool = False) -> None:
     gpu_lib = os.path.join(HERE, "_ref", "libwnref_gpu.so")
     if REF_ROOT and (force or not os.path.exists(gpu_lib)):
         subprocess.check_call(["make", "-s", "-C", HERE, "ref-gpu", f"REF_ROOT={REF_ROOT}"])
+    # the reference's marching-cubes tables and its CPU reconstructor (baselines)
+    for target, path in (("ref-mc", "libref_mc.so"), ("ref-gaussrecon", "main_GaussRecon_cpu")):
+        if REF_ROOT and (force or not os.path.exists(os.path.join(HERE, "_ref", path))):
+            if force and os.path.exists(os.path.join(HERE, "_ref", path)):
+                os.remove(os.path.join(HERE, "_ref", path))
+            subprocess.check_call(["make", "-s", "-C", HERE, target, f"REF_ROOT={REF_ROOT}"])
 
 
 def _ptr(a: np.ndarray | None):

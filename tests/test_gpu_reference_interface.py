@@ -220,7 +220,7 @@ def test_cpp_driver_mesh_is_near_the_reference_cpu_reconstruction(cuda_lib, tmp_
     on average and to about two cells at worst (distances over the bounding-box
     diagonal)."""
     from cagr_b200.build import GAUSSRECON_PATH, build_gaussrecon
-    from tests._mesh_distance import hausdorff, read_ply
+    from oracle.mesh_distance import hausdorff, read_ply
     if not os.path.exists(REF_GAUSSRECON):
         pytest.skip("the reference reconstructor is not built (make -C oracle ref-gaussrecon)")
     if not os.path.exists(GAUSSRECON_PATH):

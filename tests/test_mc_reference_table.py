@@ -124,9 +124,9 @@ def test_oracle_rejects_an_uncrossed_edge(oracle):
 
 
 def test_mesh_distance_helper_is_exact_on_triangles():
-    """tests/_mesh_distance.py's point-to-triangle distance equals the minimum
+    """oracle/mesh_distance.py's point-to-triangle distance equals the minimum
     over a dense barycentric sampling of each triangle (to the sampling step)."""
-    from tests._mesh_distance import _closest_on_triangles
+    from oracle.mesh_distance import _closest_on_triangles
     rng = np.random.default_rng(91)
     n = 200
     a, b, c = (rng.normal(size=(n, 3)) for _ in range(3))
