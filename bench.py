@@ -342,13 +342,15 @@ def interp_leg(args, P, W, MU, WV, p, widths, mu, dev, stream, flush, rank):
 
 
 def reference_reconstruction(points: np.ndarray, normals: np.ndarray, verts: np.ndarray,
-                             faces: np.ndarray) -> dict:
+                             faces: np.ndarray, like: tuple | None = None) -> dict:
     """The reference's CPU reconstructor (build_GR_cpu.sh's sources, built by
     `make -C oracle ref-gaussrecon`: its adaptive octree, host treecode with the
     plain Gauss operator, octree marching cubes) on the oriented cloud of this
     run's solve, timed as a whole program on the host cores (it sets 20 OpenMP
     threads itself), and the distance between its mesh and this run's 512^3
-    reconstruction of the same oriented cloud.  A CPU-baseline leg: the reference
+    reconstruction of the same oriented cloud (verts, faces), and `like`: a
+    512^3 reconstruction with the reference driver's own operator and weights
+    (A, unit normals times area 1e-5).  A CPU-baseline leg: the reference
     build is test infrastructure under oracle/."""
     exe = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle", "_ref",
                        "main_GaussRecon_cpu")
@@ -368,12 +370,18 @@ def reference_reconstruction(points: np.ndarray, normals: np.ndarray, verts: np.
         rv, rf = read_ply(ply)
     diag = float(np.linalg.norm(rv.max(0) - rv.min(0)))
     H, mean = hausdorff((verts.astype(np.float64), faces), (rv, rf), n=100_000)
-    return {"value": round(seconds, 3), "unit": "s", "cores": os.cpu_count(), "threads": 20,
-            "kind": "reference", "program": "main_GaussRecon_cpu (build_GR_cpu.sh sources)",
-            "input": f"this run's {len(points):,} points with their solved normals",
-            "mesh_vertices": int(rv.shape[0]), "mesh_faces": int(rf.shape[0]),
-            "hausdorff_over_diagonal_vs_ours": round(H / diag, 5),
-            "mean_distance_over_diagonal_vs_ours": round(mean / diag, 6)}
+    out = {"value": round(seconds, 3), "unit": "s", "cores": os.cpu_count(), "threads": 20,
+           "kind": "reference", "program": "main_GaussRecon_cpu (build_GR_cpu.sh sources)",
+           "input": f"this run's {len(points):,} points with their solved normals",
+           "mesh_vertices": int(rv.shape[0]), "mesh_faces": int(rf.shape[0]),
+           "hausdorff_over_diagonal_vs_ours": round(H / diag, 5),
+           "mean_distance_over_diagonal_vs_ours": round(mean / diag, 6),
+           "ours": "end_to_end's mesh: A3, weights |mu|, 512^3 over [-1.2, 1.2]^3"}
+    if like is not None:
+        H2, mean2 = hausdorff((like[0].astype(np.float64), like[1]), (rv, rf), n=100_000)
+        out["hausdorff_over_diagonal_vs_ours_same_operator"] = round(H2 / diag, 5)
+        out["mean_distance_over_diagonal_vs_ours_same_operator"] = round(mean2 / diag, 6)
+    return out
 
 
 def run_ours(args, rank: int, world: int, local_rank: int):
@@ -538,7 +546,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     # end to end: the whole CAGR normal solve on this cloud (tree build + 40
     # iterations + 8 G steps, main_CAGR.py's schedule, preset l0)
-    solve = solve64 = our_mesh = None
+    solve = solve64 = our_mesh = our_mesh_like = None
     if not args.no_solve:
         from cagr_b200.mesh import reconstruct
         from cagr_b200.solver import PRESET_WIDTHS, cagr_solve
@@ -573,6 +581,11 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         solve = record(res, rec, t_solve, t_rec, c_solve + c_rec)
         our_mesh = (rec.vertices.cpu().numpy(), rec.faces.cpu().numpy(),
                     res.normals.float().cpu().numpy())
+        del rec
+        # the same normals through the reference CPU driver's operator and weights
+        # (A, n / |n| * 1e-5), for the like-for-like mesh distance
+        rec = reconstruct(P, res.normals.float(), grid=args.grid, area=1e-5, op="A")
+        our_mesh_like = (rec.vertices.cpu().numpy(), rec.faces.cpu().numpy())
         del rec
         if not args.no_fp64:
             # the same pipeline in float64 throughout (points, widths, moments, pair
@@ -627,7 +640,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     achieved = terms_dom * fpt / (dur * 1e-3) / 1e12
     cpu = recon_ref = None
     if not args.no_cpu_baseline and our_mesh is not None:
-        recon_ref = reference_reconstruction(p, our_mesh[2], our_mesh[0], our_mesh[1])
+        recon_ref = reference_reconstruction(p, our_mesh[2], our_mesh[0], our_mesh[1],
+                                             our_mesh_like)
     if not args.no_cpu_baseline:
         import multiprocessing
         threads = multiprocessing.cpu_count()

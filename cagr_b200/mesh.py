@@ -149,7 +149,7 @@ def reconstruct(points: torch.Tensor, mu: torch.Tensor, grid: int = 128,
                 lo: float = -1.2, hi: float = 1.2, width: float = 0.01,
                 area: float | None = None, tree: WindingNumberTreecode | None = None,
                 max_tree_depth: int = 15, far_field: str = "reference", degree: int = 5,
-                theta: float = 0.5) -> Reconstruction:
+                theta: float = 0.5, op: str = "A3") -> Reconstruction:
     """Surface of oriented points on a regular grid**3 over [lo, hi]^3.
 
     points [N,3] float32 CUDA (normalised), mu [N,3] area-weighted normals (the
@@ -157,7 +157,11 @@ def reconstruct(points: torch.Tensor, mu: torch.Tensor, grid: int = 128,
     with that weight per point, as the GaussRecon driver does (area 1e-5,
     main_GaussRecon_cuda.cu:276-288); if None, mu is used as it is (weights |mu|).
     far_field / degree / theta: the far-field mode of a tree built here.
+    op: the field operator, "A3" as the CUDA GaussRecon driver or "A" as the
+    CPU one (main_GaussRecon_cpu.cpp), continuous kernel either way.
     """
+    if op not in ("A3", "A"):
+        raise ValueError("op must be 'A3' or 'A'")
     dev = points.device
     sec = {}
     t0 = time.perf_counter()
@@ -173,14 +177,14 @@ def reconstruct(points: torch.Tensor, mu: torch.Tensor, grid: int = 128,
     else:
         attrs, weights = mu.contiguous(), None
     wn.scatter(attrs, weights=weights)
-    samples = wn.multiply("A3", float(width), continuous=True)[:, 0]
+    samples = wn.multiply(op, float(width), continuous=True)[:, 0]
     n = samples.shape[0]
     # grid value = -field and iso = -(median field at the samples), as the GaussRecon
     # program sets them (main_GaussRecon_cuda.cu:478,485-486): with outward normals
     # the field is lower inside, so inside = value > iso
     iso = -float(torch.kthvalue(samples.float(), n // 2 + 1).values)  # nth_element(n/2)
     spacing = (hi - lo) / (grid - 1)
-    field = field_grid(wn, (grid, grid, grid), (lo, lo, lo), spacing, float(width))
+    field = field_grid(wn, (grid, grid, grid), (lo, lo, lo), spacing, float(width), op=op)
     field.neg_()
     torch.cuda.synchronize(dev)
     sec["field"] = time.perf_counter() - t0
