@@ -117,7 +117,10 @@ int cagr_tree_info(const cagr_tree* tree, int64_t* num_points, int64_t* num_node
 /* Writes the tree in the reference layout (build_tree's seven tensors,
  * wn_treecode_cpu_torch_interface.cpp:73-101): parent[M] i64 (-1 root),
  * children[M,8] i64 (-1 none), is_leaf[M] u8, half_w[M] (tree dtype),
- * npts[M] i64, n2p[L] i64, n2p_start[M] i64.  Any output may be NULL. */
+ * npts[M] i64, n2p[L] i64, n2p_start[M] i64.  Any output may be NULL.  The
+ * per-node point lists (n2p) are built, and kept with the tree, by the first
+ * call that asks for them (a walk over every point's leaf-to-root path and a
+ * radix sort); the build itself does not make them. */
 int cagr_tree_export(const cagr_tree* tree, int64_t* parent_dev, int64_t* children_dev,
                      uint8_t* is_leaf_dev, void* half_w_dev, int64_t* npts_dev, int64_t* n2p_dev,
                      int64_t* n2p_start_dev, void* stream);
