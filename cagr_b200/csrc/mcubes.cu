@@ -455,6 +455,11 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
     __shared__ uint8_t s_m[kEmitWarps][4][kChunk + 1];     // crossed edges (bit a: +axis a)
     __shared__ uint16_t s_pre[kEmitWarps][4][kChunk];      // in-unit vertex prefix
     __shared__ int64_t s_base[kEmitWarps][8];              // R: unit base; 4 + R: next unit's
+    __shared__ int8_t s_tri[256 * 3 * kMaxTri];            // the case table, per block
+    __shared__ uint8_t s_ntri[256];
+    for (int i = (int)threadIdx.x; i < 256 * 3 * kMaxTri; i += 32 * kEmitWarps) s_tri[i] = tri[i];
+    for (int i = (int)threadIdx.x; i < 256; i += 32 * kEmitWarps) s_ntri[i] = ntri[i];
+    __syncthreads();
     const int lane = (int)threadIdx.x & 31, wid = (int)threadIdx.x >> 5;
     const uint32_t n_act = *nactive;
     for (uint32_t a = blockIdx.x * kEmitWarps + wid; a < n_act; a += gridDim.x * kEmitWarps) {
@@ -582,28 +587,39 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
         }
         // triangles of this unit's cells, in x order
         if (j + 1 < g.ny && k + 1 < g.nz) {
-            int64_t fo = tb;
+            // the 4 words' cases and counts, then their 4 scans side by side
+            int cs[4], nt[4], incl[4];
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const int x = i0 + lane + 32 * q;
-                int cs = 0, nt = 0;
+                cs[q] = 0;
+                nt[q] = 0;
                 if (x + 1 < g.nx) {
 #pragma unroll
                     for (int R = 0; R < 4; R++)
-                        cs |= (int)((__funnelshift_r(w[R][q], w[R][q + 1], lane) & 3u) << (2 * R));
-                    nt = __ldg(&ntri[cs]);
+                        cs[q] |=
+                            (int)((__funnelshift_r(w[R][q], w[R][q + 1], lane) & 3u) << (2 * R));
+                    nt[q] = s_ntri[cs[q]];
                 }
-                int incl = nt;  // warp inclusive scan of the triangle counts
+                incl[q] = nt[q];
+            }
 #pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += t;
+            for (int o = 1; o < 32; o <<= 1) {  // warp inclusive scans of the counts
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int t = __shfl_up_sync(0xffffffffu, incl[q], o);
+                    if (lane >= o) incl[q] += t;
                 }
-                const int64_t first = fo + (incl - nt);
-                for (int t3 = 0; t3 < nt; t3++) {
+            }
+            int64_t fo = tb;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int64_t first = fo + (incl[q] - nt[q]);
+                fo += __shfl_sync(0xffffffffu, incl[q], 31);
+                for (int t3 = 0; t3 < nt[q]; t3++) {
 #pragma unroll
                     for (int sv = 0; sv < 3; sv++) {
-                        const int e = __ldg(&tri[cs * 3 * kMaxTri + 3 * t3 + sv]);
+                        const int e = s_tri[cs[q] * 3 * kMaxTri + 3 * t3 + sv];
                         const int ax = e >> 2, eu = e & 1, ew = (e >> 1) & 1;
                         // the point owning edge e of this cell: (dx, row R = dy + 2 dz)
                         const int dx = ax == 0 ? 0 : eu;
@@ -618,7 +634,6 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
                         if (first + t3 < max_faces) faces[3 * (first + t3) + sv] = (int32_t)id;
                     }
                 }
-                fo += __shfl_sync(0xffffffffu, incl, 31);
             }
         }
         __syncwarp();  // the shared rows are rewritten by the warp's next unit
