@@ -64,6 +64,10 @@ constexpr int kChunk = 2048;      // points per proxy-charge block
 // evaluate two records per instruction.
 constexpr int kBlk = 20;
 constexpr int kComp = 9;
+// The A2T sum's walk layout: blocks of kBlkES scalars, components (y0, y1, y2,
+// e0 s0, e1 s1, e2 s2) -- all its pair term reads of a source (48 bytes per
+// record pair in float: three 16-byte loads).
+constexpr int kBlkES = 12;
 constexpr unsigned kAll = 0xffffffffu;
 // the pipelined walk's shape (see k_iwalk)
 #ifndef CAGR_IW_SLOTS
@@ -107,13 +111,15 @@ struct Interp {
     void* pts[4] = {nullptr, nullptr, nullptr, nullptr};   // [N*12] T point records per slot
     void* prox[4] = {nullptr, nullptr, nullptr, nullptr};  // [num_interp*P3*12] T proxy records
     int dim[4] = {0, 0, 0, 0};     // attribute dim held by the slot (0 = empty)
+    void* ptsc = nullptr;          // slot 3 in the A2T sum's walk layout: points
+    void* proxc = nullptr;         //   and proxy records
     double cheb[kPMax] = {}, omega[kPMax] = {};  // Chebyshev points and barycentric weights
     int* err = nullptr;            // device flag: a walk's staging wait ran out
     uint32_t spin = 1u << 22;      // try_wait rounds before a staging wait runs out
     // Self-query walks run their groups longest first: each walk records every
-    // group's cost (tiles summed), and the groups are sorted by it for the next.
+    // group's cost (record pairs summed), and the groups are sorted by it for the next.
     int64_t ngroups = 0;
-    uint32_t* gcost = nullptr;     // [ngroups] tiles of each group in the last self walk
+    uint32_t* gcost = nullptr;     // [ngroups] record pairs of each group in the last self walk
     uint32_t* gcost_sorted = nullptr;
     int32_t* giota = nullptr;      // [ngroups] 0, 1, 2, ...
     int32_t* gorder = nullptr;     // [ngroups] groups, most expensive first
@@ -248,17 +254,20 @@ __global__ void k_ipoints(const T* __restrict__ spos, const int32_t* __restrict_
 }
 
 // The records of the three-column slot (sum_k A2Tk) in their walk form: the
-// exp factor e_k = exp(-y_k/2) replaced by its product with the column's
-// charge, e_k s_k, which is all the A2T sum reads of a source (the walk
-// multiplied the same two numbers for every pair; now once per record).
+// position and, per k, exp(-y_k/2) times the column's charge s_k -- all the
+// A2T sum reads of a source (the walk multiplied the same two numbers for
+// every pair; now once per record) -- in blocks of kBlkES scalars.
 template <typename T>
-__global__ void k_es_form(T* __restrict__ rec, int64_t nblocks) {
+__global__ void k_es_compact(const T* __restrict__ rec, T* __restrict__ out, int64_t nblocks) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 2 * nblocks) return;
-    T* b = rec + (i >> 1) * kBlk + (i & 1);
+    const T* b = rec + (i >> 1) * kBlk + (i & 1);
+    T* o = out + (i >> 1) * kBlkES + (i & 1);
     constexpr int kCharge[3] = {3, 7, 8};
 #pragma unroll
-    for (int k = 0; k < 3; k++) b[2 * (4 + k)] = b[2 * (4 + k)] * b[2 * kCharge[k]];
+    for (int c = 0; c < 3; c++) o[2 * c] = b[2 * c];
+#pragma unroll
+    for (int k = 0; k < 3; k++) o[2 * (3 + k)] = b[2 * (4 + k)] * b[2 * kCharge[k]];
 }
 
 template <typename T>
@@ -465,7 +474,7 @@ struct IWalk {
     int accumulate = 0;
     unsigned long long* counter = nullptr;  // next group of 32 queries (persistent launch)
     const int32_t* gorder = nullptr;        // the order groups are taken in (null: their own)
-    uint32_t* gcost = nullptr;              // tiles summed per group, when non-null
+    uint32_t* gcost = nullptr;              // record pairs summed per group, when non-null
     int* err = nullptr;                     // set when a staging wait runs out
     uint32_t spin = 0;                      // try_wait rounds before a wait runs out
 };
@@ -562,6 +571,35 @@ __device__ __forceinline__ Blk<double> load_blk(const double* b) {
     for (int c = 0; c < kComp; c++) k.c[c] = *reinterpret_cast<const double2*>(b + 2 * c);
     return k;
 }
+// A block of the A2T sum's walk layout: positions into components 0..2, the
+// e_k s_k into 4..6 (where the full layout keeps e_k).
+__device__ __forceinline__ Blk<float> load_blk_es(const float* b) {
+    const float4 A = ld4(b), B = ld4(b + 4), C = ld4(b + 8);
+    Blk<float> k;
+    k.c[0] = pk(A.x, A.y);
+    k.c[1] = pk(A.z, A.w);
+    k.c[2] = pk(B.x, B.y);
+    k.c[4] = pk(B.z, B.w);
+    k.c[5] = pk(C.x, C.y);
+    k.c[6] = pk(C.z, C.w);
+    k.c[3] = k.c[7] = k.c[8] = pk(0.0f, 0.0f);
+    return k;
+}
+__device__ __forceinline__ Blk<double> load_blk_es(const double* b) {
+    Blk<double> k;
+#pragma unroll
+    for (int c = 0; c < 3; c++) k.c[c] = *reinterpret_cast<const double2*>(b + 2 * c);
+#pragma unroll
+    for (int c = 0; c < 3; c++) k.c[4 + c] = *reinterpret_cast<const double2*>(b + 6 + 2 * c);
+    k.c[3] = k.c[7] = k.c[8] = make_double2(0.0, 0.0);
+    return k;
+}
+
+// scalars per block (record pair) in the walk of operator OP
+template <int OP>
+constexpr int blk_of() {
+    return OP == kIOpA2TSum ? kBlkES : kBlk;
+}
 
 // The query's values as pairs (both halves equal).
 template <typename T>
@@ -584,7 +622,9 @@ __device__ __forceinline__ void pterm(const IQ<T>& q, const IQ2<T>& q2, const T*
         p0 = add2(p0, pk(ra ? T(1) : T(0), rb ? T(1) : T(0)));
         return;
     } else {
-        const Blk<T> k = load_blk(b);
+        Blk<T> k;
+        if constexpr (OP == kIOpA2TSum) k = load_blk_es(b);
+        else k = load_blk(b);
         const P2<T> m1 = pk(T(-1), T(-1));
         const P2<T> dx = fma2(k.c[0], m1, q2.x);
         const P2<T> dy = fma2(k.c[1], m1, q2.y);
@@ -694,14 +734,14 @@ __device__ __forceinline__ void itile(const IQ<T>& q, const IQ2<T>& q2, bool act
     for (; j + kUnrollB <= j1; j += kUnrollB) {
 #pragma unroll
         for (int u = 0; u < kUnrollB; u++)
-            pterm<T, OP, CONT, NEAR, false>(q, q2, b + (int64_t)(j + u) * kBlk, 3u, p0, p1, p2, h0,
+            pterm<T, OP, CONT, NEAR, false>(q, q2, b + (int64_t)(j + u) * blk_of<OP>(), 3u, p0, p1, p2, h0,
                                             h1, h2, i0, i1, i2);
     }
     for (; j < j1; j++)
-        pterm<T, OP, CONT, NEAR, false>(q, q2, b + (int64_t)j * kBlk, 3u, p0, p1, p2, h0, h1, h2,
+        pterm<T, OP, CONT, NEAR, false>(q, q2, b + (int64_t)j * blk_of<OP>(), 3u, p0, p1, p2, h0, h1, h2,
                                         i0, i1, i2);
     if (last_masked)
-        pterm<T, OP, CONT, NEAR, true>(q, q2, b + (int64_t)(nb - 1) * kBlk, 1u, p0, p1, p2, h0, h1,
+        pterm<T, OP, CONT, NEAR, true>(q, q2, b + (int64_t)(nb - 1) * blk_of<OP>(), 1u, p0, p1, p2, h0, h1,
                                        h2, i0, i1, i2);
     if (!active) return;
     if constexpr (OP == kOpCount) {
@@ -904,10 +944,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
     return false;
 }
 
-// blocks (record pairs) per tile: 38 in float, 19 in double
-template <typename T>
+// blocks (record pairs) per tile: 51 in float, 25 in double (the A2T sum's walk
+// layout: 85, 42)
+template <typename T, int OP>
 constexpr int tile_blocks() {
-    return kTileBytes / (kBlk * (int)sizeof(T));
+    return kTileBytes / (blk_of<OP>() * (int)sizeof(T));
 }
 
 template <typename T>
@@ -927,7 +968,8 @@ __global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
         mbar_init_fence();
     }
     __syncwarp();
-    constexpr int kTB = tile_blocks<T>();
+    constexpr int kTB = tile_blocks<T, OP>();
+    constexpr int kB = blk_of<OP>();
     static_assert(kTB < 128 && kSlots <= 6, "tile fields: 7-bit block count, 10 bits per slot");
     // warp-uniform pipeline state: next slot to consume, tiles in flight, the
     // parity of each slot's next completion, and each slot's tile in 10 bits:
@@ -943,7 +985,10 @@ __global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
         ticket = __shfl_sync(kAll, ticket, 0);
         if ((int64_t)ticket >= ngroups) break;
         const int64_t grp = p.gorder ? (int64_t)__ldg(p.gorder + ticket) : (int64_t)ticket;
-        uint32_t ntiles = 0;  // this group's tiles (its cost, for the next walk's order)
+        // this group's record pairs (its cost, for the next walk's order: the same
+        // measure whatever the walk's layout, so walks of different operators
+        // order each other's groups alike)
+        uint32_t ncost = 0;
         const int64_t qi = grp * 32 + lane;
         IQ<T> q;
         int64_t oidx;
@@ -1042,8 +1087,8 @@ __global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
                     const int nb = min(left, kTB);
                     const int slot = (head + inflight) % kSlots;
                     if (lane == 0)
-                        tma_load_1d(tiles + (size_t)slot * kTileBytes, base + blk * kBlk,
-                                    (uint32_t)(nb * kBlk * sizeof(T)), bars + slot);
+                        tma_load_1d(tiles + (size_t)slot * kTileBytes, base + blk * kB,
+                                    (uint32_t)(nb * kB * sizeof(T)), bars + slot);
                     const uint64_t f = (uint64_t)(nb | (near << 7) | (skip_first << 8) |
                                                   ((nb == left ? skip_last : 0) << 9));
                     tinfo = (tinfo & ~(0x3ffull << (10 * slot))) | (f << (10 * slot));
@@ -1075,11 +1120,11 @@ __global__ void __launch_bounds__(kPWarps * 32) k_iwalk(const IWalk<T> p) {
                 __syncwarp();  // every lane has read the slot before it is refilled
                 head = (head + 1) % kSlots;
                 inflight--;
-                ntiles++;
+                ncost += (uint32_t)nbt;
             }
             g = gnext;
         }
-        if (p.gcost && lane == 0) p.gcost[grp] = ntiles;
+        if (p.gcost && lane == 0) p.gcost[grp] = ncost;
         if (!valid) continue;
         T* o = p.out + oidx * (int64_t)p.out_stride;
         const int acc = p.accumulate;
@@ -1272,10 +1317,18 @@ int scatter_impl(Tree* t, Interp* I, int slot, const void* attrs, int dim, cudaS
             I->chunk_first, I->num_interp, I->chunks, (const T*)I->part, (const T*)I->box_c,
             (const T*)I->box_h, cp, (T*)I->prox[slot]);
     }
-    if (slot == 3) {  // the A2T sum's slot: e_k s_k in place of e_k
+    if (slot == 3) {  // the A2T sum's slot: its walk layout
         const int64_t pb = (N + 1) / 2, xb = I->num_interp * P3e / 2;
-        k_es_form<T><<<blocks_for(2 * pb, 256), 256, 0, s>>>((T*)I->pts[slot], pb);
-        if (xb > 0) k_es_form<T><<<blocks_for(2 * xb, 256), 256, 0, s>>>((T*)I->prox[slot], xb);
+        if (!I->ptsc)
+            if (int rc = pool_alloc(&I->ptsc, sizeof(T) * kBlkES * (size_t)pb, s)) return rc;
+        if (!I->proxc)
+            if (int rc = pool_alloc(&I->proxc, sizeof(T) * kBlkES * (size_t)(xb > 0 ? xb : 1), s))
+                return rc;
+        k_es_compact<T><<<blocks_for(2 * pb, 256), 256, 0, s>>>((const T*)I->pts[slot],
+                                                                 (T*)I->ptsc, pb);
+        if (xb > 0)
+            k_es_compact<T><<<blocks_for(2 * xb, 256), 256, 0, s>>>((const T*)I->prox[slot],
+                                                                     (T*)I->proxc, xb);
     }
     CAGR_CUDA(cudaGetLastError());
     I->dim[slot] = dim;
@@ -1338,8 +1391,8 @@ int traverse_impl(const Tree* t, Interp* I, const TraverseArgs& a, cudaStream_t 
     if (I->dim[slot] == 0 || I->dim[slot] != need)
         return set_error(kErrState, "the charges of the right attribute dim are not computed "
                                     "(cagr_scatter / cagr_scatter3 first)");
-    p.pts = (const T*)I->pts[slot];
-    p.prox = (const T*)I->prox[slot];
+    p.pts = (const T*)(slot == 3 ? I->ptsc : I->pts[slot]);
+    p.prox = (const T*)(slot == 3 ? I->proxc : I->prox[slot]);
     const int out_dim = (op == kOpA || op == kOpA3 || op == kOpA21 || op == kOpA22 ||
                          op == kOpA23 || op == kOpCount) ? 1 : 3;
     p.out_stride = a.out_stride > 0 ? a.out_stride : out_dim;
@@ -1416,7 +1469,8 @@ void interp_free(Tree* t) {
     if (!I) return;
     void* arrays[] = {I->box_c, I->box_h, I->iidx, I->chunks, I->chunk_first, I->part, I->err,
                       I->pts[0], I->pts[1], I->pts[2], I->pts[3],
-                      I->prox[0], I->prox[1], I->prox[2], I->prox[3], I->gcost,
+                      I->prox[0], I->prox[1], I->prox[2], I->prox[3], I->ptsc, I->proxc,
+                      I->gcost,
                       I->gcost_sorted, I->giota, I->gorder, I->gsort_tmp};
     for (void* p : arrays) pool_free(p, nullptr);
     delete I;
