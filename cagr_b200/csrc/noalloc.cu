@@ -1,12 +1,10 @@
 // Node moments without any device allocation: cagr_scatter_noalloc.
 //
 // Who needs it: callers that cannot call cudaMalloc at the moment they need
-// node moments -- code recording a CUDA graph (allocation APIs are not
-// allowed inside a stream capture), processes whose device memory is fully
-// owned by another allocator (a framework's caching pool that must not be
-// bypassed, a fixed memory budget), or host code that already holds the tree
-// in the reference's layout (the seven arrays of build_tree) and has no tree
-// handle.  The caller passes the tree arrays, the inputs and the three output
+// node moments -- processes whose device memory is fully owned by another
+// allocator (a framework's caching pool that must not be bypassed, a fixed
+// memory budget) -- or host code that already holds the tree in the
+// reference's layout (the seven arrays of build_tree) and has no tree handle.  The caller passes the tree arrays, the inputs and the three output
 // arrays; the only scratch the computation needs -- one arrival counter per
 // node -- lives in a fixed file-scope device array, so no call allocates.
 //
@@ -21,8 +19,7 @@
 //    results.  Order them on one stream.  Each call clears the counters it
 //    uses before its kernel runs;
 //  * the first call on a device looks up the array's device address (once per
-//    device, with that device current); make that first call before any
-//    stream capture begins.
+//    device, with that device current).
 //
 // The computation is the same bottom-up pass as the tree-handle path
 // (moments.cu) and the same floating-point operation order as the reference

@@ -250,16 +250,15 @@ int cagr_mc_table(int8_t* tri, uint8_t* ntri);
  * cagr_scatter_export) computed from tree arrays in the reference layout
  * (parent, children, is_leaf, npts, n2p, n2p_start as cagr_tree_export
  * writes them; num_nodes = M) WITHOUT ANY DEVICE ALLOCATION, for callers that
- * cannot allocate at this point (inside a CUDA-graph capture, under a fixed
- * memory budget owned by another allocator, or holding only the reference
- * arrays and no tree handle).  Inputs (points [n,3], weights [n] or NULL for
+ * cannot allocate at this point (under a fixed memory budget owned by another
+ * allocator, or holding only the reference arrays and no tree handle).  Inputs (points [n,3], weights [n] or NULL for
  * |attr|, attrs [n, attr_dim]) and outputs (node_attrs [M, attr_dim],
  * reppoints [M,3], node_weights [M]) are the caller's; dtype CAGR_F32 or
  * CAGR_F64.  The per-node scratch lives in one fixed device array of
  * 2,097,152 nodes (8 MiB, held by every GPU that loads the library until
  * exit); larger trees return CAGR_ERR_INVALID.  All calls share that array:
  * calls that overlap on the GPU race, so order them on one stream.  The first
- * call on a device looks the array up; make it before any stream capture.
+ * call on a device looks the array up.
  * Every buffer and the stream must belong to the CURRENT device (the scratch
  * array is the current device's; a buffer of another device is not detected). */
 int cagr_scatter_noalloc(const int64_t* parent_dev, const int64_t* children_dev,

@@ -1,8 +1,8 @@
 """GPU: cagr_scatter_noalloc, the node-moment entry point that allocates nothing.
 
 It exists for callers that cannot call cudaMalloc when they need node
-moments (during a CUDA-graph capture, under a device-memory budget owned by
-another allocator, or holding only the reference's tree arrays).  Its scratch
+moments (under a device-memory budget owned by another allocator, or holding
+only the reference's tree arrays).  Its scratch
 is a fixed device array shared by every call, so this test runs it twice in a
 row -- with different inputs and dtypes -- and checks each result against the
 allocating path (cagr_scatter + cagr_scatter_export), which computes the same
