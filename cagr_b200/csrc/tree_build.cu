@@ -203,10 +203,9 @@ __global__ void k_chain(const int8_t* __restrict__ lcp, int64_t n, int D, int s,
 // level k0 - 1 + i at j is the min of prev[j + t h] over t < 2^i (h = 2^(k0-1),
 // positions past n skipped), the union of those windows being [j, j + 2^i h).
 // The strided reads of neighbouring threads are coalesced and come from L2.
-// (measured at 1M points: 19 launches of one level 122 us, 5 launches of four
-// levels 94 us -- a launch of L levels reads 2^L values per thread; two levels
-// per launch balance launches against reads)
-constexpr int kLevelsPerLaunch = 2;
+// (measured at 1M points, ncu launch durations: 19 launches of one level
+// 122 us, 10 of two levels 107 us, 5 of four levels 94 us)
+constexpr int kLevelsPerLaunch = 4;
 
 __global__ void k_sparse_levels(const int8_t* __restrict__ prev, int8_t* __restrict__ out,
                                 int64_t n, int64_t h, int m) {
