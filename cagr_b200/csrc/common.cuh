@@ -182,4 +182,68 @@ __device__ __forceinline__ double mac_radius2_bits(int depth, double) {
     return __longlong_as_double((long long)(1027 - 2 * depth) << 52);
 }
 
+// ---- shared-memory barriers and one-dimensional bulk copies (TMA) ----------
+//
+// A copy's completion is counted on an mbarrier as transaction bytes; a wait
+// is a bounded number of try_wait rounds, so a kernel whose copy or peer never
+// arrives sets an error flag and ends instead of spinning.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+// an mbarrier whose phase completes after `count` arrivals (and the bytes
+// announced by arrivals with expect_tx)
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count = 1) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// one arrival that also announces `bytes` of copies completing on this phase
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// bytes from global src to shared dst (both 16-byte aligned, bytes a multiple
+// of 16), counted on bar; the caller has announced them
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
+                                              uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+// before a copy overwrites shared memory that was read through the generic proxy
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// one copy on a barrier of one arrival: announce its bytes and start it
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, uint32_t bytes,
+                                            uint64_t* bar) {
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(bar, bytes);
+    bulk_copy_g2s(dst, src, bytes, bar);
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// true once the phase of the given parity has completed; false after `spin` rounds
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t spin) {
+    for (uint32_t it = 0; it < spin; it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
 }  // namespace cagr

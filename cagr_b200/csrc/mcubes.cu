@@ -51,7 +51,9 @@
 namespace cagr {
 namespace {
 
-constexpr int kMaxTri = 12;  // the generator checks the bound
+constexpr int kMaxTri = 12;   // triangles a case row of the exported table has room for
+constexpr int kCellTris = 5;  // triangles a case has (the generator and the reference-layout
+                              // check enforce it)
 constexpr int kChunk = 128;  // grid points per unit
 
 struct McTable {
@@ -175,7 +177,7 @@ bool build_table(McTable& T, std::string& err) {
             if (area[0] * g[0] + area[1] * g[1] + area[2] * g[2] < 0)
                 std::reverse(cyc.begin(), cyc.end());
             for (size_t i = 1; i + 1 < cyc.size(); i++) {
-                if (nt >= kMaxTri) {
+                if (nt >= kCellTris) {
                     err = "too many triangles in one cell";
                     return false;
                 }
@@ -241,7 +243,7 @@ bool table_from_reference_layout(const int8_t* tri16, McTable& T, std::string& e
         const int8_t* row = tri16 + 16 * ci;
         int len = 0;
         while (len < 16 && row[len] != -1) len++;
-        if (len == 16 || len % 3 != 0 || len / 3 > 5) {
+        if (len == 16 || len % 3 != 0 || len / 3 > kCellTris) {
             err = "case " + std::to_string(ci) + ": not a -1 terminated list of at most 5 triangles";
             return false;
         }
@@ -289,68 +291,168 @@ __device__ __forceinline__ float root_t(float v0, float v1, float iso) {
 // warps per block at consecutive j.  A unit needs the point rows (j, k),
 // (j+1, k), (j, k+1), (j+1, k+1); walking up in k, the k+1 rows of one unit are
 // the k rows of the next, so each unit reads two new rows, and the rows of the
-// unit after next are loaded before this one is counted (their latency overlaps
-// the work).  Lane l holds the points x = i0 + l + 32 q (q < 4, coalesced) and
-// lane 0 also x = i0 + kChunk (the next unit's first point).
+// next kCountAhead units are in flight while one is counted (their latency
+// overlaps the work).  VEC (rows 16-byte aligned: nx a multiple of 4): lane l
+// holds x = i0 + 4 l + q (q < 4) from one 16-byte load; otherwise lane l holds
+// x = i0 + l + 32 q (coalesced scalar loads).  Every lane also holds
+// x = i0 + kChunk (the next unit's first point, one broadcast load).
 //
-// Most units lie away from the surface: every point of their 4 rows is on the
-// same side.  Each row keeps, per lane, the minimum and maximum of its points
-// (a point outside the grid or in a missing row loads as NaN, which fmin and
-// fmax ignore; a NaN value of the field, which is outside, loads as -inf, or
-// +inf when inside means below the iso-value); two warp votes on the 4 rows'
-// extremes then settle such a unit with no bit work.  The others are counted
-// from ballots: inside-bit words w[q] held by every lane, where a funnel shift of
-// (w[q+1] : w[q]) by l gives the inside bits of x and x + 1, so a point's
-// crossings and cell case are a few bit operations.
+// Coordinates past the grid are clamped to the row's last point and a missing
+// row (j + 1 = ny, k + 1 = nz) is read as the unit's own row j or plane k: the
+// copies are points of the same unit, so its extremes do not change, and every
+// load is of a point inside the grid.  Most units lie away from the surface:
+// every point of their 4 rows is on the same side.  Per lane, a unit keeps two
+// extremes of its points: one that propagates NaN (min for inside = above the
+// iso-value, max for below: "every point inside" is this extreme inside, and a
+// NaN, which is outside, makes it false) and one that ignores NaN (the other
+// of max / min: "some point inside").  Two warp votes settle such a unit with
+// no bit work.  The others are counted from per-point inside bits, masked to
+// the points and rows that exist.
 constexpr int kCountWarps = 4;
 constexpr int kCountZ = 8;
+constexpr int kCountAhead = 1;  // planes in flight beyond the unit's k + 1
+constexpr int kCountSlots = kCountAhead + 2;
+constexpr unsigned kFull = 0xffffffffu;
+
+// minimum and maximum that give NaN when either operand is NaN
+__device__ __forceinline__ float min_nan(float a, float b) {
+    float d;
+    asm("min.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float max_nan(float a, float b) {
+    float d;
+    asm("max.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+// the extreme for "every point inside" (propagates NaN) and for "some point
+// inside" (ignores NaN)
+template <bool BELOW>
+__device__ __forceinline__ float ext_all(float a, float b) {
+    return BELOW ? max_nan(a, b) : min_nan(a, b);
+}
+template <bool BELOW>
+__device__ __forceinline__ float ext_any(float a, float b) {
+    return BELOW ? fminf(a, b) : fmaxf(a, b);
+}
 
 struct RowVals {
-    float v[5];  // x = i0 + lane + 32 q, and (lane 0) x = i0 + kChunk
-    float lo, hi;  // their minimum and maximum (points that do not exist ignored)
+    float v[4];  // VEC: x = i0 + 4 lane + q; else x = i0 + lane + 32 q
+    float e;     // x = i0 + kChunk
+    float xa, xn;  // the row's two extremes (ext_all, ext_any) at this lane
 };
 
-// The field value as the early-out compares it: NaN (outside) as the side
-// that is never inside.
-template <bool BELOW>
-__device__ __forceinline__ float sided(float x) {
-    return x == x ? x : (BELOW ? INFINITY : -INFINITY);
+__device__ __forceinline__ const float* row_ptr(const float* __restrict__ v, const Grid& g, int j,
+                                                int k) {
+    return v + ((int64_t)min(k, g.nz - 1) * g.ny + j) * g.nx;
 }
 
-// The row's values at this lane's points (the row's pointer is only formed
-// for rows inside the grid); a point that does not exist (ok = false: a
-// missing row) loads as NaN.
+template <bool VEC>
+__device__ __forceinline__ void load_row(const float* __restrict__ row, int i0, int nx, int lane,
+                                         RowVals& r) {
+    if constexpr (VEC) {
+        const float4 q = __ldg(reinterpret_cast<const float4*>(row + min(i0 + 4 * lane, nx - 4)));
+        r.v[0] = q.x;
+        r.v[1] = q.y;
+        r.v[2] = q.z;
+        r.v[3] = q.w;
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; q++) r.v[q] = __ldg(row + min(i0 + lane + 32 * q, nx - 1));
+    }
+    r.e = __ldg(row + min(i0 + kChunk, nx - 1));
+}
+
 template <bool BELOW>
-__device__ __forceinline__ void load_row(const float* __restrict__ v, const Grid& g, int j, int k,
-                                         bool ok, int i0, int lane, RowVals& r) {
-    const float* row = v + ((int64_t)min(k, g.nz - 1) * g.ny + min(j, g.ny - 1)) * g.nx;
+__device__ __forceinline__ void row_ext(RowVals& r) {
+    r.xa = ext_all<BELOW>(ext_all<BELOW>(ext_all<BELOW>(r.v[0], r.v[1]),
+                                         ext_all<BELOW>(r.v[2], r.v[3])), r.e);
+    r.xn = ext_any<BELOW>(ext_any<BELOW>(ext_any<BELOW>(r.v[0], r.v[1]),
+                                         ext_any<BELOW>(r.v[2], r.v[3])), r.e);
+}
+
+// VEC: the inside bits of this lane's points x0 + q (bit q) and of x0 + 4 (bit
+// 4: the next lane's first point, or x = i0 + kChunk for lane 31); 0 for a
+// point past the grid or a missing row (ok = false)
+template <bool BELOW>
+__device__ __forceinline__ uint32_t row_nibble(const RowVals& r, bool ok, int x0, int i0, int nx,
+                                               int lane, float iso) {
+    uint32_t b = 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) b |= (inside<BELOW>(r.v[q], iso) && x0 + q < nx) ? 1u << q : 0u;
+    if (!ok) b = 0;
+    const uint32_t nb = __shfl_down_sync(kFull, b, 1) & 1u;
+    const uint32_t eb = (ok && i0 + kChunk < nx && inside<BELOW>(r.e, iso)) ? 1u : 0u;
+    return b | ((lane == 31 ? eb : nb) << 4);
+}
+
+// scalar layout: ballot words, bit l of w[q] = inside at x = i0 + l + 32 q,
+// w[4] bit 0 = inside at x = i0 + kChunk
+template <bool BELOW>
+__device__ __forceinline__ void row_words(const RowVals& r, bool ok, int i0, int nx, int lane,
+                                          float iso, uint32_t (&w)[5]) {
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         const int x = i0 + lane + 32 * q;
-        r.v[q] = (ok && x < g.nx) ? sided<BELOW>(row[x]) : NAN;
+        w[q] = __ballot_sync(kFull, ok && x < nx && inside<BELOW>(r.v[q], iso));
     }
-    const int x = i0 + kChunk;
-    r.v[4] = (ok && lane == 0 && x < g.nx) ? sided<BELOW>(row[x]) : NAN;
+    w[4] = __ballot_sync(kFull, ok && lane == 0 && i0 + kChunk < nx && inside<BELOW>(r.e, iso));
 }
 
-__device__ __forceinline__ void row_flags(RowVals& r) {
-    r.lo = fminf(fminf(fminf(r.v[0], r.v[1]), fminf(r.v[2], r.v[3])), r.v[4]);
-    r.hi = fmaxf(fmaxf(fmaxf(r.v[0], r.v[1]), fmaxf(r.v[2], r.v[3])), r.v[4]);
-}
-
-template <bool BELOW>
-__device__ __forceinline__ void row_bits(const RowVals& r, bool ok, int i0, int nx, int lane,
-                                         float iso, uint32_t (&w)[5]) {
+// vertices + 2^16 * triangles of a unit the surface may cross (warp-uniform call)
+template <bool BELOW, bool VEC>
+__device__ __forceinline__ uint32_t unit_sum(const RowVals& r0, const RowVals& r1,
+                                             const RowVals& r2, const RowVals& r3, bool has_y,
+                                             bool has_z, int i0, const Grid& g, int lane,
+                                             const uint8_t* __restrict__ ntri) {
+    uint32_t packed = 0;  // this lane's 4 points
+    if constexpr (VEC) {
+        const int x0 = i0 + 4 * lane;
+        const uint32_t e0 = row_nibble<BELOW>(r0, true, x0, i0, g.nx, lane, g.iso);
+        const uint32_t e1 = row_nibble<BELOW>(r1, has_y, x0, i0, g.nx, lane, g.iso);
+        const uint32_t e2 = row_nibble<BELOW>(r2, has_z, x0, i0, g.nx, lane, g.iso);
+        const uint32_t e3 = row_nibble<BELOW>(r3, has_y && has_z, x0, i0, g.nx, lane, g.iso);
+        // points of this lane with a +x neighbour (bit q: x0 + q + 1 < nx)
+        const int room = g.nx - 1 - x0;
+        const uint32_t xm = room >= 4 ? 0xfu : room > 0 ? (1u << room) - 1u : 0u;
+        packed = __popc((e0 ^ (e0 >> 1)) & xm);
+        if (has_y) packed += __popc((e0 ^ e1) & 0xfu);
+        if (has_z) packed += __popc((e0 ^ e2) & 0xfu);
+        if (has_y && has_z) {
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int x = i0 + lane + 32 * q;
-        w[q] = __ballot_sync(0xffffffffu, ok && x < nx && inside<BELOW>(r.v[q], iso));
+            for (int q = 0; q < 4; q++) {
+                const uint32_t cs = ((e0 >> q) & 3u) | (((e1 >> q) & 3u) << 2) |
+                                    (((e2 >> q) & 3u) << 4) | (((e3 >> q) & 3u) << 6);
+                if ((xm >> q) & 1u) packed += (uint32_t)__ldg(&ntri[cs]) << 16;
+            }
+        }
+    } else {
+        uint32_t w0[5], w1[5], w2[5], w3[5];
+        row_words<BELOW>(r0, true, i0, g.nx, lane, g.iso, w0);
+        row_words<BELOW>(r1, has_y, i0, g.nx, lane, g.iso, w1);
+        row_words<BELOW>(r2, has_z, i0, g.nx, lane, g.iso, w2);
+        row_words<BELOW>(r3, has_y && has_z, i0, g.nx, lane, g.iso, w3);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int x = i0 + lane + 32 * q;
+            // bit 0: inside at x, bit 1: inside at x + 1, in rows (dy, dz)
+            const uint32_t b0 = __funnelshift_r(w0[q], w0[q + 1], lane) & 3u;
+            const uint32_t b1 = __funnelshift_r(w1[q], w1[q + 1], lane) & 3u;
+            const uint32_t b2 = __funnelshift_r(w2[q], w2[q + 1], lane) & 3u;
+            const uint32_t b3 = __funnelshift_r(w3[q], w3[q + 1], lane) & 3u;
+            const bool has_x = x + 1 < g.nx;
+            // crossings owned by x (bits past the grid and of missing rows are 0,
+            // so only the +x edge of the last point and the missing rows need masks)
+            packed += (has_x ? ((b0 ^ (b0 >> 1)) & 1u) : 0u) + (has_y ? ((b0 ^ b1) & 1u) : 0u) +
+                      (has_z ? ((b0 ^ b2) & 1u) : 0u);
+            if (has_x && has_y && has_z)
+                packed += (uint32_t)__ldg(&ntri[b0 | (b1 << 2) | (b2 << 4) | (b3 << 6)]) << 16;
+        }
     }
-    const int x = i0 + kChunk;
-    w[4] = __ballot_sync(0xffffffffu, ok && lane == 0 && x < nx && inside<BELOW>(r.v[4], iso));
+    return __reduce_add_sync(kFull, packed);
 }
 
-template <bool BELOW>
+template <bool BELOW, bool VEC>
 __global__ void __launch_bounds__(32 * kCountWarps) k_mc_count(const float* __restrict__ v, Grid g,
                                                                 const uint8_t* __restrict__ ntri,
                                                                 int32_t* __restrict__ vcnt,
@@ -363,66 +465,190 @@ __global__ void __launch_bounds__(32 * kCountWarps) k_mc_count(const float* __re
     const int i0 = (int)blockIdx.x * kChunk;
     const int k0 = (int)blockIdx.z * kCountZ, k1 = min(k0 + kCountZ, g.nz);
     const bool has_y = j + 1 < g.ny;
-    // rows (j, k) and (j+1, k) in slot (k - k0) % 3: the unit's k, its k + 1,
-    // and k + 2 in flight (the loop is unrolled, so slots are registers)
-    RowVals ra[3], rb[3];
-    load_row<BELOW>(v, g, j, k0, true, i0, lane, ra[0]);
-    load_row<BELOW>(v, g, j + 1, k0, has_y, i0, lane, rb[0]);
-    load_row<BELOW>(v, g, j, k0 + 1, k0 + 1 < g.nz, i0, lane, ra[1]);
-    load_row<BELOW>(v, g, j + 1, k0 + 1, has_y && k0 + 1 < g.nz, i0, lane, rb[1]);
-    row_flags(ra[0]);
-    row_flags(rb[0]);
+    const int jb = has_y ? j + 1 : j;
+    // rows (j, k) and (j+1, k) of plane k in slot (k - k0) % kCountSlots (the
+    // loop is unrolled, so slots are registers); planes k0 .. k0 + kCountAhead first
+    RowVals ra[kCountSlots], rb[kCountSlots];
+#pragma unroll
+    for (int p = 0; p <= kCountAhead; p++) {
+        load_row<VEC>(row_ptr(v, g, j, k0 + p), i0, g.nx, lane, ra[p]);
+        load_row<VEC>(row_ptr(v, g, jb, k0 + p), i0, g.nx, lane, rb[p]);
+    }
+    row_ext<BELOW>(ra[0]);
+    row_ext<BELOW>(rb[0]);
 #pragma unroll
     for (int kk = 0; kk < kCountZ; kk++) {
         const int k = k0 + kk;
         if (k >= k1) break;
-        const int s0 = kk % 3, s1 = (kk + 1) % 3, s2 = (kk + 2) % 3;
-        const bool has_z = k + 1 < g.nz;
-        if (kk + 1 < kCountZ && k + 1 < k1) {  // the rows of the next unit's k + 1
-            load_row<BELOW>(v, g, j, k + 2, k + 2 < g.nz, i0, lane, ra[s2]);
-            load_row<BELOW>(v, g, j + 1, k + 2, has_y && k + 2 < g.nz, i0, lane, rb[s2]);
+        const int s0 = kk % kCountSlots, s1 = (kk + 1) % kCountSlots;
+        // the plane the unit kCountAhead further up needs as its k + 1, into the
+        // slot of plane k - 1 (its unit is done)
+        constexpr int kA = kCountAhead + 1;
+        if (kk + kA <= kCountZ && k + kA <= k1) {
+            const int sn = (kk + kA) % kCountSlots;
+            load_row<VEC>(row_ptr(v, g, j, k + kA), i0, g.nx, lane, ra[sn]);
+            load_row<VEC>(row_ptr(v, g, jb, k + kA), i0, g.nx, lane, rb[sn]);
         }
-        row_flags(ra[s1]);
-        row_flags(rb[s1]);
-        // (every lane: NaN extremes, no point, compare false and vote neither way)
-        const float lo = fminf(fminf(ra[s0].lo, rb[s0].lo), fminf(ra[s1].lo, rb[s1].lo));
-        const float hi = fmaxf(fmaxf(ra[s0].hi, rb[s0].hi), fmaxf(ra[s1].hi, rb[s1].hi));
-        const bool lane_all = BELOW ? !(hi >= g.iso) : !(lo <= g.iso);  // every point inside
-        const bool lane_any = BELOW ? lo < g.iso : hi > g.iso;           // some point inside
-        const bool all_in = __all_sync(0xffffffffu, lane_all);
-        const bool any_in = __any_sync(0xffffffffu, lane_any);
+        row_ext<BELOW>(ra[s1]);
+        row_ext<BELOW>(rb[s1]);
+        const float xa = ext_all<BELOW>(ext_all<BELOW>(ra[s0].xa, rb[s0].xa),
+                                        ext_all<BELOW>(ra[s1].xa, rb[s1].xa));
+        const float xn = ext_any<BELOW>(ext_any<BELOW>(ra[s0].xn, rb[s0].xn),
+                                        ext_any<BELOW>(ra[s1].xn, rb[s1].xn));
+        const bool all_in = __all_sync(kFull, inside<BELOW>(xa, g.iso));
+        const bool any_in = __any_sync(kFull, inside<BELOW>(xn, g.iso));
         uint32_t sum = 0;  // vertices + 2^16 * triangles of the unit
-        if (any_in && !all_in) {
-            uint32_t w0[5], w1[5], w2[5], w3[5];
-            row_bits<BELOW>(ra[s0], true, i0, g.nx, lane, g.iso, w0);
-            row_bits<BELOW>(rb[s0], has_y, i0, g.nx, lane, g.iso, w1);
-            row_bits<BELOW>(ra[s1], has_z, i0, g.nx, lane, g.iso, w2);
-            row_bits<BELOW>(rb[s1], has_y && has_z, i0, g.nx, lane, g.iso, w3);
-            uint32_t packed = 0;  // this lane's 4 points
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int x = i0 + lane + 32 * q;
-                // bit 0: inside at x, bit 1: inside at x + 1, in rows (dy, dz)
-                const uint32_t b0 = __funnelshift_r(w0[q], w0[q + 1], lane) & 3u;
-                const uint32_t b1 = __funnelshift_r(w1[q], w1[q + 1], lane) & 3u;
-                const uint32_t b2 = __funnelshift_r(w2[q], w2[q + 1], lane) & 3u;
-                const uint32_t b3 = __funnelshift_r(w3[q], w3[q + 1], lane) & 3u;
-                const bool has_x = x + 1 < g.nx;
-                // crossings owned by x (bits past the grid and of missing rows are 0,
-                // so only the +x edge of the last point and the missing rows need masks)
-                packed += (has_x ? ((b0 ^ (b0 >> 1)) & 1u) : 0u) +
-                          (has_y ? ((b0 ^ b1) & 1u) : 0u) + (has_z ? ((b0 ^ b2) & 1u) : 0u);
-                if (has_x && has_y && has_z)
-                    packed += (uint32_t)__ldg(&ntri[b0 | (b1 << 2) | (b2 << 4) | (b3 << 6)]) << 16;
-            }
-            sum = __reduce_add_sync(0xffffffffu, packed);
-        }
+        if (any_in && !all_in)
+            sum = unit_sum<BELOW, VEC>(ra[s0], rb[s0], ra[s1], rb[s1], has_y, k + 1 < g.nz, i0, g,
+                                       lane, ntri);
         if (lane == 0) {
             const int64_t u = ((int64_t)k * g.ny + j) * g.nchunks + blockIdx.x;
             vcnt[u] = (int32_t)(sum & 0xffffu);
             tcnt[u] = (int32_t)(sum >> 16);
             if (sum != 0u) active[atomicAdd(nactive, 1u)] = (int32_t)u;  // order is free
         }
+    }
+}
+
+// The count pass for rows that start on 16-byte boundaries (nx a multiple of
+// 4), with the rows staged in shared memory by bulk copies.  A block takes one
+// x-tile of kTileChunks units (and the next tile's first 4 points) of the row
+// pair (j, j + 1) for kBulkZ planes: a producer warp copies each plane's two
+// tile rows (one cp.async.bulk per row, completion counted on the slot's full
+// barrier) into a ring of kBulkSlots plane slots, and consumer warp c counts
+// the units of chunk c from the slots as the count kernel above does from its
+// registers (16-byte lane layout, the same clamped points, extremes and bit
+// path).  A consumer copies a plane's values to registers as soon as it has
+// arrived and releases the slot on its empty barrier, so the producer keeps up
+// to kBulkSlots planes in flight per block without holding registers for
+// them.  Every wait is bounded: a wait that runs out sets *err and ends the
+// warp (the producer first waits, bounded again, for its copies in flight).
+constexpr int kTileChunks = 4;                      // consumer warps per block
+constexpr int kTileX = kTileChunks * kChunk + 4;    // floats of a staged tile row
+constexpr int kBulkZ = 16;                          // units per warp, stacked in z
+constexpr int kBulkSlots = 4;                       // planes staged at once
+constexpr uint32_t kBulkSpin = 1u << 22;            // try_wait rounds before a wait gives up
+
+constexpr size_t bulk_smem_bytes() {
+    return sizeof(float) * 2 * kTileX * kBulkSlots + 2 * kBulkSlots * sizeof(uint64_t);
+}
+
+// a row of this lane's values from a staged tile row (off4: the lane's 4
+// points, a multiple of 4; offe: the unit's x = i0 + kChunk, both clamped to the
+// staged points)
+__device__ __forceinline__ void load_srow(const float* srow, int off4, int offe, RowVals& r) {
+    const float4 q = *reinterpret_cast<const float4*>(srow + off4);
+    r.v[0] = q.x;
+    r.v[1] = q.y;
+    r.v[2] = q.z;
+    r.v[3] = q.w;
+    r.e = srow[offe];
+}
+
+// plane p's two rows (row ry stands for row j + 1) into registers once the
+// plane has arrived, then the slot is released; false when the wait ran out
+__device__ __forceinline__ bool take_plane(const float* stage, uint64_t* full, uint64_t* empty,
+                                           int p, int ry, int off4, int offe, int lane,
+                                           RowVals& a, RowVals& b) {
+    const int s = p % kBulkSlots;
+    if (!mbar_wait(full + s, (uint32_t)(p / kBulkSlots) & 1u, kBulkSpin)) return false;
+    load_srow(stage + (size_t)(2 * s) * kTileX, off4, offe, a);
+    load_srow(stage + (size_t)(2 * s + ry) * kTileX, off4, offe, b);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(empty + s);
+    return true;
+}
+
+template <bool BELOW>
+__global__ void __launch_bounds__(32 * (kTileChunks + 1), 8) k_mc_count_bulk(
+    const float* __restrict__ v, Grid g, const uint8_t* __restrict__ ntri,
+    int32_t* __restrict__ vcnt, int32_t* __restrict__ tcnt, int32_t* __restrict__ active,
+    uint32_t* __restrict__ nactive, uint32_t* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char dsm[];
+    float* stage = reinterpret_cast<float*>(dsm);  // slot s, row r: stage + (2 s + r) kTileX
+    uint64_t* full = reinterpret_cast<uint64_t*>(dsm + sizeof(float) * 2 * kTileX * kBulkSlots);
+    uint64_t* empty = full + kBulkSlots;
+    const int warp = (int)threadIdx.x >> 5, lane = (int)threadIdx.x & 31;
+    const int x0 = (int)blockIdx.x * (kTileChunks * kChunk);
+    const int j = (int)blockIdx.y;
+    const int k0 = (int)blockIdx.z * kBulkZ, k1 = min(k0 + kBulkZ, g.nz);
+    const int nvalid = min(kTileX, g.nx - x0);                           // staged floats per row
+    const int nw = min(kTileChunks, (g.nx - x0 + kChunk - 1) / kChunk);  // chunks in the tile
+    const bool has_y = j + 1 < g.ny;
+    const int nplanes = k1 - k0 + 1;  // planes k0 .. k1 (k1 = nz: the last plane again)
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kBulkSlots; s++) {
+            mbar_init(full + s, 1);
+            mbar_init(empty + s, (uint32_t)nw);
+        }
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (warp == kTileChunks) {  // the producer
+        if (lane != 0) return;
+        const uint32_t bytes = (uint32_t)nvalid * 4u;
+        int issued = 0;
+        bool ok = true;
+        for (int p = 0; p < nplanes; p++) {
+            const int s = p % kBulkSlots;
+            // the slot's previous plane released by every consumer
+            if (p >= kBulkSlots && !mbar_wait(empty + s, (uint32_t)((p / kBulkSlots) - 1) & 1u,
+                                             kBulkSpin)) {
+                ok = false;
+                break;
+            }
+            const float* src = v + ((int64_t)min(k0 + p, g.nz - 1) * g.ny + j) * g.nx + x0;
+            float* dst = stage + (size_t)(2 * s) * kTileX;
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(full + s, has_y ? 2u * bytes : bytes);
+            bulk_copy_g2s(dst, src, bytes, full + s);
+            if (has_y) bulk_copy_g2s(dst + kTileX, src + g.nx, bytes, full + s);
+            issued = p + 1;
+        }
+        if (!ok) {
+            atomicOr(err, 1u);
+            // the copies still in flight: the last plane issued into each slot
+            for (int p = max(0, issued - kBulkSlots); p < issued; p++)
+                mbar_wait(full + p % kBulkSlots, (uint32_t)(p / kBulkSlots) & 1u, kBulkSpin);
+        }
+        return;
+    }
+    if (warp >= nw) return;  // no chunk of the grid (its barriers count nw consumers)
+    const int lx = warp * kChunk;  // the chunk's offset in the tile
+    const int i0 = x0 + lx;
+    const int64_t chunk = (int64_t)blockIdx.x * kTileChunks + warp;
+    const int off4 = min(lx + 4 * lane, nvalid - 4), offe = min(lx + kChunk, nvalid - 1);
+    const int ry = has_y ? 1 : 0;  // a missing row j + 1 is read as row j
+    RowVals ra0, rb0;
+    if (!take_plane(stage, full, empty, 0, ry, off4, offe, lane, ra0, rb0)) {
+        if (lane == 0) atomicOr(err, 1u);
+        return;
+    }
+    row_ext<BELOW>(ra0);
+    row_ext<BELOW>(rb0);
+    for (int k = k0; k < k1; k++) {
+        RowVals ra1, rb1;
+        if (!take_plane(stage, full, empty, k - k0 + 1, ry, off4, offe, lane, ra1, rb1)) {
+            if (lane == 0) atomicOr(err, 1u);
+            return;
+        }
+        row_ext<BELOW>(ra1);
+        row_ext<BELOW>(rb1);
+        const float xa = ext_all<BELOW>(ext_all<BELOW>(ra0.xa, rb0.xa), ext_all<BELOW>(ra1.xa, rb1.xa));
+        const float xn = ext_any<BELOW>(ext_any<BELOW>(ra0.xn, rb0.xn), ext_any<BELOW>(ra1.xn, rb1.xn));
+        const bool all_in = __all_sync(kFull, inside<BELOW>(xa, g.iso));
+        const bool any_in = __any_sync(kFull, inside<BELOW>(xn, g.iso));
+        uint32_t sum = 0;  // vertices + 2^16 * triangles of the unit
+        if (any_in && !all_in)
+            sum = unit_sum<BELOW, true>(ra0, rb0, ra1, rb1, has_y, k + 1 < g.nz, i0, g, lane, ntri);
+        if (lane == 0) {
+            const int64_t u = ((int64_t)k * g.ny + j) * g.nchunks + chunk;
+            vcnt[u] = (int32_t)(sum & 0xffffu);
+            tcnt[u] = (int32_t)(sum >> 16);
+            if (sum != 0u) active[atomicAdd(nactive, 1u)] = (int32_t)u;  // order is free
+        }
+        ra0 = ra1;
+        rb0 = rb1;
     }
 }
 
@@ -439,7 +665,15 @@ __global__ void __launch_bounds__(32 * kCountWarps) k_mc_count(const float* __re
 // points' edge mask and in-unit vertex prefix to per-warp shared memory; a
 // triangle's vertex is then that point's unit base + prefix + the edge's rank
 // among the point's crossed edges (the next unit's base for x = i0 + 128).
+// The output is written from two lists in per-warp shared memory, so that the
+// work is spread over the lanes whichever cells the surface crosses: the
+// unit's vertices (point, axis) in vertex order, and its triangles (cell,
+// case, triangle of the case) in triangle order.  Lane l takes entries l,
+// l + 32, ...: a vertex each, and of the triangles a face's vertex id each
+// (3 per triangle), so consecutive lanes write consecutive words.
 constexpr int kEmitWarps = 4;
+constexpr int kUnitVerts = 3 * kChunk;          // a point owns at most 3 edges
+constexpr int kUnitTris = kCellTris * kChunk;  // a cell has at most kCellTris triangles
 
 template <bool BELOW>
 __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __restrict__ v, Grid g,
@@ -452,18 +686,27 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
                                                               float* __restrict__ verts,
                                                               int32_t* __restrict__ faces,
                                                               int64_t max_verts, int64_t max_faces) {
-    __shared__ uint8_t s_m[kEmitWarps][4][kChunk + 1];     // crossed edges (bit a: +axis a)
-    __shared__ uint16_t s_pre[kEmitWarps][4][kChunk];      // in-unit vertex prefix
-    __shared__ int64_t s_base[kEmitWarps][8];              // R: unit base; 4 + R: next unit's
-    __shared__ int8_t s_tri[256 * 3 * kMaxTri];            // the case table, per block
+    __shared__ uint8_t s_m[kEmitWarps][4][kChunk + 1];  // crossed edges (bit a: +axis a)
+    __shared__ uint16_t s_pre[kEmitWarps][4][kChunk];   // in-unit vertex prefix
+    __shared__ float s_val[kEmitWarps][3][kChunk + 1];  // point row 0 (with x = i0 + 128),
+                                                        // rows 1 (+y) and 2 (+z)
+    __shared__ uint16_t s_vl[kEmitWarps][kUnitVerts];   // vertices: point | axis << 8
+    __shared__ uint32_t s_tl[kEmitWarps][kUnitTris];    // triangles: cell | t << 7 | case << 10
+    __shared__ int64_t s_base[kEmitWarps][8];           // R: unit base; 4 + R: next unit's
+    __shared__ int8_t s_tri[256 * 3 * kCellTris];       // the case table, per block
     __shared__ uint8_t s_ntri[256];
-    for (int i = (int)threadIdx.x; i < 256 * 3 * kMaxTri; i += 32 * kEmitWarps) s_tri[i] = tri[i];
+    for (int i = (int)threadIdx.x; i < 256 * 3 * kCellTris; i += 32 * kEmitWarps)
+        s_tri[i] = tri[(i / (3 * kCellTris)) * 3 * kMaxTri + i % (3 * kCellTris)];
     for (int i = (int)threadIdx.x; i < 256; i += 32 * kEmitWarps) s_ntri[i] = ntri[i];
     __syncthreads();
     const int lane = (int)threadIdx.x & 31, wid = (int)threadIdx.x >> 5;
     const uint32_t n_act = *nactive;
-    for (uint32_t a = blockIdx.x * kEmitWarps + wid; a < n_act; a += gridDim.x * kEmitWarps) {
-        const int64_t u = active[a];
+    const uint32_t stride = gridDim.x * kEmitWarps;
+    uint32_t a = blockIdx.x * kEmitWarps + wid;
+    int64_t u_next = a < n_act ? active[a] : 0;  // the warp's next unit, read a unit ahead
+    for (; a < n_act; a += stride) {
+        const int64_t u = u_next;
+        if (a + stride < n_act) u_next = active[a + stride];
         const int chunk = (int)(u % g.nchunks);
         const int64_t rowid = u / g.nchunks;
         const int j = (int)(rowid % g.ny), k = (int)(rowid / g.ny);
@@ -483,7 +726,6 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
         // 6, 7 = (0, 2), (1, 2)
         constexpr int kDy[8] = {0, 1, 0, 1, 2, 2, 0, 1}, kDz[8] = {0, 0, 1, 1, 0, 1, 2, 2};
         uint32_t w[8][5];
-        float val[3][5];  // raw values of point rows 0, 1, 2 (the vertex roots)
 #pragma unroll
         for (int r = 0; r < 8; r++) {
             const int jj = j + kDy[r], kz = k + kDz[r];
@@ -500,19 +742,21 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const int x = i0 + lane + 32 * q;
-                w[r][q] = __ballot_sync(0xffffffffu, ok && x < g.nx && inside<BELOW>(x5[q], g.iso));
+                w[r][q] = __ballot_sync(kFull, ok && x < g.nx && inside<BELOW>(x5[q], g.iso));
             }
-            w[r][4] = __ballot_sync(0xffffffffu,
-                                    ok && lane < 2 && xe < g.nx && inside<BELOW>(x5[4], g.iso));
-            if (r < 3)
+            w[r][4] = __ballot_sync(kFull, ok && lane < 2 && xe < g.nx && inside<BELOW>(x5[4], g.iso));
+            if (r < 3) {  // the values the unit's vertices interpolate
 #pragma unroll
-                for (int q = 0; q < 5; q++) val[r][q] = x5[q];
+                for (int q = 0; q < 4; q++) s_val[wid][r][lane + 32 * q] = x5[q];
+                if (r == 0 && lane == 0) s_val[wid][0][kChunk] = x5[4];
+            }
         }
-        // per point row: crossed-edge words, each lane's points' masks and prefixes
+        // per point row: crossed-edge words, each lane's points' masks and prefixes;
+        // row 0's crossed edges are the unit's vertices, listed in vertex order
         const bool row_ok[4] = {true, j + 1 < g.ny, k + 1 < g.nz, j + 1 < g.ny && k + 1 < g.nz};
         const int ny_of[4] = {1, 4, 3, 5};  // the row one step +y of point row R
         const int nz_of[4] = {2, 3, 6, 7};  // the row one step +z of point row R
-        uint32_t m0[4];  // this lane's points' crossed edges in row 0
+        uint32_t nverts = 0;
 #pragma unroll
         for (int R = 0; R < 4; R++) {
             const int dy = R & 1, dz = R >> 1;
@@ -523,21 +767,28 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
             for (int q = 0; q < 4; q++) {
                 const int xl = g.nx - 1 - (i0 + 32 * q);  // bits whose point has x + 1 < nx
                 const uint32_t X = (w[R][q] ^ __funnelshift_r(w[R][q], w[R][q + 1], 1)) &
-                                   (xl >= 32 ? 0xffffffffu : (xl <= 0 ? 0u : (1u << xl) - 1u));
+                                   (xl >= 32 ? kFull : (xl <= 0 ? 0u : (1u << xl) - 1u));
                 const uint32_t Y = yok ? (w[R][q] ^ w[ny_of[R]][q]) : 0u;
                 const uint32_t Z = zok ? (w[R][q] ^ w[nz_of[R]][q]) : 0u;
                 const uint32_t lo = (1u << lane) - 1u;
                 const uint32_t m = ((X >> lane) & 1u) | (((Y >> lane) & 1u) << 1) |
                                    (((Z >> lane) & 1u) << 2);
-                if (R == 0) m0[q] = m;
                 // (a word without crossings owns no vertex: no triangle reads its entries)
                 if ((X | Y | Z) != 0u) {
+                    const uint32_t pre = cum + __popc(X & lo) + __popc(Y & lo) + __popc(Z & lo);
                     s_m[wid][R][lane + 32 * q] = (uint8_t)m;
-                    s_pre[wid][R][lane + 32 * q] =
-                        (uint16_t)(cum + __popc(X & lo) + __popc(Y & lo) + __popc(Z & lo));
+                    s_pre[wid][R][lane + 32 * q] = (uint16_t)pre;
+                    if (R == 0) {
+                        uint32_t o = pre;
+#pragma unroll
+                        for (int ax = 0; ax < 3; ax++)
+                            if ((m >> ax) & 1u)
+                                s_vl[wid][o++] = (uint16_t)((lane + 32 * q) | (ax << 8));
+                    }
                     cum += __popc(X) + __popc(Y) + __popc(Z);
                 }
             }
+            if (R == 0) nverts = cum;
             if (lane == R) {  // the next unit's first point, x = i0 + 128, in this row
                 const int x = i0 + kChunk;
                 uint32_t m = 0;
@@ -551,41 +802,9 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
             }
         }
         if (lane < 8) s_base[wid][lane] = base;
-        const int64_t tb = __shfl_sync(0xffffffffu, base, 8);
-        __syncwarp();
-        // vertices of this unit's points (row 0)
-        const int64_t vb = s_base[wid][0];
-        float vx1[4];  // the +x neighbours: the next lane's value (lane 31: lane 0's of
-                       // the next word, or the next unit's first point)
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const float wrap = __shfl_sync(0xffffffffu, q < 3 ? val[0][q + 1] : val[0][4], 0);
-            const float down = __shfl_down_sync(0xffffffffu, val[0][q], 1);
-            vx1[q] = lane == 31 ? wrap : down;
-        }
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const uint32_t m = m0[q];
-            if (!m) continue;
-            const int i = i0 + lane + 32 * q;
-            const float x = __fmaf_rn(float(i), g.h, g.ox), y = __fmaf_rn(float(j), g.h, g.oy),
-                        z = __fmaf_rn(float(k), g.h, g.oz);
-            const float v0 = val[0][q];
-            const float nbr[3] = {vx1[q], val[1][q], val[2][q]};
-            int64_t o = vb + s_pre[wid][0][lane + 32 * q];
-#pragma unroll
-            for (int ax = 0; ax < 3; ax++) {
-                if (!((m >> ax) & 1u)) continue;
-                const float d = __fmul_rn(root_t(v0, nbr[ax], g.iso), g.h);
-                if (o < max_verts) {  // the host reports a mesh larger than the buffers
-                    verts[3 * o + 0] = ax == 0 ? __fadd_rn(x, d) : x;
-                    verts[3 * o + 1] = ax == 1 ? __fadd_rn(y, d) : y;
-                    verts[3 * o + 2] = ax == 2 ? __fadd_rn(z, d) : z;
-                }
-                o++;
-            }
-        }
-        // triangles of this unit's cells, in x order
+        const int64_t tb = __shfl_sync(kFull, base, 8);
+        // the triangles of this unit's cells, listed in x order
+        uint32_t ntris = 0;
         if (j + 1 < g.ny && k + 1 < g.nz) {
             // the 4 words' cases and counts, then their 4 scans side by side
             int cs[4], nt[4], incl[4];
@@ -607,34 +826,56 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
             for (int o = 1; o < 32; o <<= 1) {  // warp inclusive scans of the counts
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
-                    const int t = __shfl_up_sync(0xffffffffu, incl[q], o);
+                    const int t = __shfl_up_sync(kFull, incl[q], o);
                     if (lane >= o) incl[q] += t;
                 }
             }
-            int64_t fo = tb;
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                const int64_t first = fo + (incl[q] - nt[q]);
-                fo += __shfl_sync(0xffffffffu, incl[q], 31);
-                for (int t3 = 0; t3 < nt[q]; t3++) {
-#pragma unroll
-                    for (int sv = 0; sv < 3; sv++) {
-                        const int e = s_tri[cs[q] * 3 * kMaxTri + 3 * t3 + sv];
-                        const int ax = e >> 2, eu = e & 1, ew = (e >> 1) & 1;
-                        // the point owning edge e of this cell: (dx, row R = dy + 2 dz)
-                        const int dx = ax == 0 ? 0 : eu;
-                        const int dy = ax == 0 ? eu : (ax == 1 ? 0 : ew);
-                        const int dz = ax == 2 ? 0 : ew;
-                        const int R = dy + 2 * dz, xi = lane + 32 * q + dx;
-                        const uint32_t below = (1u << ax) - 1u;
-                        const int64_t id =
-                            xi < kChunk ? s_base[wid][R] + s_pre[wid][R][xi] +
-                                              __popc(s_m[wid][R][xi] & below)
-                                        : s_base[wid][4 + R] + __popc(s_m[wid][R][kChunk] & below);
-                        if (first + t3 < max_faces) faces[3 * (first + t3) + sv] = (int32_t)id;
-                    }
+                const uint32_t first = ntris + (uint32_t)(incl[q] - nt[q]);
+                for (int t3 = 0; t3 < nt[q]; t3++)
+                    s_tl[wid][first + t3] =
+                        (uint32_t)(lane + 32 * q) | ((uint32_t)t3 << 7) | ((uint32_t)cs[q] << 10);
+                ntris += (uint32_t)__shfl_sync(kFull, incl[q], 31);
+            }
+        }
+        __syncwarp();
+        // vertices
+        {
+            const int64_t vb = s_base[wid][0];
+            const float y = __fmaf_rn(float(j), g.h, g.oy), z = __fmaf_rn(float(k), g.h, g.oz);
+            for (uint32_t e = lane; e < nverts; e += 32) {
+                const uint32_t ent = s_vl[wid][e];
+                const int xi = (int)(ent & 0xffu), ax = (int)(ent >> 8);
+                const float v0 = s_val[wid][0][xi];
+                const float v1 = ax == 0 ? s_val[wid][0][xi + 1] : s_val[wid][ax][xi];
+                const float x = __fmaf_rn(float(i0 + xi), g.h, g.ox);
+                const float d = __fmul_rn(root_t(v0, v1, g.iso), g.h);
+                const int64_t o = vb + e;
+                if (o < max_verts) {  // the host reports a mesh larger than the buffers
+                    verts[3 * o + 0] = ax == 0 ? __fadd_rn(x, d) : x;
+                    verts[3 * o + 1] = ax == 1 ? __fadd_rn(y, d) : y;
+                    verts[3 * o + 2] = ax == 2 ? __fadd_rn(z, d) : z;
                 }
             }
+        }
+        // faces: entry e is vertex e % 3 of the unit's triangle e / 3
+        for (uint32_t e = lane; e < 3 * ntris; e += 32) {
+            const uint32_t t = e / 3, sv = e - 3 * t;
+            const uint32_t ent = s_tl[wid][t];
+            const int xc = (int)(ent & 127u), t3 = (int)((ent >> 7) & 7u), c = (int)(ent >> 10);
+            const int ed = s_tri[c * 3 * kCellTris + 3 * t3 + (int)sv];
+            const int ax = ed >> 2, eu = ed & 1, ew = (ed >> 1) & 1;
+            // the point owning edge ed of this cell: (dx, row R = dy + 2 dz)
+            const int dx = ax == 0 ? 0 : eu;
+            const int dy = ax == 0 ? eu : (ax == 1 ? 0 : ew);
+            const int dz = ax == 2 ? 0 : ew;
+            const int R = dy + 2 * dz, xi = xc + dx;
+            const uint32_t below = (1u << ax) - 1u;
+            const int64_t id = xi < kChunk ? s_base[wid][R] + s_pre[wid][R][xi] +
+                                                 __popc(s_m[wid][R][xi] & below)
+                                           : s_base[wid][4 + R] + __popc(s_m[wid][R][kChunk] & below);
+            if (tb + (int64_t)t < max_faces) faces[3 * tb + e] = (int32_t)id;
         }
         __syncwarp();  // the shared rows are rewritten by the warp's next unit
     }
@@ -708,7 +949,7 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
     };
     int rc = pool_alloc((void**)&vcnt, 4 * (U + 1), s);
     if (!rc) rc = pool_alloc((void**)&act, 4 * U, s);  // units with output, any order
-    if (!rc) rc = pool_alloc((void**)&nact, 4, s);
+    if (!rc) rc = pool_alloc((void**)&nact, 8, s);  // listed units, then the error flag
     if (!rc) rc = pool_alloc((void**)&tcnt, 4 * (U + 1), s);
     if (!rc) rc = pool_alloc((void**)&vbase, 8 * (U + 1), s);
     if (!rc) rc = pool_alloc((void**)&tbase, 8 * (U + 1), s);
@@ -737,13 +978,24 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
     const bool below = ref_table != nullptr;
     cudaMemsetAsync(vcnt + U, 0, 4, s);
     cudaMemsetAsync(tcnt + U, 0, 4, s);
-    cudaMemsetAsync(nact, 0, 4, s);
-    if (below)
-        k_mc_count<true><<<grid_c, 32 * kCountWarps, 0, s>>>(values, g, ntri, vcnt, tcnt, act,
-                                                              nact);
+    cudaMemsetAsync(nact, 0, 8, s);
+    uint32_t* nerr = nact + 1;
+    // rows staged by bulk copies when every row starts on a 16-byte boundary
+    const bool vec = nx % 4 == 0 && ((uintptr_t)values & 15u) == 0;
+    const dim3 grid_b((unsigned)((nx + kTileChunks * kChunk - 1) / (kTileChunks * kChunk)),
+                      (unsigned)ny, (unsigned)((nz + kBulkZ - 1) / kBulkZ));
+    if (below && vec)
+        k_mc_count_bulk<true><<<grid_b, 32 * (kTileChunks + 1), bulk_smem_bytes(), s>>>(
+            values, g, ntri, vcnt, tcnt, act, nact, nerr);
+    else if (vec)
+        k_mc_count_bulk<false><<<grid_b, 32 * (kTileChunks + 1), bulk_smem_bytes(), s>>>(
+            values, g, ntri, vcnt, tcnt, act, nact, nerr);
+    else if (below)
+        k_mc_count<true, false><<<grid_c, 32 * kCountWarps, 0, s>>>(values, g, ntri, vcnt, tcnt,
+                                                                     act, nact);
     else
-        k_mc_count<false><<<grid_c, 32 * kCountWarps, 0, s>>>(values, g, ntri, vcnt, tcnt, act,
-                                                               nact);
+        k_mc_count<false, false><<<grid_c, 32 * kCountWarps, 0, s>>>(values, g, ntri, vcnt, tcnt,
+                                                                      act, nact);
     rc = cub_scan([&](void* t, size_t& b) {
         return cub::DeviceScan::ExclusiveSum(t, b, vcnt, vbase, U + 1, s);
     }, s);
@@ -766,11 +1018,14 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
         if (cudaGetLastError() != cudaSuccess) rc = set_error(kErrCuda, "marching cubes launch");
     }
     int64_t nv = 0, nf = 0;
+    uint32_t herr = 0;
     if (!rc) {
         cudaMemcpyAsync(&nv, vbase + U, 8, cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(&nf, tbase + U, 8, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&herr, nerr, 4, cudaMemcpyDeviceToHost, s);
         if (cudaStreamSynchronize(s) != cudaSuccess) rc = set_error(kErrCuda, "marching cubes counts");
     }
+    if (!rc && herr) rc = set_error(kErrCuda, "marching cubes: a staging wait ran out");
     if (!rc && nv > INT32_MAX) rc = set_error(kErrOverflow, "more than 2^31 - 1 vertices");
     if (!rc) {
         *nverts = nv;

@@ -174,3 +174,38 @@ def test_reference_table_mode_rejects_a_bad_table(cuda_lib):
     vals = torch.zeros(4, 4, 4, device="cuda")
     with pytest.raises(RuntimeError, match="not an edge the case crosses"):
         marching_cubes(vals, (0, 0, 0), 1.0, 0.5, table=tri)
+
+
+@pytest.mark.parametrize("table_mode", [False, True])
+@pytest.mark.parametrize("shape", [(6, 7, 256), (4, 3, 260), (5, 9, 133), (7, 6, 129)])
+def test_non_finite_values_bit_exact_against_oracle(cuda_lib, oracle, shape, table_mode):
+    """NaN (outside in both modes), +inf, -inf and values exactly at the
+    iso-value in the field: vertices and triangles equal the oracle's bit for
+    bit (NaN positions where an edge has a NaN end), for rows whose length is
+    a multiple of 4 (16-byte row loads; 260: a last unit of 4 points) and rows
+    that are not (133, 129: a last unit of 5 points and of 1)."""
+    import os
+    import torch
+    from cagr_b200.mesh import marching_cubes, mc_table
+    rng = np.random.default_rng(54)
+    nz, ny, nx = shape
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    vals = (np.sin(0.3 * x) + np.cos(0.5 * y) * np.sin(0.7 * z)).astype(np.float32)
+    u = rng.random(shape)
+    vals[u < 0.03] = np.nan
+    vals[(u >= 0.03) & (u < 0.04)] = np.inf
+    vals[(u >= 0.04) & (u < 0.05)] = -np.inf
+    vals[(u >= 0.05) & (u < 0.07)] = 0.125
+    vals[:, :, : nx // 3][rng.random((nz, ny, nx // 3)) < 0.5] = np.nan  # stretches of NaN
+    org, h, iso = (0.5, -0.25, 1.0), 0.0625, 0.125
+    if table_mode:
+        tri = np.load(os.path.join(os.path.dirname(__file__), "golden",
+                                   "mc_reference_tables.npz"))["triangles"]
+        v_gpu, f_gpu = marching_cubes(torch.from_numpy(vals).cuda(), org, h, iso, table=tri)
+        v_ref, f_ref = oracle.marching_cubes_reftable(vals, org, h, iso, tri)
+    else:
+        v_gpu, f_gpu = marching_cubes(torch.from_numpy(vals).cuda(), org, h, iso)
+        v_ref, f_ref = oracle.marching_cubes(vals, org, h, iso, *mc_table())
+    assert len(f_ref) > 100 and np.isnan(v_ref).any()
+    assert np.array_equal(f_gpu.cpu().numpy(), f_ref)
+    assert np.array_equal(v_gpu.cpu().numpy(), v_ref, equal_nan=True)
