@@ -668,15 +668,16 @@ __global__ void __launch_bounds__(32 * (kTileChunks + 1), 8) k_mc_count_bulk(
 // The output is written from two lists in per-warp shared memory, so that the
 // work is spread over the lanes whichever cells the surface crosses: the
 // unit's vertices (point, axis) in vertex order, and its triangles (cell,
-// case, triangle of the case) in triangle order.  Lane l takes entries l,
+// triangle of the cell's case) in triangle order, with each cell's case.  Lane l takes entries l,
 // l + 32, ...: a vertex each, and of the triangles a face's vertex id each
 // (3 per triangle), so consecutive lanes write consecutive words.
 constexpr int kEmitWarps = 4;
+constexpr int kEmitBlocksPerSM = 8;              // resident blocks the launch bound asks for
 constexpr int kUnitVerts = 3 * kChunk;          // a point owns at most 3 edges
 constexpr int kUnitTris = kCellTris * kChunk;  // a cell has at most kCellTris triangles
 
 template <bool BELOW>
-__global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __restrict__ v, Grid g,
+__global__ void __launch_bounds__(32 * kEmitWarps, kEmitBlocksPerSM) k_mc_emit(const float* __restrict__ v, Grid g,
                                                               const int8_t* __restrict__ tri,
                                                               const uint8_t* __restrict__ ntri,
                                                               const int64_t* __restrict__ vbase,
@@ -691,8 +692,10 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
     __shared__ float s_val[kEmitWarps][3][kChunk + 1];  // point row 0 (with x = i0 + 128),
                                                         // rows 1 (+y) and 2 (+z)
     __shared__ uint16_t s_vl[kEmitWarps][kUnitVerts];   // vertices: point | axis << 8
-    __shared__ uint32_t s_tl[kEmitWarps][kUnitTris];    // triangles: cell | t << 7 | case << 10
+    __shared__ uint16_t s_tl[kEmitWarps][kUnitTris];    // triangles: cell | t << 7
+    __shared__ uint8_t s_case[kEmitWarps][kChunk];      // each cell's case
     __shared__ int64_t s_base[kEmitWarps][8];           // R: unit base; 4 + R: next unit's
+    __shared__ uint32_t s_w[kEmitWarps][8][5];          // the rows' inside-bit words
     __shared__ int8_t s_tri[256 * 3 * kCellTris];       // the case table, per block
     __shared__ uint8_t s_ntri[256];
     for (int i = (int)threadIdx.x; i < 256 * 3 * kCellTris; i += 32 * kEmitWarps)
@@ -725,7 +728,9 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
         // rows: 0..3 = point rows (dy, dz) = (R & 1, R >> 1); 4, 5 = (2, 0), (2, 1);
         // 6, 7 = (0, 2), (1, 2)
         constexpr int kDy[8] = {0, 1, 0, 1, 2, 2, 0, 1}, kDz[8] = {0, 0, 1, 1, 0, 1, 2, 2};
-        uint32_t w[8][5];
+        // (the words go to shared memory: every lane reads them as broadcasts, and
+        // the registers they would hold go to more resident warps)
+        uint32_t(&w)[8][5] = s_w[wid];
 #pragma unroll
         for (int r = 0; r < 8; r++) {
             const int jj = j + kDy[r], kz = k + kDz[r];
@@ -742,15 +747,20 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const int x = i0 + lane + 32 * q;
-                w[r][q] = __ballot_sync(kFull, ok && x < g.nx && inside<BELOW>(x5[q], g.iso));
+                const uint32_t b =
+                    __ballot_sync(kFull, ok && x < g.nx && inside<BELOW>(x5[q], g.iso));
+                if (lane == 0) w[r][q] = b;
             }
-            w[r][4] = __ballot_sync(kFull, ok && lane < 2 && xe < g.nx && inside<BELOW>(x5[4], g.iso));
+            const uint32_t b4 =
+                __ballot_sync(kFull, ok && lane < 2 && xe < g.nx && inside<BELOW>(x5[4], g.iso));
+            if (lane == 0) w[r][4] = b4;
             if (r < 3) {  // the values the unit's vertices interpolate
 #pragma unroll
                 for (int q = 0; q < 4; q++) s_val[wid][r][lane + 32 * q] = x5[q];
                 if (r == 0 && lane == 0) s_val[wid][0][kChunk] = x5[4];
             }
         }
+        __syncwarp();
         // per point row: crossed-edge words, each lane's points' masks and prefixes;
         // row 0's crossed edges are the unit's vertices, listed in vertex order
         const bool row_ok[4] = {true, j + 1 < g.ny, k + 1 < g.nz, j + 1 < g.ny && k + 1 < g.nz};
@@ -820,6 +830,7 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
                             (int)((__funnelshift_r(w[R][q], w[R][q + 1], lane) & 3u) << (2 * R));
                     nt[q] = s_ntri[cs[q]];
                 }
+                if (nt[q]) s_case[wid][lane + 32 * q] = (uint8_t)cs[q];
                 incl[q] = nt[q];
             }
 #pragma unroll
@@ -834,8 +845,7 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
             for (int q = 0; q < 4; q++) {
                 const uint32_t first = ntris + (uint32_t)(incl[q] - nt[q]);
                 for (int t3 = 0; t3 < nt[q]; t3++)
-                    s_tl[wid][first + t3] =
-                        (uint32_t)(lane + 32 * q) | ((uint32_t)t3 << 7) | ((uint32_t)cs[q] << 10);
+                    s_tl[wid][first + t3] = (uint16_t)((lane + 32 * q) | (t3 << 7));
                 ntris += (uint32_t)__shfl_sync(kFull, incl[q], 31);
             }
         }
@@ -863,7 +873,7 @@ __global__ void __launch_bounds__(32 * kEmitWarps, 5) k_mc_emit(const float* __r
         for (uint32_t e = lane; e < 3 * ntris; e += 32) {
             const uint32_t t = e / 3, sv = e - 3 * t;
             const uint32_t ent = s_tl[wid][t];
-            const int xc = (int)(ent & 127u), t3 = (int)((ent >> 7) & 7u), c = (int)(ent >> 10);
+            const int xc = (int)(ent & 127u), t3 = (int)(ent >> 7), c = s_case[wid][xc];
             const int ed = s_tri[c * 3 * kCellTris + 3 * t3 + (int)sv];
             const int ax = ed >> 2, eu = ed & 1, ew = (ed >> 1) & 1;
             // the point owning edge ed of this cell: (dx, row R = dy + 2 dz)
@@ -930,10 +940,13 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
     // k / kCountZ); emit: a persistent grid whose warps take the listed units
     if (ny > 65535 || nz > 65535)
         return set_error(kErrInvalid, "marching cubes needs ny, nz <= 65535");
+    int dev = 0, sms = 0;
+    CAGR_CUDA(cudaGetDevice(&dev));
+    CAGR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const dim3 grid_c((unsigned)nchunks, (unsigned)((ny + kCountWarps - 1) / kCountWarps),
                       (unsigned)((nz + kCountZ - 1) / kCountZ)),
-        grid_e(148u * 5u);  // persistent (5 blocks per SM): warps stride over the
-                            // listed units
+        grid_e((unsigned)(sms * kEmitBlocksPerSM));  // persistent: warps stride over the
+                                                     // listed units
     int32_t *vcnt = nullptr, *tcnt = nullptr, *act = nullptr;
     uint32_t* nact = nullptr;
     int64_t *vbase = nullptr, *tbase = nullptr;
