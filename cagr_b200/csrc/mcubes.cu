@@ -287,15 +287,16 @@ __device__ __forceinline__ float root_t(float v0, float v1, float iso) {
 // so per-unit counts scanned give each unit's first vertex and triangle.
 
 // per unit: vertices (crossed edges owned by its points), triangles (its cells).
+// This kernel takes rows that need not start on a 16-byte boundary; rows that
+// do go to k_mc_count_bulk below, which shares its per-unit steps.
 // A warp takes kCountZ units stacked along z at one (chunk, j), kCountWarps
 // warps per block at consecutive j.  A unit needs the point rows (j, k),
 // (j+1, k), (j, k+1), (j+1, k+1); walking up in k, the k+1 rows of one unit are
 // the k rows of the next, so each unit reads two new rows, and the rows of the
 // next kCountAhead units are in flight while one is counted (their latency
-// overlaps the work).  VEC (rows 16-byte aligned: nx a multiple of 4): lane l
-// holds x = i0 + 4 l + q (q < 4) from one 16-byte load; otherwise lane l holds
-// x = i0 + l + 32 q (coalesced scalar loads).  Every lane also holds
-// x = i0 + kChunk (the next unit's first point, one broadcast load).
+// overlaps the work).  Lane l holds x = i0 + l + 32 q (q < 4, coalesced scalar
+// loads) and x = i0 + kChunk (the next unit's first point, one broadcast
+// load).  (The bulk kernel's lanes hold x = i0 + 4 l + q instead: VEC below.)
 //
 // Coordinates past the grid are clamped to the row's last point and a missing
 // row (j + 1 = ny, k + 1 = nz) is read as the unit's own row j or plane k: the
@@ -337,7 +338,7 @@ __device__ __forceinline__ float ext_any(float a, float b) {
 }
 
 struct RowVals {
-    float v[4];  // VEC: x = i0 + 4 lane + q; else x = i0 + lane + 32 q
+    float v[4];  // x = i0 + lane + 32 q (VEC: x = i0 + 4 lane + q)
     float e;     // x = i0 + kChunk
     float xa, xn;  // the row's two extremes (ext_all, ext_any) at this lane
 };
@@ -347,19 +348,10 @@ __device__ __forceinline__ const float* row_ptr(const float* __restrict__ v, con
     return v + ((int64_t)min(k, g.nz - 1) * g.ny + j) * g.nx;
 }
 
-template <bool VEC>
 __device__ __forceinline__ void load_row(const float* __restrict__ row, int i0, int nx, int lane,
                                          RowVals& r) {
-    if constexpr (VEC) {
-        const float4 q = __ldg(reinterpret_cast<const float4*>(row + min(i0 + 4 * lane, nx - 4)));
-        r.v[0] = q.x;
-        r.v[1] = q.y;
-        r.v[2] = q.z;
-        r.v[3] = q.w;
-    } else {
 #pragma unroll
-        for (int q = 0; q < 4; q++) r.v[q] = __ldg(row + min(i0 + lane + 32 * q, nx - 1));
-    }
+    for (int q = 0; q < 4; q++) r.v[q] = __ldg(row + min(i0 + lane + 32 * q, nx - 1));
     r.e = __ldg(row + min(i0 + kChunk, nx - 1));
 }
 
@@ -452,7 +444,7 @@ __device__ __forceinline__ uint32_t unit_sum(const RowVals& r0, const RowVals& r
     return __reduce_add_sync(kFull, packed);
 }
 
-template <bool BELOW, bool VEC>
+template <bool BELOW>
 __global__ void __launch_bounds__(32 * kCountWarps) k_mc_count(const float* __restrict__ v, Grid g,
                                                                 const uint8_t* __restrict__ ntri,
                                                                 int32_t* __restrict__ vcnt,
@@ -471,8 +463,8 @@ __global__ void __launch_bounds__(32 * kCountWarps) k_mc_count(const float* __re
     RowVals ra[kCountSlots], rb[kCountSlots];
 #pragma unroll
     for (int p = 0; p <= kCountAhead; p++) {
-        load_row<VEC>(row_ptr(v, g, j, k0 + p), i0, g.nx, lane, ra[p]);
-        load_row<VEC>(row_ptr(v, g, jb, k0 + p), i0, g.nx, lane, rb[p]);
+        load_row(row_ptr(v, g, j, k0 + p), i0, g.nx, lane, ra[p]);
+        load_row(row_ptr(v, g, jb, k0 + p), i0, g.nx, lane, rb[p]);
     }
     row_ext<BELOW>(ra[0]);
     row_ext<BELOW>(rb[0]);
@@ -486,8 +478,8 @@ __global__ void __launch_bounds__(32 * kCountWarps) k_mc_count(const float* __re
         constexpr int kA = kCountAhead + 1;
         if (kk + kA <= kCountZ && k + kA <= k1) {
             const int sn = (kk + kA) % kCountSlots;
-            load_row<VEC>(row_ptr(v, g, j, k + kA), i0, g.nx, lane, ra[sn]);
-            load_row<VEC>(row_ptr(v, g, jb, k + kA), i0, g.nx, lane, rb[sn]);
+            load_row(row_ptr(v, g, j, k + kA), i0, g.nx, lane, ra[sn]);
+            load_row(row_ptr(v, g, jb, k + kA), i0, g.nx, lane, rb[sn]);
         }
         row_ext<BELOW>(ra[s1]);
         row_ext<BELOW>(rb[s1]);
@@ -499,7 +491,7 @@ __global__ void __launch_bounds__(32 * kCountWarps) k_mc_count(const float* __re
         const bool any_in = __any_sync(kFull, inside<BELOW>(xn, g.iso));
         uint32_t sum = 0;  // vertices + 2^16 * triangles of the unit
         if (any_in && !all_in)
-            sum = unit_sum<BELOW, VEC>(ra[s0], rb[s0], ra[s1], rb[s1], has_y, k + 1 < g.nz, i0, g,
+            sum = unit_sum<BELOW, false>(ra[s0], rb[s0], ra[s1], rb[s1], has_y, k + 1 < g.nz, i0, g,
                                        lane, ntri);
         if (lane == 0) {
             const int64_t u = ((int64_t)k * g.ny + j) * g.nchunks + blockIdx.x;
@@ -1004,10 +996,10 @@ int marching_cubes(const float* values, int nx, int ny, int nz, const double* or
         k_mc_count_bulk<false><<<grid_b, 32 * (kTileChunks + 1), bulk_smem_bytes(), s>>>(
             values, g, ntri, vcnt, tcnt, act, nact, nerr);
     else if (below)
-        k_mc_count<true, false><<<grid_c, 32 * kCountWarps, 0, s>>>(values, g, ntri, vcnt, tcnt,
+        k_mc_count<true><<<grid_c, 32 * kCountWarps, 0, s>>>(values, g, ntri, vcnt, tcnt,
                                                                      act, nact);
     else
-        k_mc_count<false, false><<<grid_c, 32 * kCountWarps, 0, s>>>(values, g, ntri, vcnt, tcnt,
+        k_mc_count<false><<<grid_c, 32 * kCountWarps, 0, s>>>(values, g, ntri, vcnt, tcnt,
                                                                       act, nact);
     rc = cub_scan([&](void* t, size_t& b) {
         return cub::DeviceScan::ExclusiveSum(t, b, vcnt, vbase, U + 1, s);
