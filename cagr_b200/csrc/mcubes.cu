@@ -363,19 +363,38 @@ __device__ __forceinline__ void row_ext(RowVals& r) {
                                          ext_any<BELOW>(r.v[2], r.v[3])), r.e);
 }
 
+// VEC: a lane's fixed facts about its points x0 + q (x0 = i0 + 4 lane), set
+// once per warp: xin bit q = the point exists (x0 + q < nx), xm bit q = it has
+// a +x neighbour (x0 + q + 1 < nx), e_ok = x = i0 + kChunk exists, last = lane 31
+struct LaneVec {
+    uint32_t xin = 0, xm = 0;
+    bool e_ok = false, last = false;
+};
+
+__device__ __forceinline__ LaneVec lane_vec(int i0, int nx, int lane) {
+    LaneVec l;
+    const int x0 = i0 + 4 * lane;
+    const int have = nx - x0, room = nx - 1 - x0;
+    l.xin = have >= 4 ? 0xfu : have > 0 ? (1u << have) - 1u : 0u;
+    l.xm = room >= 4 ? 0xfu : room > 0 ? (1u << room) - 1u : 0u;
+    l.e_ok = i0 + kChunk < nx;
+    l.last = lane == 31;
+    return l;
+}
+
 // VEC: the inside bits of this lane's points x0 + q (bit q) and of x0 + 4 (bit
 // 4: the next lane's first point, or x = i0 + kChunk for lane 31); 0 for a
 // point past the grid or a missing row (ok = false)
 template <bool BELOW>
-__device__ __forceinline__ uint32_t row_nibble(const RowVals& r, bool ok, int x0, int i0, int nx,
-                                               int lane, float iso) {
+__device__ __forceinline__ uint32_t row_nibble(const RowVals& r, bool ok, const LaneVec& l,
+                                               float iso) {
     uint32_t b = 0;
 #pragma unroll
-    for (int q = 0; q < 4; q++) b |= (inside<BELOW>(r.v[q], iso) && x0 + q < nx) ? 1u << q : 0u;
-    if (!ok) b = 0;
+    for (int q = 0; q < 4; q++) b |= inside<BELOW>(r.v[q], iso) ? 1u << q : 0u;
+    b = ok ? b & l.xin : 0u;
     const uint32_t nb = __shfl_down_sync(kFull, b, 1) & 1u;
-    const uint32_t eb = (ok && i0 + kChunk < nx && inside<BELOW>(r.e, iso)) ? 1u : 0u;
-    return b | ((lane == 31 ? eb : nb) << 4);
+    const uint32_t eb = (ok && l.e_ok && inside<BELOW>(r.e, iso)) ? 1u : 0u;
+    return b | ((l.last ? eb : nb) << 4);
 }
 
 // scalar layout: ballot words, bit l of w[q] = inside at x = i0 + l + 32 q,
@@ -396,17 +415,14 @@ template <bool BELOW, bool VEC>
 __device__ __forceinline__ uint32_t unit_sum(const RowVals& r0, const RowVals& r1,
                                              const RowVals& r2, const RowVals& r3, bool has_y,
                                              bool has_z, int i0, const Grid& g, int lane,
-                                             const uint8_t* __restrict__ ntri) {
+                                             const uint8_t* __restrict__ ntri, const LaneVec& lv) {
     uint32_t packed = 0;  // this lane's 4 points
     if constexpr (VEC) {
-        const int x0 = i0 + 4 * lane;
-        const uint32_t e0 = row_nibble<BELOW>(r0, true, x0, i0, g.nx, lane, g.iso);
-        const uint32_t e1 = row_nibble<BELOW>(r1, has_y, x0, i0, g.nx, lane, g.iso);
-        const uint32_t e2 = row_nibble<BELOW>(r2, has_z, x0, i0, g.nx, lane, g.iso);
-        const uint32_t e3 = row_nibble<BELOW>(r3, has_y && has_z, x0, i0, g.nx, lane, g.iso);
-        // points of this lane with a +x neighbour (bit q: x0 + q + 1 < nx)
-        const int room = g.nx - 1 - x0;
-        const uint32_t xm = room >= 4 ? 0xfu : room > 0 ? (1u << room) - 1u : 0u;
+        const uint32_t e0 = row_nibble<BELOW>(r0, true, lv, g.iso);
+        const uint32_t e1 = row_nibble<BELOW>(r1, has_y, lv, g.iso);
+        const uint32_t e2 = row_nibble<BELOW>(r2, has_z, lv, g.iso);
+        const uint32_t e3 = row_nibble<BELOW>(r3, has_y && has_z, lv, g.iso);
+        const uint32_t xm = lv.xm;  // points of this lane with a +x neighbour
         packed = __popc((e0 ^ (e0 >> 1)) & xm);
         if (has_y) packed += __popc((e0 ^ e1) & 0xfu);
         if (has_z) packed += __popc((e0 ^ e2) & 0xfu);
@@ -492,7 +508,7 @@ __global__ void __launch_bounds__(32 * kCountWarps) k_mc_count(const float* __re
         uint32_t sum = 0;  // vertices + 2^16 * triangles of the unit
         if (any_in && !all_in)
             sum = unit_sum<BELOW, false>(ra[s0], rb[s0], ra[s1], rb[s1], has_y, k + 1 < g.nz, i0, g,
-                                       lane, ntri);
+                                         lane, ntri, LaneVec{});
         if (lane == 0) {
             const int64_t u = ((int64_t)k * g.ny + j) * g.nchunks + blockIdx.x;
             vcnt[u] = (int32_t)(sum & 0xffffu);
@@ -618,6 +634,9 @@ __global__ void __launch_bounds__(32 * (kTileChunks + 1), 8) k_mc_count_bulk(
     }
     row_ext<BELOW>(ra0);
     row_ext<BELOW>(rb0);
+    const LaneVec lv = lane_vec(i0, g.nx, lane);
+    // (unrolled by two: the compiler renames the rows instead of copying them)
+#pragma unroll 2
     for (int k = k0; k < k1; k++) {
         RowVals ra1, rb1;
         if (!take_plane(stage, full, empty, k - k0 + 1, ry, off4, offe, lane, ra1, rb1)) {
@@ -632,7 +651,8 @@ __global__ void __launch_bounds__(32 * (kTileChunks + 1), 8) k_mc_count_bulk(
         const bool any_in = __any_sync(kFull, inside<BELOW>(xn, g.iso));
         uint32_t sum = 0;  // vertices + 2^16 * triangles of the unit
         if (any_in && !all_in)
-            sum = unit_sum<BELOW, true>(ra0, rb0, ra1, rb1, has_y, k + 1 < g.nz, i0, g, lane, ntri);
+            sum = unit_sum<BELOW, true>(ra0, rb0, ra1, rb1, has_y, k + 1 < g.nz, i0, g, lane, ntri,
+                                        lv);
         if (lane == 0) {
             const int64_t u = ((int64_t)k * g.ny + j) * g.nchunks + chunk;
             vcnt[u] = (int32_t)(sum & 0xffffu);
