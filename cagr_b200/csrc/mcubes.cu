@@ -524,9 +524,10 @@ __global__ void __launch_bounds__(32 * kCountWarps) k_mc_count(const float* __re
 // pair (j, j + 1) for kBulkZ planes: a producer warp copies each plane's two
 // tile rows (one cp.async.bulk per row, completion counted on the slot's full
 // barrier) into a ring of kBulkSlots plane slots, and consumer warp c counts
-// the units of chunk c from the slots as the count kernel above does from its
-// registers (16-byte lane layout, the same clamped points, extremes and bit
-// path).  A consumer copies a plane's values to registers as soon as it has
+// the units of chunk c from the slots with the count kernel's per-unit steps
+// (the same clamped points and extremes; lane l holds x = i0 + 4 l + q, read
+// as one 16-byte word, and counts with the VEC bit path of unit_sum).  A
+// consumer copies a plane's values to registers as soon as it has
 // arrived and releases the slot on its empty barrier, so the producer keeps up
 // to kBulkSlots planes in flight per block without holding registers for
 // them.  Every wait is bounded: a wait that runs out sets *err and ends the
