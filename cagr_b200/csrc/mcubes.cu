@@ -431,7 +431,7 @@ __device__ __forceinline__ uint32_t unit_sum(const RowVals& r0, const RowVals& r
             for (int q = 0; q < 4; q++) {
                 const uint32_t cs = ((e0 >> q) & 3u) | (((e1 >> q) & 3u) << 2) |
                                     (((e2 >> q) & 3u) << 4) | (((e3 >> q) & 3u) << 6);
-                if ((xm >> q) & 1u) packed += (uint32_t)__ldg(&ntri[cs]) << 16;
+                if ((xm >> q) & 1u) packed += (uint32_t)ntri[cs] << 16;  // (shared memory)
             }
         }
     } else {
@@ -585,6 +585,8 @@ __global__ void __launch_bounds__(32 * (kTileChunks + 1), 8) k_mc_count_bulk(
     const int nw = min(kTileChunks, (g.nx - x0 + kChunk - 1) / kChunk);  // chunks in the tile
     const bool has_y = j + 1 < g.ny;
     const int nplanes = k1 - k0 + 1;  // planes k0 .. k1 (k1 = nz: the last plane again)
+    __shared__ uint8_t s_ntri[256];  // the case table's triangle counts
+    for (int i = (int)threadIdx.x; i < 256; i += (int)blockDim.x) s_ntri[i] = ntri[i];
     if (threadIdx.x == 0) {
         for (int s = 0; s < kBulkSlots; s++) {
             mbar_init(full + s, 1);
@@ -652,8 +654,8 @@ __global__ void __launch_bounds__(32 * (kTileChunks + 1), 8) k_mc_count_bulk(
         const bool any_in = __any_sync(kFull, inside<BELOW>(xn, g.iso));
         uint32_t sum = 0;  // vertices + 2^16 * triangles of the unit
         if (any_in && !all_in)
-            sum = unit_sum<BELOW, true>(ra0, rb0, ra1, rb1, has_y, k + 1 < g.nz, i0, g, lane, ntri,
-                                        lv);
+            sum = unit_sum<BELOW, true>(ra0, rb0, ra1, rb1, has_y, k + 1 < g.nz, i0, g, lane,
+                                        s_ntri, lv);
         if (lane == 0) {
             const int64_t u = ((int64_t)k * g.ny + j) * g.nchunks + chunk;
             vcnt[u] = (int32_t)(sum & 0xffffu);
